@@ -1,0 +1,229 @@
+/*
+ * mvr.h -- C ABI of libmvr, the B200-native (sm_100a) GPU multi-vector
+ * (ColBERT-style) search engine: centroid scoring -> IVF probe -> candidate
+ * filter -> residual decompression -> exact MaxSim rerank -> top-k.
+ *
+ * Plain pointers and sizes only.  Every entry point returns an mvr_status
+ * (MVR_OK == 0); on failure mvr_last_error() describes the error of the
+ * calling thread.  No entry point calls exit().  One index handle is used
+ * from one host thread at a time.  Index-resident arrays live in the HBM of
+ * the device named at load; search workspaces are owned by the handle and
+ * reused across calls (the reference re-allocates and frees them per call).
+ *
+ * The product path never falls back to the CPU: without a usable CUDA device
+ * the entry points fail with MVR_ERR_CUDA.
+ */
+#ifndef MVR_H
+#define MVR_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  MVR_OK = 0,
+  MVR_ERR_INVALID_ARG = 1, /* bad size / shape / parameter */
+  MVR_ERR_IO = 2,          /* file missing, unreadable or malformed */
+  MVR_ERR_CUDA = 3,        /* CUDA runtime or kernel error, no device */
+  MVR_ERR_OOM = 4,         /* device or host allocation failed */
+  MVR_ERR_UNSUPPORTED = 5  /* valid for the reference, not supported here */
+} mvr_status;
+
+/* search flags */
+#define MVR_SEM_PP 0u    /* rerank over each doc's true token count
+                            (RerankPP.hpp:115-161) */
+#define MVR_SEM_BASIC 1u /* rerank over docs zero-padded to the longest doc,
+                            i.e. max(0, .) per query token for shorter docs
+                            (Rerank.hpp:166-179,287-306) */
+
+typedef struct mvr_index mvr_index;
+
+typedef struct {
+  uint32_t n_item, n_centroid, dim, n_bit;
+  uint64_t n_vec, n_ele_ivf;
+  uint32_t max_item_n_vec, max_ivf_list;
+  uint64_t device_bytes; /* HBM held by the index arrays */
+  int device;
+} mvr_index_info;
+
+typedef struct {
+  double wall_s;          /* host wall time of the whole call */
+  double device_ms;       /* CUDA-event time of the device pipeline */
+  double batch_ms_max;    /* slowest batch (device time) */
+  uint32_t n_batch;       /* query batches processed */
+  uint32_t gpu_launches;  /* kernels launched by the call */
+  uint64_t h2d_bytes, d2h_bytes;
+  uint64_t n_cand_total;  /* sum over queries of candidate-set sizes */
+  uint64_t n_rerank_tok;  /* sum over queries of reranked doc tokens */
+  uint64_t n_list_ent;    /* sum over queries of probed IVF entries read */
+  double stage_ms[5];     /* CUDA-event time summed over batches: query
+                             copy, scoring + probe, filter, rerank + top-k,
+                             result copy */
+} mvr_stats;
+
+/* Per-query stage trace (parity tests).  Caller-owned host buffers. */
+typedef struct {
+  uint32_t *probe_id;    /* [nq*nprobe] per token, by (score desc, id asc) */
+  float *probe_score;    /* [nq*nprobe] S = q.c + 1 */
+  uint32_t cand_cap;     /* capacity of cand_id / cand_score */
+  uint32_t n_cand;       /* out: candidate-set size */
+  uint32_t *cand_id;     /* [cand_cap] candidate doc ids, ascending */
+  float *cand_score;     /* [cand_cap] approximate score of cand_id[i] */
+  uint32_t n_short;      /* out: shortlist size = min(probe_topk, n_cand) */
+  uint32_t *short_id;    /* [probe_topk] shortlist, ascending doc id */
+  float *short_approx;   /* [probe_topk] approximate score */
+  float *short_exact;    /* [probe_topk] exact MaxSim */
+  float *topk_score;     /* [topk] final result */
+  uint32_t *topk_id;     /* [topk] */
+} mvr_trace;
+
+/* Error text of the last failing call on this thread ("" if none). */
+const char *mvr_last_error(void);
+
+/* Number of visible CUDA devices (0 when none). */
+int mvr_device_count(void);
+
+/* Load the reference's on-disk index from `index_dir`:
+ *   item_n_vec_l.npy  uint32 [n_item]          doc lengths
+ *   centroid_l.npy    float32 [C, dim]
+ *   vq_code_l.npy     int32/uint32 [n_vec]     token -> centroid
+ *   weight_l.npy      float32 [2^n_bit]        bucket weights
+ *   residual_code_l.npy uint8 [n_vec*dim*n_bit/8] MSB-first packed buckets
+ *   ivf.index         binary CSR (IVFIndex.hpp:168-183)
+ * Replaces IGPGPUPP(item_n_vec_l_fname, n_cpu_thread) + buildIndex(...)
+ * (src/impl/IGPGPUPP.hpp:67-92,120-251) and the IGPGPUBasic equivalents
+ * (src/impl/IGPGPUBasic.hpp:71-94,122-188).  n_centroid / n_bit must match
+ * the files (the reference asserts the same).  dim must be 128. */
+int mvr_index_load(const char *index_dir, uint32_t n_centroid, uint32_t n_bit,
+                   int device, mvr_index **out);
+
+/* Same, from the individual files (IGPGPUPP::buildIndex's argument list,
+ * src/impl/IGPGPUPP.hpp:120-124, plus the item_n_vec_l file its constructor
+ * takes). */
+int mvr_index_load_files(const char *item_n_vec_l_fname,
+                         const char *centroid_l_fname,
+                         const char *vq_code_l_fname,
+                         const char *ivf_index_fname,
+                         const char *weight_l_fname,
+                         const char *residual_code_l_fname,
+                         uint32_t n_centroid, uint32_t n_bit, int device,
+                         mvr_index **out);
+
+/* Same index from host arrays (the contents of the files above; ivf as the
+ * CSR triple offsets/sizes/ids).  Arrays are copied; the caller keeps them. */
+int mvr_index_from_arrays(const uint32_t *item_n_vec_l, uint32_t n_item,
+                          const float *centroid_l, uint32_t n_centroid,
+                          uint32_t dim, const uint32_t *vq_code_l,
+                          uint64_t n_vec, const uint64_t *ivf_offset_l,
+                          const uint32_t *ivf_size_l, const uint32_t *ivf,
+                          uint64_t n_ele_ivf, const float *weight_l,
+                          uint32_t n_bit, const uint8_t *residual_code_l,
+                          int device, mvr_index **out);
+
+/* Same, from arrays already resident on `device` (device pointers; copied
+ * device-to-device), e.g. an index built on the GPU. */
+int mvr_index_from_device_arrays(const uint32_t *item_n_vec_l, uint32_t n_item,
+                                 const float *centroid_l, uint32_t n_centroid,
+                                 uint32_t dim, const uint32_t *vq_code_l,
+                                 uint64_t n_vec, const uint64_t *ivf_offset_l,
+                                 const uint32_t *ivf_size_l, const uint32_t *ivf,
+                                 uint64_t n_ele_ivf, const float *weight_l,
+                                 uint32_t n_bit,
+                                 const uint8_t *residual_code_l, int device,
+                                 mvr_index **out);
+
+int mvr_index_free(mvr_index *h);
+int mvr_index_get_info(const mvr_index *h, mvr_index_info *info);
+
+/* Queries per device batch (default chosen from the index size). */
+int mvr_index_set_batch(mvr_index *h, uint32_t max_batch_queries);
+
+/* Batched search with HOST buffers (queries in, results out; copies inside).
+ * query_l: float32 tokens, query i = rows [tok_off[i], tok_off[i+1]) of a
+ * [*, dim] matrix; tok_off == NULL means every query has query_n_vec tokens
+ * (the reference's uniform layout, IGPGPUPP::search src/impl/IGPGPUPP.hpp:
+ * 253-331).  1 <= tokens per query <= 64, 1 <= nprobe <= min(32, C),
+ * topk <= probe_topk <= 8192, topk <= 1024 (probe_topk >= topk is the
+ * reference's own check, IGPGPUPP.hpp:256-259).  Results per query are
+ * sorted by (score desc, doc id asc); when fewer than topk docs qualify the
+ * tail holds id 0xffffffff and score -inf.  query_time_s (nullable) receives
+ * each query's batch latency in seconds. */
+int mvr_search(mvr_index *h, const float *query_l, const uint64_t *tok_off,
+               uint32_t n_query, uint32_t query_n_vec, uint32_t topk,
+               uint32_t nprobe, uint32_t probe_topk, uint32_t flags,
+               float *result_score_l, uint32_t *result_id_l,
+               double *query_time_s, mvr_stats *stats);
+
+/* mvr_search plus per-query stage times (seconds, of the query's batch):
+ * stage_time_s[i*5 + k], k = 0 query copy, 1 centroid scoring + probe,
+ * 2 candidate filter + shortlist, 3 rerank + top-k, 4 result copy -- the
+ * stage columns of the reference's performance TSV (IGPGPUBasic.cpp:183-204). */
+int mvr_search_staged(mvr_index *h, const float *query_l,
+                      const uint64_t *tok_off, uint32_t n_query,
+                      uint32_t query_n_vec, uint32_t topk, uint32_t nprobe,
+                      uint32_t probe_topk, uint32_t flags,
+                      float *result_score_l, uint32_t *result_id_l,
+                      double *query_time_s, double *stage_time_s,
+                      mvr_stats *stats);
+
+/* Same search with DEVICE buffers already resident on the index's device;
+ * tok_off stays a host array.  Runs on `cuda_stream` (NULL: the legacy
+ * default stream) and returns after the results are written (the stream is
+ * synchronised). */
+int mvr_search_device(mvr_index *h, const float *d_query_l,
+                      const uint64_t *tok_off, uint32_t n_query,
+                      uint32_t query_n_vec, uint32_t topk, uint32_t nprobe,
+                      uint32_t probe_topk, uint32_t flags,
+                      float *d_result_score_l, uint32_t *d_result_id_l,
+                      void *cuda_stream, mvr_stats *stats);
+
+/* One query through the same kernels with every stage's output copied back
+ * (parity tests).  query: host float32 [nq, dim]. */
+int mvr_search_trace(mvr_index *h, const float *query, uint32_t nq,
+                     uint32_t topk, uint32_t nprobe, uint32_t probe_topk,
+                     uint32_t flags, mvr_trace *trace);
+
+/* Decompressed token vectors x = centroid[code] + W[bucket] for the given
+ * global token ids (host in/out, out: float32 [n, dim]); the decoder of
+ * decompressAndAddResidual (RerankPP.hpp:65-113). */
+int mvr_decompress(mvr_index *h, const uint64_t *vec_id, uint64_t n,
+                   float *out);
+
+/* Bucket index of every dimension of the given tokens (host out: uint8
+ * [n, dim]), unpacked on the device by the rerank decoder's bit layout. */
+int mvr_unpack_buckets(mvr_index *h, const uint64_t *vec_id, uint64_t n,
+                       uint8_t *out);
+
+/* ---- index build (device pointers; GPU counterpart of the reference's
+ *      build pipeline, vq_sq_pack.py:30-109 and
+ *      ResidualScalarQuantizationPackGPU.hpp:30-80) ---- */
+
+/* code[i] = argmax_c dot(vec_i, centroid_c), lowest id on ties; score[i]
+ * (nullable) = that max + 1.  FP32, canonical dot order. */
+int mvr_assign_device(const float *d_vec, uint64_t n_vec,
+                      const float *d_centroid, uint32_t n_centroid,
+                      uint32_t dim, uint32_t *d_code, float *d_score,
+                      void *cuda_stream);
+
+/* Packed residual bytes (MSB-first, bucket = #cutoffs <= vec - centroid):
+ * out [n_vec * dim*n_bit/8]. */
+int mvr_pack_residual_device(const float *d_vec, uint64_t n_vec,
+                             const float *d_centroid, uint32_t dim,
+                             const uint32_t *d_code, const float *cutoff_l,
+                             uint32_t n_bit, uint8_t *d_out,
+                             void *cuda_stream);
+
+/* FP64 k-means update: sum[c][d] += vec[i][d] and count[c] += 1 over
+ * code[i] == c (double accumulation; caller zeroes sum/count). */
+int mvr_kmeans_accumulate_device(const float *d_vec, uint64_t n_vec,
+                                 uint32_t dim, const uint32_t *d_code,
+                                 double *d_sum, uint64_t *d_count,
+                                 void *cuda_stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MVR_H */

@@ -1,0 +1,904 @@
+// mvr_capi.cu -- the C ABI of libmvr (include/mvr.h): index residency in
+// HBM, per-handle search workspaces, the batched asynchronous search
+// pipeline and the index-build entry points.
+#include "mvr.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "mvr_aux.cuh"
+#include "mvr_common.cuh"
+#include "mvr_io.hpp"
+#include "mvr_kernels.cuh"
+
+using namespace mvr;
+
+namespace {
+
+thread_local std::string g_err;
+
+int set_err(int code, const char *fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define CUDA_TRY(expr)                                                              \
+  do {                                                                              \
+    cudaError_t e_ = (expr);                                                        \
+    if (e_ != cudaSuccess) {                                                        \
+      return set_err(e_ == cudaErrorMemoryAllocation ? MVR_ERR_OOM : MVR_ERR_CUDA,  \
+                     "%s: %s (%s:%d)", #expr, cudaGetErrorString(e_), __FILE__,     \
+                     __LINE__);                                                     \
+    }                                                                               \
+  } while (0)
+
+#define MVR_TRY(expr)            \
+  do {                           \
+    int r_ = (expr);             \
+    if (r_ != MVR_OK) return r_; \
+  } while (0)
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int d) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    cudaSetDevice(d);
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+template <class T>
+int dalloc(T **p, size_t n, std::vector<void *> *owner = nullptr) {
+  *p = nullptr;
+  if (n == 0) n = 1;
+  CUDA_TRY(cudaMalloc((void **)p, n * sizeof(T)));
+  if (owner) owner->push_back(*p);
+  return MVR_OK;
+}
+
+void dfree(void *p) {
+  if (p) cudaFree(p);
+}
+
+// One decode-table row per byte value: weights of its 8/b values, MSB-first
+// (SQInfoPP ctor, DataStructPP.hpp:150-187).
+std::vector<float> make_lut(uint32_t n_bit, const float *weight) {
+  const uint32_t vpb = 8u / n_bit, mask = (1u << n_bit) - 1u;
+  std::vector<float> lut(256 * vpb);
+  for (uint32_t code = 0; code < 256; code++)
+    for (uint32_t i = 0; i < vpb; i++)
+      lut[code * vpb + i] = weight[(code >> (8u - n_bit * (i + 1u))) & mask];
+  return lut;
+}
+
+__global__ void validate_kernel(const uint32_t *code, uint64_t n_vec, uint32_t n_cent,
+                                const uint32_t *ids, uint64_t n_ele, uint32_t n_item,
+                                unsigned *flag) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_vec; i += stride)
+    if (code[i] >= n_cent) atomicOr(flag, 1u);
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_ele; i += stride)
+    if (ids[i] >= n_item) atomicOr(flag, 2u);
+}
+
+}  // namespace
+
+// ----------------------------------------------------------------------
+// handle
+// ----------------------------------------------------------------------
+struct Workspace {
+  uint32_t slots = 0, rank_stride = 0;
+  uint32_t *stamp = nullptr;
+  uint8_t *rank = nullptr;
+  uint64_t *key = nullptr;
+  // per batch
+  uint32_t batch_slots = 0, tok_cap = 0, np_cap = 0, short_cap = 0, topk_cap = 0;
+  size_t part_cap = 0;
+  float *q = nullptr;
+  uint32_t *probe_id = nullptr, *part_id = nullptr;
+  float *probe_s = nullptr, *part_s = nullptr;
+  uint32_t *short_id = nullptr, *n_short = nullptr;
+  float *short_approx = nullptr, *exact = nullptr;
+  float *out_s = nullptr;
+  uint32_t *out_id = nullptr;
+  // per call
+  size_t off_cap = 0, stat_cap = 0;
+  uint64_t *q_off = nullptr;    // device, all batches' relative offsets
+  uint64_t *h_off = nullptr;    // pinned mirror
+  uint32_t *qstat = nullptr;    // device [n_query][3]
+  uint32_t *h_qstat = nullptr;  // pinned mirror
+};
+
+struct mvr_index {
+  int device = 0;
+  int n_sm = 148;
+  DevIndex dix{};
+  std::vector<void *> bufs;
+  uint32_t max_ivf_list = 0;
+  uint64_t device_bytes = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<cudaEvent_t> events;
+  uint32_t batch_cap = 0;
+  uint32_t epoch = 0;
+  Workspace ws;
+
+  ~mvr_index() {
+    DeviceGuard g(device);
+    if (stream) cudaStreamSynchronize(stream);
+    for (void *p : bufs) dfree(p);
+    free_scratch();
+    free_batch();
+    dfree(ws.q_off);
+    dfree(ws.qstat);
+    if (ws.h_off) cudaFreeHost(ws.h_off);
+    if (ws.h_qstat) cudaFreeHost(ws.h_qstat);
+    for (auto e : events) cudaEventDestroy(e);
+    if (stream) cudaStreamDestroy(stream);
+  }
+  void free_scratch() {
+    dfree(ws.stamp); dfree(ws.rank); dfree(ws.key);
+    ws.stamp = nullptr; ws.rank = nullptr; ws.key = nullptr;
+    ws.slots = 0;
+  }
+  void free_batch() {
+    for (void *p : {(void *)ws.q, (void *)ws.probe_id, (void *)ws.part_id, (void *)ws.probe_s,
+                    (void *)ws.part_s, (void *)ws.short_id, (void *)ws.n_short,
+                    (void *)ws.short_approx, (void *)ws.exact, (void *)ws.out_s, (void *)ws.out_id})
+      dfree(p);
+    ws.q = nullptr; ws.probe_id = ws.part_id = nullptr; ws.probe_s = ws.part_s = nullptr;
+    ws.short_id = ws.n_short = nullptr; ws.short_approx = ws.exact = nullptr;
+    ws.out_s = nullptr; ws.out_id = nullptr;
+    ws.batch_slots = ws.tok_cap = ws.np_cap = ws.short_cap = ws.topk_cap = 0;
+    ws.part_cap = 0;
+  }
+};
+
+namespace {
+
+uint32_t default_batch(const mvr_index *h) {
+  // Per-slot filter scratch is n_item * (4 + 32 + 8) bytes; keep all slots
+  // within ~16 GB and aim for two waves of 1024-thread filter CTAs.
+  const double per_slot = (double)h->dix.n_item * 44.0;
+  uint32_t b = 2u * (uint32_t)h->n_sm;
+  const double budget = 16.0 * (1ull << 30);
+  while (b > 1 && per_slot * b > budget) b--;
+  return std::max(1u, b);
+}
+
+int ensure_scratch(mvr_index *h, uint32_t slots, uint32_t rank_stride) {
+  Workspace &w = h->ws;
+  if (w.slots >= slots && w.rank_stride >= rank_stride) return MVR_OK;
+  h->free_scratch();
+  const size_t n = (size_t)h->dix.n_item;
+  MVR_TRY(dalloc(&w.stamp, slots * n));
+  MVR_TRY(dalloc(&w.rank, slots * n * rank_stride));
+  MVR_TRY(dalloc(&w.key, slots * n));
+  CUDA_TRY(cudaMemsetAsync(w.stamp, 0, slots * n * sizeof(uint32_t), h->stream));
+  CUDA_TRY(cudaMemsetAsync(w.rank, 0xff, slots * n * rank_stride, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  w.slots = slots;
+  w.rank_stride = rank_stride;
+  h->epoch = 0;
+  return MVR_OK;
+}
+
+int ensure_batch(mvr_index *h, uint32_t slots, uint32_t tok_cap, uint32_t nprobe,
+                 uint32_t short_cap, uint32_t topk, size_t part_need) {
+  Workspace &w = h->ws;
+  if (w.batch_slots >= slots && w.tok_cap >= tok_cap && w.np_cap >= nprobe &&
+      w.short_cap >= short_cap && w.topk_cap >= topk && w.part_cap >= part_need)
+    return MVR_OK;
+  const uint32_t s = std::max(slots, w.batch_slots);
+  tok_cap = std::max(tok_cap, w.tok_cap);
+  nprobe = std::max(nprobe, w.np_cap);
+  short_cap = std::max(short_cap, w.short_cap);
+  topk = std::max(topk, w.topk_cap);
+  part_need = std::max(part_need, w.part_cap);
+  h->free_batch();
+  MVR_TRY(dalloc(&w.q, (size_t)tok_cap * kDim));
+  MVR_TRY(dalloc(&w.probe_id, (size_t)tok_cap * nprobe));
+  MVR_TRY(dalloc(&w.probe_s, (size_t)tok_cap * nprobe));
+  MVR_TRY(dalloc(&w.part_id, part_need));
+  MVR_TRY(dalloc(&w.part_s, part_need));
+  MVR_TRY(dalloc(&w.short_id, (size_t)s * short_cap));
+  MVR_TRY(dalloc(&w.short_approx, (size_t)s * short_cap));
+  MVR_TRY(dalloc(&w.exact, (size_t)s * short_cap));
+  MVR_TRY(dalloc(&w.n_short, (size_t)s));
+  MVR_TRY(dalloc(&w.out_s, (size_t)s * topk));
+  MVR_TRY(dalloc(&w.out_id, (size_t)s * topk));
+  w.batch_slots = s;
+  w.tok_cap = tok_cap;
+  w.np_cap = nprobe;
+  w.short_cap = short_cap;
+  w.topk_cap = topk;
+  w.part_cap = part_need;
+  return MVR_OK;
+}
+
+int ensure_call(mvr_index *h, size_t n_off, size_t n_stat, size_t n_events) {
+  Workspace &w = h->ws;
+  if (w.off_cap < n_off) {
+    dfree(w.q_off);
+    w.q_off = nullptr;
+    if (w.h_off) cudaFreeHost(w.h_off);
+    w.h_off = nullptr;
+    MVR_TRY(dalloc(&w.q_off, n_off));
+    CUDA_TRY(cudaMallocHost((void **)&w.h_off, n_off * sizeof(uint64_t)));
+    w.off_cap = n_off;
+  }
+  if (w.stat_cap < n_stat) {
+    dfree(w.qstat);
+    w.qstat = nullptr;
+    if (w.h_qstat) cudaFreeHost(w.h_qstat);
+    w.h_qstat = nullptr;
+    MVR_TRY(dalloc(&w.qstat, n_stat));
+    CUDA_TRY(cudaMallocHost((void **)&w.h_qstat, n_stat * sizeof(uint32_t)));
+    w.stat_cap = n_stat;
+  }
+  while (h->events.size() < n_events) {
+    cudaEvent_t e;
+    CUDA_TRY(cudaEventCreate(&e));
+    h->events.push_back(e);
+  }
+  return MVR_OK;
+}
+
+size_t part_entries(const mvr_index *h, uint32_t n_tok, uint32_t nprobe, int *splits_out) {
+  const int splits = probe_splits(n_tok, h->dix.n_centroid_pad, h->n_sm);
+  *splits_out = splits;
+  return splits > 1 ? (size_t)splits * n_tok * nprobe : 1;
+}
+
+int check_search_args(const mvr_index *h, uint32_t n_query, uint32_t topk, uint32_t nprobe,
+                      uint32_t probe_topk) {
+  if (!h) return set_err(MVR_ERR_INVALID_ARG, "null index handle");
+  if (probe_topk < topk)
+    return set_err(MVR_ERR_INVALID_ARG,
+                   "probe_topk (%u) is smaller than topk (%u)", probe_topk, topk);
+  if (topk == 0 || topk > (uint32_t)kMaxTopk)
+    return set_err(MVR_ERR_INVALID_ARG, "topk must be in [1, %d], got %u", kMaxTopk, topk);
+  if (probe_topk > (uint32_t)kMaxShort)
+    return set_err(MVR_ERR_INVALID_ARG, "probe_topk must be <= %d, got %u", kMaxShort, probe_topk);
+  if (nprobe == 0 || nprobe > h->dix.n_centroid)
+    return set_err(MVR_ERR_INVALID_ARG, "nprobe (%u) must be in [1, n_centroid=%u]", nprobe,
+                   h->dix.n_centroid);
+  if (nprobe > (uint32_t)kMaxProbe)
+    return set_err(MVR_ERR_UNSUPPORTED, "nprobe > %d is not supported", kMaxProbe);
+  (void)n_query;
+  return MVR_OK;
+}
+
+int build_offsets(const uint64_t *tok_off, uint32_t n_query, uint32_t query_n_vec,
+                  std::vector<uint64_t> &off, uint32_t *nq_max) {
+  off.resize((size_t)n_query + 1);
+  *nq_max = 0;
+  if (!tok_off) {
+    if (query_n_vec == 0 || query_n_vec > (uint32_t)kMaxQueryTok)
+      return set_err(MVR_ERR_INVALID_ARG, "query_n_vec must be in [1, %d], got %u", kMaxQueryTok,
+                     query_n_vec);
+    for (uint32_t i = 0; i <= n_query; i++) off[i] = (uint64_t)i * query_n_vec;
+    *nq_max = query_n_vec;
+    return MVR_OK;
+  }
+  if (tok_off[0] != 0) return set_err(MVR_ERR_INVALID_ARG, "tok_off[0] must be 0");
+  for (uint32_t i = 0; i < n_query; i++) {
+    if (tok_off[i + 1] <= tok_off[i] || tok_off[i + 1] - tok_off[i] > (uint64_t)kMaxQueryTok)
+      return set_err(MVR_ERR_INVALID_ARG, "query %u has %lld tokens (allowed 1..%d)", i,
+                     (long long)(tok_off[i + 1] - tok_off[i]), kMaxQueryTok);
+    *nq_max = std::max(*nq_max, (uint32_t)(tok_off[i + 1] - tok_off[i]));
+  }
+  std::memcpy(off.data(), tok_off, off.size() * sizeof(uint64_t));
+  return MVR_OK;
+}
+
+// The shared batched pipeline.  host_io: queries/results are host buffers
+// (copied per batch inside the call); otherwise device buffers.
+// Events: 5 per batch (start, query copied, probed, filtered, reranked) plus
+// one closing event; stage_s (nullable) receives per query the 5 stage times
+// of its batch: query copy, centroid scoring + probe, filter, rerank + top-k,
+// result copy.
+int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, uint32_t n_query,
+                uint32_t query_n_vec, uint32_t topk, uint32_t nprobe, uint32_t probe_topk,
+                uint32_t flags, float *out_s, uint32_t *out_id, double *query_time_s,
+                double *stage_s, mvr_stats *stats, cudaStream_t st, bool host_io) {
+  const auto t_start = std::chrono::steady_clock::now();
+  MVR_TRY(check_search_args(h, n_query, topk, nprobe, probe_topk));
+  if (n_query == 0) {
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    return MVR_OK;
+  }
+  if (!query || !out_s || !out_id) return set_err(MVR_ERR_INVALID_ARG, "null query/result buffer");
+  if (flags > MVR_SEM_BASIC) return set_err(MVR_ERR_INVALID_ARG, "unknown flags %u", flags);
+  std::vector<uint64_t> off;
+  uint32_t nq_max = 0;
+  MVR_TRY(build_offsets(tok_off_in, n_query, query_n_vec, off, &nq_max));
+  DeviceGuard g(h->device);
+
+  const uint32_t B = h->batch_cap ? h->batch_cap : default_batch(h);
+  const uint32_t n_batch = (n_query + B - 1) / B;
+  uint32_t tok_cap = 0;
+  size_t part_need = 1;
+  for (uint32_t bt = 0; bt < n_batch; bt++) {
+    const uint32_t s = bt * B, e = std::min(n_query, s + B);
+    const uint32_t T = (uint32_t)(off[e] - off[s]);
+    tok_cap = std::max(tok_cap, T);
+    int sp;
+    part_need = std::max(part_need, part_entries(h, T, nprobe, &sp));
+  }
+  const uint32_t rank_stride = nq_max <= 32 ? 32u : 64u;
+  MVR_TRY(ensure_scratch(h, std::min(B, n_query), rank_stride));
+  MVR_TRY(ensure_batch(h, std::min(B, n_query), tok_cap, nprobe, probe_topk, topk, part_need));
+  MVR_TRY(ensure_call(h, (size_t)n_query + n_batch, (size_t)n_query * 3, 5 * n_batch + 1));
+  Workspace &w = h->ws;
+
+  // relative token offsets of every batch, uploaded once
+  for (uint32_t bt = 0, pos = 0; bt < n_batch; bt++) {
+    const uint32_t s = bt * B, e = std::min(n_query, s + B);
+    for (uint32_t i = s; i <= e; i++) w.h_off[pos++] = off[i] - off[s];
+  }
+  CUDA_TRY(cudaMemcpyAsync(w.q_off, w.h_off, ((size_t)n_query + n_batch) * sizeof(uint64_t),
+                           cudaMemcpyHostToDevice, st));
+
+  FilterScratch scr{w.stamp, w.rank, w.key, h->dix.n_item, w.rank_stride};
+  int launches = 0;
+  uint64_t h2d = ((size_t)n_query + n_batch) * sizeof(uint64_t), d2h = 0;
+  for (uint32_t bt = 0; bt < n_batch; bt++) {
+    const uint32_t s = bt * B, e = std::min(n_query, s + B), nb = e - s;
+    CUDA_TRY(cudaEventRecord(h->events[bt * 5 + 0], st));
+    const uint32_t T = (uint32_t)(off[e] - off[s]);
+    const uint64_t *qo = w.q_off + (size_t)s + bt;
+    const float *qp;
+    if (host_io) {
+      CUDA_TRY(cudaMemcpyAsync(w.q, query + off[s] * kDim, (size_t)T * kDim * sizeof(float),
+                               cudaMemcpyHostToDevice, st));
+      h2d += (size_t)T * kDim * sizeof(float);
+      qp = w.q;
+    } else {
+      qp = query + off[s] * kDim;
+    }
+    CUDA_TRY(cudaEventRecord(h->events[bt * 5 + 1], st));
+    int splits;
+    part_entries(h, T, nprobe, &splits);
+    CUDA_TRY(launch_probe(h->dix, qp, T, nprobe, splits, w.part_id, w.part_s, w.probe_id,
+                          w.probe_s, st, &launches));
+    CUDA_TRY(cudaEventRecord(h->events[bt * 5 + 2], st));
+    if (++h->epoch == 0) {  // stamps wrapped: clear them
+      CUDA_TRY(cudaMemsetAsync(w.stamp, 0, (size_t)w.slots * h->dix.n_item * sizeof(uint32_t), st));
+      h->epoch = 1;
+    }
+    CUDA_TRY(launch_filter(h->dix, w.probe_id, w.probe_s, nprobe, qo, nb, probe_topk, scr, h->epoch,
+                           w.short_id, w.short_approx, w.n_short, w.qstat + (size_t)s * 3, st,
+                           &launches));
+    CUDA_TRY(cudaEventRecord(h->events[bt * 5 + 3], st));
+    CUDA_TRY(launch_rerank(h->dix, qp, qo, nb, w.short_id, w.n_short, probe_topk, (int)flags,
+                           w.exact, st, &launches));
+    float *os = host_io ? w.out_s : out_s + (size_t)s * topk;
+    uint32_t *oi = host_io ? w.out_id : out_id + (size_t)s * topk;
+    CUDA_TRY(launch_topk(w.short_id, w.exact, w.n_short, nb, probe_topk, topk, os, oi, st, &launches));
+    CUDA_TRY(cudaEventRecord(h->events[bt * 5 + 4], st));
+    if (host_io) {
+      CUDA_TRY(cudaMemcpyAsync(out_s + (size_t)s * topk, w.out_s, (size_t)nb * topk * sizeof(float),
+                               cudaMemcpyDeviceToHost, st));
+      CUDA_TRY(cudaMemcpyAsync(out_id + (size_t)s * topk, w.out_id,
+                               (size_t)nb * topk * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+      d2h += (size_t)nb * topk * 8;
+    }
+  }
+  CUDA_TRY(cudaEventRecord(h->events[n_batch * 5], st));
+  CUDA_TRY(cudaMemcpyAsync(w.h_qstat, w.qstat, (size_t)n_query * 3 * sizeof(uint32_t),
+                           cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  CUDA_TRY(cudaGetLastError());
+
+  float total_ms = 0.f, max_ms = 0.f;
+  CUDA_TRY(cudaEventElapsedTime(&total_ms, h->events[0], h->events[n_batch * 5]));
+  for (uint32_t bt = 0; bt < n_batch; bt++) {
+    float ms = 0.f, st_ms[5];
+    CUDA_TRY(cudaEventElapsedTime(&ms, h->events[bt * 5], h->events[(bt + 1) * 5]));
+    for (int k = 0; k < 5; k++)
+      CUDA_TRY(cudaEventElapsedTime(&st_ms[k], h->events[bt * 5 + k], h->events[bt * 5 + k + 1]));
+    max_ms = std::max(max_ms, ms);
+    const uint32_t s = bt * B, e = std::min(n_query, s + B);
+    for (uint32_t i = s; i < e; i++) {
+      if (query_time_s) query_time_s[i] = ms * 1e-3;
+      if (stage_s)
+        for (int k = 0; k < 5; k++) stage_s[(size_t)i * 5 + k] = st_ms[k] * 1e-3;
+    }
+  }
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->device_ms = total_ms;
+    stats->batch_ms_max = max_ms;
+    stats->n_batch = n_batch;
+    stats->gpu_launches = (uint32_t)launches;
+    stats->h2d_bytes = h2d;
+    stats->d2h_bytes = d2h;
+    for (uint32_t i = 0; i < n_query; i++) {
+      stats->n_cand_total += w.h_qstat[i * 3 + 0];
+      stats->n_list_ent += w.h_qstat[i * 3 + 1];
+      stats->n_rerank_tok += w.h_qstat[i * 3 + 2];
+    }
+    for (uint32_t bt = 0; bt < n_batch; bt++)
+      for (int k = 0; k < 5; k++) {
+        float ms = 0.f;
+        CUDA_TRY(cudaEventElapsedTime(&ms, h->events[bt * 5 + k], h->events[bt * 5 + k + 1]));
+        stats->stage_ms[k] += ms;
+      }
+    stats->wall_s =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+  }
+  return MVR_OK;
+}
+
+int finish_index(mvr_index *h, const uint32_t *item_n_vec_host, const uint32_t *ivf_size_host,
+                 const float *weight, std::unique_ptr<mvr_index> &owner, mvr_index **out) {
+  DevIndex &d = h->dix;
+  uint32_t mx = 0;
+  for (uint32_t i = 0; i < d.n_item; i++) mx = std::max(mx, item_n_vec_host[i]);
+  d.max_item_n_vec = mx;
+  uint32_t ml = 0;
+  for (uint32_t c = 0; c < d.n_centroid; c++) ml = std::max(ml, ivf_size_host[c]);
+  h->max_ivf_list = ml;
+  const std::vector<float> lut = make_lut(d.n_bit, weight);
+  float *dl;
+  MVR_TRY(dalloc(&dl, lut.size(), &h->bufs));
+  CUDA_TRY(cudaMemcpy(dl, lut.data(), lut.size() * sizeof(float), cudaMemcpyHostToDevice));
+  d.lut = dl;
+  float *ct;
+  MVR_TRY(dalloc(&ct, (size_t)kDim * d.n_centroid_pad, &h->bufs));
+  CUDA_TRY(launch_transpose_centroid(d.centroid, d.n_centroid, d.n_centroid_pad, ct, h->stream));
+  d.centroid_t = ct;
+  unsigned *flag;
+  MVR_TRY(dalloc(&flag, 1));
+  std::unique_ptr<void, void (*)(void *)> flag_guard(flag, dfree);
+  CUDA_TRY(cudaMemsetAsync(flag, 0, sizeof(unsigned), h->stream));
+  validate_kernel<<<4 * h->n_sm, 256, 0, h->stream>>>(d.vq_code, d.n_vec, d.n_centroid, d.ivf_ids,
+                                                     d.n_ele_ivf, d.n_item, flag);
+  CUDA_TRY(cudaGetLastError());
+  unsigned hflag = 0;
+  CUDA_TRY(cudaMemcpyAsync(&hflag, flag, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  if (hflag & 1u) return set_err(MVR_ERR_INVALID_ARG, "vq_code holds a centroid id >= n_centroid");
+  if (hflag & 2u) return set_err(MVR_ERR_INVALID_ARG, "ivf holds a doc id >= n_item");
+  h->device_bytes = 0;
+  h->device_bytes += (size_t)d.n_centroid * kDim * 4 * 1 + (size_t)kDim * d.n_centroid_pad * 4;
+  h->device_bytes += d.n_vec * (4 + d.bytes_per_vec) + (size_t)d.n_item * 12;
+  h->device_bytes += (size_t)d.n_centroid * 12 + d.n_ele_ivf * 4 + lut.size() * 4;
+  h->batch_cap = 0;
+  *out = owner.release();
+  return MVR_OK;
+}
+
+int check_index_args(uint32_t n_item, uint32_t n_centroid, uint32_t dim, uint64_t n_vec,
+                     uint32_t n_bit) {
+  if (dim != (uint32_t)kDim)
+    return set_err(MVR_ERR_UNSUPPORTED, "vector dimension %u is not supported (only %d)", dim, kDim);
+  if (n_bit != 1 && n_bit != 2 && n_bit != 4 && n_bit != 8)
+    return set_err(MVR_ERR_INVALID_ARG, "n_bit must be 1, 2, 4 or 8, got %u", n_bit);
+  if (n_item == 0 || n_centroid == 0 || n_vec == 0)
+    return set_err(MVR_ERR_INVALID_ARG, "empty index (n_item=%u n_centroid=%u n_vec=%llu)", n_item,
+                   n_centroid, (unsigned long long)n_vec);
+  return MVR_OK;
+}
+
+int new_handle(int device, std::unique_ptr<mvr_index> &h) {
+  int n_dev = 0;
+  if (cudaGetDeviceCount(&n_dev) != cudaSuccess || n_dev == 0) {
+    cudaGetLastError();
+    return set_err(MVR_ERR_CUDA, "no CUDA device available");
+  }
+  if (device < 0 || device >= n_dev)
+    return set_err(MVR_ERR_INVALID_ARG, "device %d out of range (have %d)", device, n_dev);
+  h.reset(new mvr_index());
+  h->device = device;
+  CUDA_TRY(cudaSetDevice(device));
+  CUDA_TRY(cudaDeviceGetAttribute(&h->n_sm, cudaDevAttrMultiProcessorCount, device));
+  CUDA_TRY(configure_kernels());
+  CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  return MVR_OK;
+}
+
+template <class T>
+int upload(const T *src, size_t n, T **dst, std::vector<void *> &owner, cudaMemcpyKind kind) {
+  MVR_TRY(dalloc(dst, n, &owner));
+  if (n) CUDA_TRY(cudaMemcpy(*dst, src, n * sizeof(T), kind));
+  return MVR_OK;
+}
+
+int from_arrays_impl(const uint32_t *item_n_vec_l, uint32_t n_item, const float *centroid_l,
+                     uint32_t n_centroid, uint32_t dim, const uint32_t *vq_code_l, uint64_t n_vec,
+                     const uint64_t *ivf_offset_l, const uint32_t *ivf_size_l, const uint32_t *ivf,
+                     uint64_t n_ele_ivf, const float *weight_l, uint32_t n_bit,
+                     const uint8_t *residual_code_l, int device, mvr_index **out, bool on_device) {
+  if (!out) return set_err(MVR_ERR_INVALID_ARG, "null output handle");
+  *out = nullptr;
+  MVR_TRY(check_index_args(n_item, n_centroid, dim, n_vec, n_bit));
+  if (!item_n_vec_l || !centroid_l || !vq_code_l || !ivf_offset_l || !ivf_size_l || !weight_l ||
+      !residual_code_l || (n_ele_ivf && !ivf))
+    return set_err(MVR_ERR_INVALID_ARG, "null index array");
+  DeviceGuard g(device);
+  std::unique_ptr<mvr_index> h;
+  MVR_TRY(new_handle(device, h));
+  const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+
+  // host copies of the small arrays the host logic needs
+  std::vector<uint32_t> inv(n_item), isz(n_centroid);
+  std::vector<uint64_t> ioff(n_centroid);
+  CUDA_TRY(cudaMemcpy(inv.data(), item_n_vec_l, n_item * 4ull, on_device ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost));
+  CUDA_TRY(cudaMemcpy(isz.data(), ivf_size_l, n_centroid * 4ull, on_device ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost));
+  CUDA_TRY(cudaMemcpy(ioff.data(), ivf_offset_l, n_centroid * 8ull, on_device ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost));
+  std::vector<float> weight(1u << n_bit);
+  CUDA_TRY(cudaMemcpy(weight.data(), weight_l, weight.size() * 4, on_device ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost));
+  uint64_t tot = 0;
+  std::vector<uint64_t> item_off(n_item);
+  for (uint32_t i = 0; i < n_item; i++) { item_off[i] = tot; tot += inv[i]; }
+  if (tot != n_vec)
+    return set_err(MVR_ERR_INVALID_ARG, "sum of item_n_vec (%llu) != n_vec (%llu)",
+                   (unsigned long long)tot, (unsigned long long)n_vec);
+  for (uint32_t c = 0; c < n_centroid; c++)
+    if (ioff[c] + isz[c] > n_ele_ivf)
+      return set_err(MVR_ERR_INVALID_ARG, "ivf list %u exceeds n_ele_ivf", c);
+
+  DevIndex &d = h->dix;
+  d.n_item = n_item;
+  d.n_centroid = n_centroid;
+  d.n_centroid_pad = (n_centroid + 127u) / 128u * 128u;
+  d.n_bit = n_bit;
+  d.bytes_per_vec = kDim * n_bit / 8;
+  d.n_vec = n_vec;
+  d.n_ele_ivf = n_ele_ivf;
+  float *cen;
+  uint32_t *code, *dinv, *dsz, *dids;
+  uint8_t *res;
+  uint64_t *doff, *dioff;
+  MVR_TRY(upload(centroid_l, (size_t)n_centroid * kDim, &cen, h->bufs, kind));
+  MVR_TRY(upload(vq_code_l, (size_t)n_vec, &code, h->bufs, kind));
+  MVR_TRY(upload(residual_code_l, (size_t)n_vec * d.bytes_per_vec, &res, h->bufs, kind));
+  MVR_TRY(upload(inv.data(), n_item, &dinv, h->bufs, cudaMemcpyHostToDevice));
+  MVR_TRY(upload(item_off.data(), n_item, &doff, h->bufs, cudaMemcpyHostToDevice));
+  MVR_TRY(upload(ioff.data(), n_centroid, &dioff, h->bufs, cudaMemcpyHostToDevice));
+  MVR_TRY(upload(isz.data(), n_centroid, &dsz, h->bufs, cudaMemcpyHostToDevice));
+  MVR_TRY(upload(ivf, (size_t)n_ele_ivf, &dids, h->bufs, kind));
+  d.centroid = cen;
+  d.vq_code = code;
+  d.residual = res;
+  d.item_n_vec = dinv;
+  d.item_off = doff;
+  d.ivf_off = dioff;
+  d.ivf_size = dsz;
+  d.ivf_ids = dids;
+  return finish_index(h.get(), inv.data(), isz.data(), weight.data(), h, out);
+}
+
+bool npy_u32(const NpyArray &a, std::vector<uint32_t> &out) {
+  const uint64_t n = a.numel();
+  out.resize(n);
+  const std::string t = a.descr.substr(1);
+  if (t == "u4" || t == "i4") {
+    std::memcpy(out.data(), a.data.data(), n * 4);
+  } else if (t == "u8" || t == "i8") {
+    const int64_t *p = reinterpret_cast<const int64_t *>(a.data.data());
+    for (uint64_t i = 0; i < n; i++) out[i] = (uint32_t)p[i];
+  } else {
+    return false;
+  }
+  return true;
+}
+
+}  // namespace
+
+// ----------------------------------------------------------------------
+// C ABI
+// ----------------------------------------------------------------------
+extern "C" {
+
+const char *mvr_last_error(void) { return g_err.c_str(); }
+
+int mvr_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+int mvr_index_from_arrays(const uint32_t *item_n_vec_l, uint32_t n_item, const float *centroid_l,
+                          uint32_t n_centroid, uint32_t dim, const uint32_t *vq_code_l,
+                          uint64_t n_vec, const uint64_t *ivf_offset_l, const uint32_t *ivf_size_l,
+                          const uint32_t *ivf, uint64_t n_ele_ivf, const float *weight_l,
+                          uint32_t n_bit, const uint8_t *residual_code_l, int device,
+                          mvr_index **out) {
+  return from_arrays_impl(item_n_vec_l, n_item, centroid_l, n_centroid, dim, vq_code_l, n_vec,
+                          ivf_offset_l, ivf_size_l, ivf, n_ele_ivf, weight_l, n_bit,
+                          residual_code_l, device, out, false);
+}
+
+int mvr_index_from_device_arrays(const uint32_t *item_n_vec_l, uint32_t n_item,
+                                 const float *centroid_l, uint32_t n_centroid, uint32_t dim,
+                                 const uint32_t *vq_code_l, uint64_t n_vec,
+                                 const uint64_t *ivf_offset_l, const uint32_t *ivf_size_l,
+                                 const uint32_t *ivf, uint64_t n_ele_ivf, const float *weight_l,
+                                 uint32_t n_bit, const uint8_t *residual_code_l, int device,
+                                 mvr_index **out) {
+  return from_arrays_impl(item_n_vec_l, n_item, centroid_l, n_centroid, dim, vq_code_l, n_vec,
+                          ivf_offset_l, ivf_size_l, ivf, n_ele_ivf, weight_l, n_bit,
+                          residual_code_l, device, out, true);
+}
+
+int mvr_index_load(const char *index_dir, uint32_t n_centroid, uint32_t n_bit, int device,
+                   mvr_index **out) {
+  if (!index_dir || !out) return set_err(MVR_ERR_INVALID_ARG, "null argument");
+  const std::string dir(index_dir);
+  return mvr_index_load_files((dir + "/item_n_vec_l.npy").c_str(), (dir + "/centroid_l.npy").c_str(),
+                              (dir + "/vq_code_l.npy").c_str(), (dir + "/ivf.index").c_str(),
+                              (dir + "/weight_l.npy").c_str(), (dir + "/residual_code_l.npy").c_str(),
+                              n_centroid, n_bit, device, out);
+}
+
+int mvr_index_load_files(const char *item_n_vec_l_fname, const char *centroid_l_fname,
+                         const char *vq_code_l_fname, const char *ivf_index_fname,
+                         const char *weight_l_fname, const char *residual_code_l_fname,
+                         uint32_t n_centroid, uint32_t n_bit, int device, mvr_index **out) {
+  if (!item_n_vec_l_fname || !centroid_l_fname || !vq_code_l_fname || !ivf_index_fname ||
+      !weight_l_fname || !residual_code_l_fname || !out)
+    return set_err(MVR_ERR_INVALID_ARG, "null argument");
+  std::string err;
+  NpyArray a_inv, a_cen, a_code, a_w, a_res;
+  if (!npy_load(item_n_vec_l_fname, a_inv, err) || !npy_load(centroid_l_fname, a_cen, err) ||
+      !npy_load(vq_code_l_fname, a_code, err) || !npy_load(weight_l_fname, a_w, err) ||
+      !npy_load(residual_code_l_fname, a_res, err))
+    return set_err(MVR_ERR_IO, "%s", err.c_str());
+  IvfCsr ivf;
+  if (!ivf_load(ivf_index_fname, ivf, err)) return set_err(MVR_ERR_IO, "%s", err.c_str());
+  std::vector<uint32_t> inv, code;
+  if (a_inv.shape.size() != 1 || !npy_u32(a_inv, inv))
+    return set_err(MVR_ERR_IO, "item_n_vec_l.npy: expected 1-D integer array (%s)", a_inv.descr.c_str());
+  if (a_code.shape.size() != 1 || !npy_u32(a_code, code))
+    return set_err(MVR_ERR_IO, "vq_code_l.npy: expected 1-D integer array (%s)", a_code.descr.c_str());
+  if (a_cen.shape.size() != 2 || a_cen.descr.substr(1) != "f4")
+    return set_err(MVR_ERR_IO, "centroid_l.npy: expected 2-D float32 array");
+  if (a_w.shape.size() != 1 || a_w.descr.substr(1) != "f4")
+    return set_err(MVR_ERR_IO, "weight_l.npy: expected 1-D float32 array");
+  if (a_res.descr.substr(1) != "u1")
+    return set_err(MVR_ERR_IO, "residual_code_l.npy: expected uint8 array");
+  const uint32_t C = (uint32_t)a_cen.shape[0], dim = (uint32_t)a_cen.shape[1];
+  if (C != n_centroid)
+    return set_err(MVR_ERR_INVALID_ARG, "centroid_l.npy has %u centroids, expected %u", C, n_centroid);
+  if (ivf.n_centroid != n_centroid)
+    return set_err(MVR_ERR_IO, "ivf.index has %u lists, expected %u", ivf.n_centroid, n_centroid);
+  if (a_w.shape[0] != (1ull << n_bit))
+    return set_err(MVR_ERR_INVALID_ARG, "weight_l.npy has %llu weights, n_bit=%u needs %u",
+                   (unsigned long long)a_w.shape[0], n_bit, 1u << n_bit);
+  MVR_TRY(check_index_args((uint32_t)inv.size(), C, dim, code.size(), n_bit));
+  const uint64_t bpv = (uint64_t)dim * n_bit / 8;
+  if (a_res.numel() != code.size() * bpv)
+    return set_err(MVR_ERR_IO, "residual_code_l.npy has %llu bytes, expected %llu",
+                   (unsigned long long)a_res.numel(), (unsigned long long)(code.size() * bpv));
+  return mvr_index_from_arrays(inv.data(), (uint32_t)inv.size(),
+                               reinterpret_cast<const float *>(a_cen.data.data()), C, dim,
+                               code.data(), code.size(), ivf.offset.data(), ivf.size.data(),
+                               ivf.ids.data(), ivf.n_ele,
+                               reinterpret_cast<const float *>(a_w.data.data()), n_bit,
+                               a_res.data.data(), device, out);
+}
+
+int mvr_index_free(mvr_index *h) {
+  delete h;
+  return MVR_OK;
+}
+
+int mvr_index_get_info(const mvr_index *h, mvr_index_info *info) {
+  if (!h || !info) return set_err(MVR_ERR_INVALID_ARG, "null argument");
+  info->n_item = h->dix.n_item;
+  info->n_centroid = h->dix.n_centroid;
+  info->dim = kDim;
+  info->n_bit = h->dix.n_bit;
+  info->n_vec = h->dix.n_vec;
+  info->n_ele_ivf = h->dix.n_ele_ivf;
+  info->max_item_n_vec = h->dix.max_item_n_vec;
+  info->max_ivf_list = h->max_ivf_list;
+  info->device_bytes = h->device_bytes;
+  info->device = h->device;
+  return MVR_OK;
+}
+
+int mvr_index_set_batch(mvr_index *h, uint32_t max_batch_queries) {
+  if (!h) return set_err(MVR_ERR_INVALID_ARG, "null index handle");
+  h->batch_cap = max_batch_queries;
+  return MVR_OK;
+}
+
+int mvr_search(mvr_index *h, const float *query_l, const uint64_t *tok_off, uint32_t n_query,
+               uint32_t query_n_vec, uint32_t topk, uint32_t nprobe, uint32_t probe_topk,
+               uint32_t flags, float *result_score_l, uint32_t *result_id_l, double *query_time_s,
+               mvr_stats *stats) {
+  if (!h) return set_err(MVR_ERR_INVALID_ARG, "null index handle");
+  return search_impl(h, query_l, tok_off, n_query, query_n_vec, topk, nprobe, probe_topk, flags,
+                     result_score_l, result_id_l, query_time_s, nullptr, stats, h->stream, true);
+}
+
+int mvr_search_staged(mvr_index *h, const float *query_l, const uint64_t *tok_off,
+                      uint32_t n_query, uint32_t query_n_vec, uint32_t topk, uint32_t nprobe,
+                      uint32_t probe_topk, uint32_t flags, float *result_score_l,
+                      uint32_t *result_id_l, double *query_time_s, double *stage_time_s,
+                      mvr_stats *stats) {
+  if (!h) return set_err(MVR_ERR_INVALID_ARG, "null index handle");
+  return search_impl(h, query_l, tok_off, n_query, query_n_vec, topk, nprobe, probe_topk, flags,
+                     result_score_l, result_id_l, query_time_s, stage_time_s, stats, h->stream,
+                     true);
+}
+
+int mvr_search_device(mvr_index *h, const float *d_query_l, const uint64_t *tok_off,
+                      uint32_t n_query, uint32_t query_n_vec, uint32_t topk, uint32_t nprobe,
+                      uint32_t probe_topk, uint32_t flags, float *d_result_score_l,
+                      uint32_t *d_result_id_l, void *cuda_stream, mvr_stats *stats) {
+  if (!h) return set_err(MVR_ERR_INVALID_ARG, "null index handle");
+  cudaStream_t st = cuda_stream ? (cudaStream_t)cuda_stream : (cudaStream_t)0;
+  return search_impl(h, d_query_l, tok_off, n_query, query_n_vec, topk, nprobe, probe_topk, flags,
+                     d_result_score_l, d_result_id_l, nullptr, nullptr, stats, st, false);
+}
+
+int mvr_search_trace(mvr_index *h, const float *query, uint32_t nq, uint32_t topk,
+                     uint32_t nprobe, uint32_t probe_topk, uint32_t flags, mvr_trace *tr) {
+  if (!h || !query || !tr) return set_err(MVR_ERR_INVALID_ARG, "null argument");
+  if (!tr->topk_score || !tr->topk_id) return set_err(MVR_ERR_INVALID_ARG, "null trace result buffer");
+  MVR_TRY(search_impl(h, query, nullptr, 1, nq, topk, nprobe, probe_topk, flags, tr->topk_score,
+                      tr->topk_id, nullptr, nullptr, nullptr, h->stream, true));
+  DeviceGuard g(h->device);
+  Workspace &w = h->ws;
+  if (tr->probe_id)
+    CUDA_TRY(cudaMemcpy(tr->probe_id, w.probe_id, (size_t)nq * nprobe * 4, cudaMemcpyDeviceToHost));
+  if (tr->probe_score)
+    CUDA_TRY(cudaMemcpy(tr->probe_score, w.probe_s, (size_t)nq * nprobe * 4, cudaMemcpyDeviceToHost));
+  uint32_t n_short = 0;
+  CUDA_TRY(cudaMemcpy(&n_short, w.n_short, 4, cudaMemcpyDeviceToHost));
+  const uint32_t n_cand = w.h_qstat[0];
+  tr->n_cand = n_cand;
+  tr->n_short = n_short;
+  if (tr->cand_id || tr->cand_score) {
+    std::vector<uint64_t> keys(n_cand);
+    if (n_cand) CUDA_TRY(cudaMemcpy(keys.data(), w.key, (size_t)n_cand * 8, cudaMemcpyDeviceToHost));
+    std::sort(keys.begin(), keys.end(),
+              [](uint64_t a, uint64_t b) { return key_id(a) < key_id(b); });
+    for (uint32_t i = 0; i < n_cand && i < tr->cand_cap; i++) {
+      if (tr->cand_id) tr->cand_id[i] = key_id(keys[i]);
+      if (tr->cand_score) tr->cand_score[i] = key_score(keys[i]);
+    }
+  }
+  std::vector<uint32_t> sid(n_short);
+  std::vector<float> sa(n_short), se(n_short);
+  if (n_short) {
+    CUDA_TRY(cudaMemcpy(sid.data(), w.short_id, n_short * 4ull, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(sa.data(), w.short_approx, n_short * 4ull, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(se.data(), w.exact, n_short * 4ull, cudaMemcpyDeviceToHost));
+  }
+  std::vector<uint32_t> ord(n_short);
+  for (uint32_t i = 0; i < n_short; i++) ord[i] = i;
+  std::sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) { return sid[a] < sid[b]; });
+  for (uint32_t i = 0; i < n_short; i++) {
+    if (tr->short_id) tr->short_id[i] = sid[ord[i]];
+    if (tr->short_approx) tr->short_approx[i] = sa[ord[i]];
+    if (tr->short_exact) tr->short_exact[i] = se[ord[i]];
+  }
+  return MVR_OK;
+}
+
+static int gather_vec_ids(mvr_index *h, const uint64_t *vec_id, uint64_t n, uint64_t **d_ids) {
+  for (uint64_t i = 0; i < n; i++)
+    if (vec_id[i] >= h->dix.n_vec)
+      return set_err(MVR_ERR_INVALID_ARG, "token id %llu >= n_vec %llu",
+                     (unsigned long long)vec_id[i], (unsigned long long)h->dix.n_vec);
+  MVR_TRY(dalloc(d_ids, n));
+  CUDA_TRY(cudaMemcpy(*d_ids, vec_id, n * 8, cudaMemcpyHostToDevice));
+  return MVR_OK;
+}
+
+int mvr_decompress(mvr_index *h, const uint64_t *vec_id, uint64_t n, float *out) {
+  if (!h || (n && (!vec_id || !out))) return set_err(MVR_ERR_INVALID_ARG, "null argument");
+  if (n == 0) return MVR_OK;
+  DeviceGuard g(h->device);
+  uint64_t *ids;
+  MVR_TRY(gather_vec_ids(h, vec_id, n, &ids));
+  std::unique_ptr<void, void (*)(void *)> ig(ids, dfree);
+  float *d_out;
+  MVR_TRY(dalloc(&d_out, n * kDim));
+  std::unique_ptr<void, void (*)(void *)> og(d_out, dfree);
+  CUDA_TRY(launch_decompress(h->dix, ids, n, d_out, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  CUDA_TRY(cudaMemcpy(out, d_out, n * kDim * sizeof(float), cudaMemcpyDeviceToHost));
+  return MVR_OK;
+}
+
+int mvr_unpack_buckets(mvr_index *h, const uint64_t *vec_id, uint64_t n, uint8_t *out) {
+  if (!h || (n && (!vec_id || !out))) return set_err(MVR_ERR_INVALID_ARG, "null argument");
+  if (n == 0) return MVR_OK;
+  DeviceGuard g(h->device);
+  uint64_t *ids;
+  MVR_TRY(gather_vec_ids(h, vec_id, n, &ids));
+  std::unique_ptr<void, void (*)(void *)> ig(ids, dfree);
+  uint8_t *d_out;
+  MVR_TRY(dalloc(&d_out, n * kDim));
+  std::unique_ptr<void, void (*)(void *)> og(d_out, dfree);
+  CUDA_TRY(launch_unpack(h->dix, ids, n, d_out, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  CUDA_TRY(cudaMemcpy(out, d_out, n * kDim, cudaMemcpyDeviceToHost));
+  return MVR_OK;
+}
+
+int mvr_assign_device(const float *d_vec, uint64_t n_vec, const float *d_centroid,
+                      uint32_t n_centroid, uint32_t dim, uint32_t *d_code, float *d_score,
+                      void *cuda_stream) {
+  if (dim != (uint32_t)kDim) return set_err(MVR_ERR_UNSUPPORTED, "dim %u not supported", dim);
+  if (!d_vec || !d_centroid || !d_code || n_centroid == 0)
+    return set_err(MVR_ERR_INVALID_ARG, "null argument or no centroids");
+  if (mvr_device_count() == 0) return set_err(MVR_ERR_CUDA, "no CUDA device available");
+  cudaStream_t st = (cudaStream_t)cuda_stream;
+  CUDA_TRY(configure_kernels());
+  DevIndex d{};
+  d.n_centroid = n_centroid;
+  d.n_centroid_pad = (n_centroid + 127u) / 128u * 128u;
+  float *ct;
+  MVR_TRY(dalloc(&ct, (size_t)kDim * d.n_centroid_pad));
+  std::unique_ptr<void, void (*)(void *)> cg(ct, dfree);
+  CUDA_TRY(launch_transpose_centroid(d_centroid, n_centroid, d.n_centroid_pad, ct, st));
+  d.centroid_t = ct;
+  float *score = d_score;
+  std::unique_ptr<void, void (*)(void *)> sg(nullptr, dfree);
+  if (!score) {
+    const uint64_t chunk_max = std::min<uint64_t>(n_vec, 2ull << 20);
+    MVR_TRY(dalloc(&score, chunk_max));
+    sg.reset(score);
+  }
+  int launches = 0;
+  for (uint64_t s = 0; s < n_vec; s += (2ull << 20)) {  // grid.y <= 32768
+    const uint32_t T = (uint32_t)std::min<uint64_t>(2ull << 20, n_vec - s);
+    CUDA_TRY(launch_probe(d, d_vec + s * kDim, T, 1, 1, nullptr, nullptr, d_code + s,
+                          d_score ? d_score + s : score, st, &launches));
+  }
+  CUDA_TRY(cudaStreamSynchronize(st));
+  return MVR_OK;
+}
+
+int mvr_pack_residual_device(const float *d_vec, uint64_t n_vec, const float *d_centroid,
+                             uint32_t dim, const uint32_t *d_code, const float *cutoff_l,
+                             uint32_t n_bit, uint8_t *d_out, void *cuda_stream) {
+  if (dim != (uint32_t)kDim) return set_err(MVR_ERR_UNSUPPORTED, "dim %u not supported", dim);
+  if (n_bit != 1 && n_bit != 2 && n_bit != 4 && n_bit != 8)
+    return set_err(MVR_ERR_INVALID_ARG, "n_bit must be 1, 2, 4 or 8");
+  if (!d_vec || !d_centroid || !d_code || !cutoff_l || !d_out)
+    return set_err(MVR_ERR_INVALID_ARG, "null argument");
+  Cutoffs cut{};
+  for (uint32_t i = 0; i + 1 < (1u << n_bit); i++) cut.v[i] = cutoff_l[i];
+  cudaStream_t st = (cudaStream_t)cuda_stream;
+  CUDA_TRY(launch_pack_residual(d_vec, n_vec, d_centroid, d_code, cut, n_bit, d_out, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  return MVR_OK;
+}
+
+int mvr_kmeans_accumulate_device(const float *d_vec, uint64_t n_vec, uint32_t dim,
+                                 const uint32_t *d_code, double *d_sum, uint64_t *d_count,
+                                 void *cuda_stream) {
+  if (dim != (uint32_t)kDim) return set_err(MVR_ERR_UNSUPPORTED, "dim %u not supported", dim);
+  if (!d_vec || !d_code || !d_sum || !d_count) return set_err(MVR_ERR_INVALID_ARG, "null argument");
+  cudaStream_t st = (cudaStream_t)cuda_stream;
+  CUDA_TRY(launch_kmeans_accumulate(d_vec, n_vec, d_code, d_sum, d_count, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  return MVR_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,682 @@
+// mvr_kernels.cu -- the plain FP32 search kernels of libmvr (sm_100a).
+//
+// Stage map (reference -> kernel):
+//   centroid scoring S = Q.C^T + 1 and per-token top-nprobe
+//       (GenerateVQScoreCandidatePP.hpp:118-179: cuBLAS SGEMM, thrust +1,
+//        RAFT select_k)                       -> probe_topk_kernel (+ merge)
+//   IVF gather, candidate flag/compaction, max-over-probes, sum over tokens,
+//   top-probe_topk shortlist (FilterPP.hpp:19-142, 267-398)
+//                                             -> filter_kernel
+//   VQ/residual gather, decompress, SGEMM, max over doc tokens, sum over
+//   query tokens (RerankPP.hpp:16-161, 368-475) -> rerank_kernel
+//   host std::sort of the shortlist (IGPGPURetrievalPP.hpp:153-161)
+//                                             -> topk_kernel
+//
+// Every dot product is a sequential __fmaf_rn chain over d = 0..127 from
+// 0.0f, every other add is a single rounded FP32 add and every sum runs in a
+// fixed order, so results are bit-identical to the CPU oracle's canonical
+// arithmetic and independent of launch shape.
+#include "mvr_common.cuh"
+#include "mvr_kernels.cuh"
+
+#include <cfloat>
+
+namespace mvr {
+
+// ---------------------------------------------------------------------
+// small helpers
+// ---------------------------------------------------------------------
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::);
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+constexpr unsigned kFull = 0xffffffffu;
+
+// Insert (s, id) into the sorted per-warp list held one entry per lane
+// (lanes < np).  thr is the list's worst entry, uniform across the warp.
+__device__ __forceinline__ void warp_list_insert(float &ls, uint32_t &lid,
+                                                 float &thr_s, uint32_t &thr_id,
+                                                 float ns, uint32_t nid,
+                                                 int lane, int np) {
+  const bool ahead = lane < np && better(ls, lid, ns, nid);
+  const int pos = __popc(__ballot_sync(kFull, ahead));
+  const float up_s = __shfl_up_sync(kFull, ls, 1);
+  const uint32_t up_id = __shfl_up_sync(kFull, lid, 1);
+  if (lane > pos) {
+    ls = up_s;
+    lid = up_id;
+  } else if (lane == pos) {
+    ls = ns;
+    lid = nid;
+  }
+  thr_s = __shfl_sync(kFull, ls, np - 1);
+  thr_id = __shfl_sync(kFull, lid, np - 1);
+}
+
+// ---------------------------------------------------------------------
+// K1: S = Q.C^T + 1 over a centroid range, running top-nprobe per token.
+// CTA = 64 tokens x (tiles_per_split * 128) centroids, 256 threads.
+// Thread (warp w, lane l): tokens w*8..w*8+7, centroids l*4..l*4+3 of the
+// current 128-wide tile.  Qs[k][64] and double-buffered Cs[k][128] in smem.
+// ---------------------------------------------------------------------
+constexpr int kProbeTokTile = 64;
+constexpr int kProbeCenTile = 128;
+constexpr size_t kProbeSmem =
+    (size_t)(kDim * kProbeTokTile + 2 * kDim * kProbeCenTile) * sizeof(float);
+
+__global__ void __launch_bounds__(256, 1)
+probe_topk_kernel(const float *__restrict__ q, uint32_t n_tok,
+                  const float *__restrict__ ct, uint32_t n_cent,
+                  uint32_t n_cent_pad, uint32_t nprobe,
+                  uint32_t tiles_per_split, uint32_t *__restrict__ out_id,
+                  float *__restrict__ out_s) {
+  extern __shared__ __align__(16) float smem[];
+  float *Qs = smem;                          // [128][64]
+  float *Cs = smem + kDim * kProbeTokTile;   // [2][128][128]
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t t0 = blockIdx.y * kProbeTokTile;
+  const uint32_t n_tiles = n_cent_pad / kProbeCenTile;
+  const uint32_t tile_begin = blockIdx.x * tiles_per_split;
+  const uint32_t tile_end = min(n_tiles, tile_begin + tiles_per_split);
+
+  for (int i = tid; i < kProbeTokTile * (kDim / 4); i += 256) {
+    const int t = i % kProbeTokTile, k4 = i / kProbeTokTile;
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (t0 + t < n_tok) v = __ldg(reinterpret_cast<const float4 *>(q + (size_t)(t0 + t) * kDim) + k4);
+    Qs[(k4 * 4 + 0) * kProbeTokTile + t] = v.x;
+    Qs[(k4 * 4 + 1) * kProbeTokTile + t] = v.y;
+    Qs[(k4 * 4 + 2) * kProbeTokTile + t] = v.z;
+    Qs[(k4 * 4 + 3) * kProbeTokTile + t] = v.w;
+  }
+
+  auto load_tile = [&](uint32_t tile, int buf) {
+    float *dst = Cs + buf * kDim * kProbeCenTile;
+    const float *src = ct + (size_t)tile * kProbeCenTile;
+    // 128 rows x 32 chunks of 16 B
+#pragma unroll
+    for (int i = 0; i < (kDim * kProbeCenTile / 4) / 256; i++) {
+      const int ch = tid + i * 256;
+      const int k = ch >> 5, c4 = ch & 31;
+      cp_async16(dst + k * kProbeCenTile + c4 * 4, src + (size_t)k * n_cent_pad + c4 * 4);
+    }
+    cp_async_commit();
+  };
+
+  float Ls[8], thr_s[8];
+  uint32_t Lid[8], thr_id[8];
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    Ls[i] = -INFINITY; Lid[i] = 0xffffffffu;
+    thr_s[i] = -INFINITY; thr_id[i] = 0xffffffffu;
+  }
+  const int np = (int)nprobe;
+
+  if (tile_begin < tile_end) load_tile(tile_begin, 0);
+  for (uint32_t tile = tile_begin; tile < tile_end; tile++) {
+    const int buf = (tile - tile_begin) & 1;
+    if (tile + 1 < tile_end) {
+      load_tile(tile + 1, buf ^ 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+
+    float acc[8][4];
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+#pragma unroll
+      for (int j = 0; j < 4; j++) acc[i][j] = 0.0f;
+    const float *qs = Qs + warp * 8;
+    const float *cs = Cs + buf * kDim * kProbeCenTile + lane * 4;
+#pragma unroll 4
+    for (int k = 0; k < kDim; k++) {
+      const float4 a0 = *reinterpret_cast<const float4 *>(qs + k * kProbeTokTile);
+      const float4 a1 = *reinterpret_cast<const float4 *>(qs + k * kProbeTokTile + 4);
+      const float4 b = *reinterpret_cast<const float4 *>(cs + k * kProbeCenTile);
+      const float a[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+      const float bb[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = __fmaf_rn(a[i], bb[j], acc[i][j]);
+    }
+
+    const uint32_t c0 = tile * kProbeCenTile + lane * 4;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const float s = __fadd_rn(acc[i][j], 1.0f);
+        const uint32_t id = c0 + j;
+        const bool cand = id < n_cent && better(s, id, thr_s[i], thr_id[i]);
+        unsigned m = __ballot_sync(kFull, cand);
+        while (m) {
+          const int src = __ffs(m) - 1;
+          m &= m - 1;
+          const float ns = __shfl_sync(kFull, s, src);
+          const uint32_t nid = __shfl_sync(kFull, id, src);
+          if (better(ns, nid, thr_s[i], thr_id[i]))
+            warp_list_insert(Ls[i], Lid[i], thr_s[i], thr_id[i], ns, nid, lane, np);
+        }
+      }
+    }
+    __syncthreads();
+  }
+
+  const size_t split_off = (size_t)blockIdx.x * n_tok * nprobe;
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    const uint32_t t = t0 + warp * 8 + i;
+    if (t < n_tok && lane < np) {
+      out_id[split_off + (size_t)t * nprobe + lane] = Lid[i];
+      out_s[split_off + (size_t)t * nprobe + lane] = Ls[i];
+    }
+  }
+}
+
+// Merge n_split sorted partial lists per token (one warp per token).
+__global__ void __launch_bounds__(256)
+probe_merge_kernel(const uint32_t *__restrict__ part_id,
+                   const float *__restrict__ part_s, uint32_t n_split,
+                   uint32_t n_tok, uint32_t nprobe, uint32_t *__restrict__ out_id,
+                   float *__restrict__ out_s) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t t = blockIdx.x * 8 + (threadIdx.x >> 5);
+  if (t >= n_tok) return;
+  const int np = (int)nprobe;
+  float ls = -INFINITY, thr_s = -INFINITY;
+  uint32_t lid = 0xffffffffu, thr_id = 0xffffffffu;
+  for (uint32_t sp = 0; sp < n_split; sp++) {
+    const size_t base = ((size_t)sp * n_tok + t) * nprobe;
+    float ps = -INFINITY;
+    uint32_t pid = 0xffffffffu;
+    if (lane < np) { ps = part_s[base + lane]; pid = part_id[base + lane]; }
+    for (int e = 0; e < np; e++) {
+      const float ns = __shfl_sync(kFull, ps, e);
+      const uint32_t nid = __shfl_sync(kFull, pid, e);
+      if (!better(ns, nid, thr_s, thr_id)) break;  // partial lists are sorted
+      warp_list_insert(ls, lid, thr_s, thr_id, ns, nid, lane, np);
+    }
+  }
+  if (lane < np) {
+    out_id[(size_t)t * nprobe + lane] = lid;
+    out_s[(size_t)t * nprobe + lane] = ls;
+  }
+}
+
+// ---------------------------------------------------------------------
+// K2: candidate filter + shortlist, one CTA per query.
+//
+// Phase A visits the probed lists rank by rank (all tokens' j-th probe, then
+// j+1, ...; probes are sorted best-first) so that the first visit of
+// (doc, token) carries the max over probes; the rank j is recorded in a
+// per-slot byte table rank[doc][token] (0xff = unvisited).  A doc enters the
+// candidate set the first time any token visits it (per-slot epoch stamps,
+// no O(n_item) reset).  Phase B sums the per-token maxima in token order and
+// restores the touched rank rows to 0xff.  Phase C/D radix-select the top
+// probe_topk candidates by the 64-bit key (score desc, id asc).
+// ---------------------------------------------------------------------
+constexpr int kFilterThreads = 1024;
+
+__device__ __forceinline__ uint32_t find_seg(const uint32_t *pref, int n, uint32_t e) {
+  // largest i in [0, n) with pref[i] <= e   (pref[0] = 0, non-decreasing)
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (pref[mid] <= e) lo = mid; else hi = mid - 1;
+  }
+  return (uint32_t)lo;
+}
+
+__global__ void __launch_bounds__(kFilterThreads, 1)
+filter_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
+              const float *__restrict__ probe_s, uint32_t nprobe,
+              const uint64_t *__restrict__ q_off, uint32_t probe_topk,
+              FilterScratch scr, uint32_t epoch,
+              uint32_t *__restrict__ short_id, float *__restrict__ short_approx,
+              uint32_t *__restrict__ n_short_out, uint32_t *__restrict__ qstat) {
+  __shared__ float ps[kMaxQueryTok * kMaxProbe];
+  __shared__ uint32_t pid[kMaxQueryTok * kMaxProbe];
+  __shared__ uint32_t pref[kMaxQueryTok + 1];
+  __shared__ uint32_t hist[256];
+  __shared__ uint32_t s_ncand, s_sel, s_digit, s_need, s_done, s_entries, s_stok;
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int n_warp = blockDim.x >> 5;
+  const uint32_t b = blockIdx.x;
+  const uint64_t tok0 = q_off[b];
+  const uint32_t nq = (uint32_t)(q_off[b + 1] - tok0);
+  uint32_t *stamp = scr.stamp + (size_t)b * scr.n_item;
+  uint8_t *rank = scr.rank + (size_t)b * scr.n_item * scr.rank_stride;
+  uint64_t *key = scr.key + (size_t)b * scr.n_item;
+
+  for (uint32_t i = tid; i < nq * nprobe; i += blockDim.x) {
+    pid[i] = probe_id[tok0 * nprobe + i];
+    ps[i] = probe_s[tok0 * nprobe + i];
+  }
+  if (tid == 0) { s_ncand = 0; s_entries = 0; s_stok = 0; }
+  __syncthreads();
+
+  // ---- phase A: scatter probed lists rank by rank ----
+  for (uint32_t j = 0; j < nprobe; j++) {
+    if (tid == 0) {
+      uint32_t acc = 0;
+      for (uint32_t t = 0; t < nq; t++) {
+        pref[t] = acc;
+        const uint32_t c = pid[t * nprobe + j];  // 0xffffffff if no finite score
+        acc += c < ix.n_centroid ? ix.ivf_size[c] : 0u;
+      }
+      pref[nq] = acc;
+      s_entries += acc;
+    }
+    __syncthreads();
+    const uint32_t total = pref[nq];
+    for (uint32_t e0 = warp * 32; e0 < total; e0 += n_warp * 32) {
+      const uint32_t e = e0 + lane;
+      if (e < total) {
+        const uint32_t t = find_seg(pref, (int)nq, e);
+        const uint32_t c = pid[t * nprobe + j];
+        const uint32_t item = ix.ivf_ids[ix.ivf_off[c] + (e - pref[t])];
+        uint8_t *r = rank + (size_t)item * scr.rank_stride + t;
+        if (*r == 0xff) {
+          *r = (uint8_t)j;
+          if (atomicExch(stamp + item, epoch) != epoch) {
+            const uint32_t pos = atomicAdd(&s_ncand, 1u);
+            key[pos] = item;
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  const uint32_t n_cand = s_ncand;
+
+  // ---- phase B: approximate score, restore rank rows ----
+  for (uint32_t i = tid; i < n_cand; i += blockDim.x) {
+    const uint32_t item = (uint32_t)key[i];
+    uint8_t *row = rank + (size_t)item * scr.rank_stride;
+    float s = 0.0f;
+    for (uint32_t t0 = 0; t0 < nq; t0 += 16) {
+      uint4 w = *reinterpret_cast<uint4 *>(row + t0);
+      const uint8_t *bytes = reinterpret_cast<const uint8_t *>(&w);
+#pragma unroll
+      for (int u = 0; u < 16; u++) {
+        const uint32_t t = t0 + u;
+        if (t < nq && bytes[u] != 0xff) s = __fadd_rn(s, ps[t * nprobe + bytes[u]]);
+      }
+      *reinterpret_cast<uint4 *>(row + t0) = make_uint4(~0u, ~0u, ~0u, ~0u);
+    }
+    key[i] = make_key(s, item);
+  }
+  __syncthreads();
+
+  // ---- phase C: radix select of the probe_topk largest keys ----
+  uint64_t prefix = 0, mask = 0;
+  if (n_cand > probe_topk) {
+    if (tid == 0) { s_need = probe_topk; s_done = 0; }
+    for (int pass = 0; pass < 8; pass++) {
+      const int shift = 56 - 8 * pass;
+      for (int i = tid; i < 256; i += blockDim.x) hist[i] = 0;
+      __syncthreads();
+      for (uint32_t i0 = 0; i0 < n_cand; i0 += blockDim.x) {
+        const uint32_t i = i0 + tid;
+        uint32_t dig = 256;
+        if (i < n_cand) {
+          const uint64_t k = key[i];
+          if ((k & mask) == prefix) dig = (uint32_t)(k >> shift) & 0xffu;
+        }
+        const unsigned grp = __match_any_sync(kFull, dig);
+        if (dig < 256 && lane == __ffs(grp) - 1) atomicAdd(&hist[dig], (uint32_t)__popc(grp));
+      }
+      __syncthreads();
+      if (warp == 0) {
+        // lane l owns bins 255-8l .. 248-8l (high to low)
+        uint32_t cnt[8], sum = 0;
+#pragma unroll
+        for (int u = 0; u < 8; u++) { cnt[u] = hist[255 - 8 * lane - u]; sum += cnt[u]; }
+        uint32_t incl = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t v = __shfl_up_sync(kFull, incl, o);
+          if (lane >= o) incl += v;
+        }
+        const uint32_t excl = incl - sum;
+        const uint32_t need = s_need;
+        if (excl < need && need <= incl) {
+          uint32_t above = excl;
+#pragma unroll
+          for (int u = 0; u < 8; u++) {
+            if (above < need && need <= above + cnt[u]) {
+              s_digit = 255 - 8 * lane - u;
+              s_need = need - above;
+              s_done = (need - above == cnt[u]) ? 1u : 0u;
+            }
+            above += cnt[u];
+          }
+        }
+      }
+      __syncthreads();
+      prefix |= (uint64_t)s_digit << shift;
+      mask |= (uint64_t)0xff << shift;
+      const uint32_t done = s_done;
+      __syncthreads();
+      if (done) break;
+    }
+  }
+
+  // ---- phase D: emit the shortlist (unordered) ----
+  if (tid == 0) s_sel = 0;
+  __syncthreads();
+  for (uint32_t i = tid; i < n_cand; i += blockDim.x) {
+    const uint64_t k = key[i];
+    if ((k & mask) >= prefix) {
+      const uint32_t pos = atomicAdd(&s_sel, 1u);
+      if (pos < probe_topk) {
+        short_id[(size_t)b * probe_topk + pos] = key_id(k);
+        short_approx[(size_t)b * probe_topk + pos] = key_score(k);
+        atomicAdd(&s_stok, ix.item_n_vec[key_id(k)]);
+      }
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    n_short_out[b] = min(s_sel, probe_topk);
+    qstat[b * 3 + 0] = n_cand;
+    qstat[b * 3 + 1] = s_entries;
+    qstat[b * 3 + 2] = s_stok;
+  }
+}
+
+// ---------------------------------------------------------------------
+// K3: decompress + exact MaxSim for CH shortlisted docs of one query.
+// 256 threads; 128 doc tokens per tile decompressed into Xs[k][128] (FP32);
+// thread (warp w, lane l): query tokens (w&3)*8..+8 of the current 32-token
+// block, doc tokens (w>>2)*64 + 2l, +1.  Per-(token, doc) maxima go through
+// warp match/reduce into shared best[q][doc]; max is order-free and the final
+// sum over query tokens runs in token order.
+// ---------------------------------------------------------------------
+constexpr int kRerankDocs = 16;
+constexpr int kRerankTile = 128;
+
+template <int NBIT>
+__global__ void __launch_bounds__(256)
+rerank_kernel(DevIndex ix, const float *__restrict__ q,
+              const uint64_t *__restrict__ q_off,
+              const uint32_t *__restrict__ short_id,
+              const uint32_t *__restrict__ n_short, uint32_t probe_topk,
+              int semantics, float *__restrict__ exact) {
+  constexpr int VPB = 8 / NBIT;
+  constexpr int HALF_BYTES = 64 / VPB;  // residual bytes for 64 dims
+  extern __shared__ __align__(16) float smem[];
+  float *Xs = smem;                            // [128][128]
+  float *Qs = Xs + kDim * kRerankTile;         // [128][64]
+  float *lut = Qs + kDim * kMaxQueryTok;       // [256][VPB]
+  int *best = reinterpret_cast<int *>(lut + 256 * VPB);  // [64][CH]
+  __shared__ uint32_t d_item[kRerankDocs], d_len[kRerankDocs], d_pref[kRerankDocs + 1];
+  __shared__ uint64_t d_off[kRerankDocs];
+  __shared__ int tok_doc[kRerankTile];
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t b = blockIdx.y;
+  const uint32_t ns = n_short[b];
+  const uint32_t d0 = blockIdx.x * kRerankDocs;
+  if (d0 >= ns) return;
+  const uint32_t nd = min((uint32_t)kRerankDocs, ns - d0);
+  const uint64_t tok0 = q_off[b];
+  const uint32_t nq = (uint32_t)(q_off[b + 1] - tok0);
+
+  if (tid < (int)nd) {
+    const uint32_t it = short_id[(size_t)b * probe_topk + d0 + tid];
+    d_item[tid] = it;
+    d_len[tid] = ix.item_n_vec[it];
+    d_off[tid] = ix.item_off[it];
+  }
+  for (int i = tid; i < 256 * VPB; i += 256) lut[i] = ix.lut[i];
+  for (int i = tid; i < kMaxQueryTok * kRerankDocs; i += 256) best[i] = f2si(-INFINITY);
+  for (int i = tid; i < kMaxQueryTok * (kDim / 4); i += 256) {
+    const int t = i % kMaxQueryTok, k4 = i / kMaxQueryTok;
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if ((uint32_t)t < nq) v = __ldg(reinterpret_cast<const float4 *>(q + (tok0 + t) * kDim) + k4);
+    Qs[(k4 * 4 + 0) * kMaxQueryTok + t] = v.x;
+    Qs[(k4 * 4 + 1) * kMaxQueryTok + t] = v.y;
+    Qs[(k4 * 4 + 2) * kMaxQueryTok + t] = v.z;
+    Qs[(k4 * 4 + 3) * kMaxQueryTok + t] = v.w;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    uint32_t acc = 0;
+    for (uint32_t i = 0; i < nd; i++) { d_pref[i] = acc; acc += d_len[i]; }
+    d_pref[nd] = acc;
+  }
+  __syncthreads();
+  const uint32_t n_tok = d_pref[nd];
+
+  for (uint32_t p0 = 0; p0 < n_tok; p0 += kRerankTile) {
+    // -- decompress 128 tokens: thread = (token tid&127, half tid>>7) --
+    {
+      const int t = tid & (kRerankTile - 1), half = tid >> 7;
+      const uint32_t s = p0 + t;
+      float *xcol = Xs + (half * 64) * kRerankTile + t;
+      if (s < n_tok) {
+        const uint32_t di = find_seg(d_pref, (int)nd, s);
+        const uint64_t v = d_off[di] + (s - d_pref[di]);
+        if (half == 0) tok_doc[t] = (int)di;
+        const float4 *cen = reinterpret_cast<const float4 *>(ix.centroid + (size_t)ix.vq_code[v] * kDim + half * 64);
+        const uint8_t *res = ix.residual + v * ix.bytes_per_vec + half * HALF_BYTES;
+        uint8_t rb[HALF_BYTES];
+#pragma unroll
+        for (int u = 0; u < HALF_BYTES / 8; u++)
+          *reinterpret_cast<uint2 *>(rb + 8 * u) = __ldg(reinterpret_cast<const uint2 *>(res) + u);
+#pragma unroll
+        for (int d4 = 0; d4 < 16; d4++) {
+          const float4 c = __ldg(cen + d4);
+          const float cc[4] = {c.x, c.y, c.z, c.w};
+#pragma unroll
+          for (int u = 0; u < 4; u++) {
+            const int d = d4 * 4 + u;
+            const float w = lut[(uint32_t)rb[d / VPB] * VPB + (d % VPB)];
+            xcol[d * kRerankTile] = __fadd_rn(cc[u], w);
+          }
+        }
+      } else {
+        if (half == 0) tok_doc[t] = -1;
+#pragma unroll 8
+        for (int d = 0; d < 64; d++) xcol[d * kRerankTile] = 0.0f;
+      }
+    }
+    __syncthreads();
+
+    const int tcol = (warp >> 2) * 64 + lane * 2;
+    const int doc0 = tok_doc[tcol], doc1 = tok_doc[tcol + 1];
+    const unsigned g0 = __match_any_sync(kFull, doc0);
+    const unsigned g1 = __match_any_sync(kFull, doc1);
+    for (uint32_t qb = 0; qb < nq; qb += 32) {
+      float acc[8][2];
+#pragma unroll
+      for (int i = 0; i < 8; i++) acc[i][0] = acc[i][1] = 0.0f;
+      const float *qs = Qs + qb + (warp & 3) * 8;
+      const float *xs = Xs + tcol;
+#pragma unroll 4
+      for (int k = 0; k < kDim; k++) {
+        const float4 a0 = *reinterpret_cast<const float4 *>(qs + k * kMaxQueryTok);
+        const float4 a1 = *reinterpret_cast<const float4 *>(qs + k * kMaxQueryTok + 4);
+        const float2 x = *reinterpret_cast<const float2 *>(xs + k * kRerankTile);
+        const float a[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+          acc[i][0] = __fmaf_rn(a[i], x.x, acc[i][0]);
+          acc[i][1] = __fmaf_rn(a[i], x.y, acc[i][1]);
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        const uint32_t qt = qb + (warp & 3) * 8 + i;
+        const int m0 = __reduce_max_sync(g0, f2si(acc[i][0]));
+        const int m1 = __reduce_max_sync(g1, f2si(acc[i][1]));
+        if (qt < nq) {
+          if (doc0 >= 0 && lane == __ffs(g0) - 1) atomicMax(&best[qt * kRerankDocs + doc0], m0);
+          if (doc1 >= 0 && lane == __ffs(g1) - 1) atomicMax(&best[qt * kRerankDocs + doc1], m1);
+        }
+      }
+    }
+    __syncthreads();
+  }
+
+  if (tid < (int)nd) {
+    const bool clamp = semantics == 1 && d_len[tid] < ix.max_item_n_vec;
+    float s = 0.0f;
+    for (uint32_t t = 0; t < nq; t++) {
+      float m = si2f(best[t * kRerankDocs + tid]);
+      if (clamp) m = fmaxf(m, 0.0f);
+      s = __fadd_rn(s, m);
+    }
+    exact[(size_t)b * probe_topk + d0 + tid] = s;
+  }
+}
+
+// ---------------------------------------------------------------------
+// K4: final top-k of the reranked shortlist (bitonic sort of 64-bit keys).
+// ---------------------------------------------------------------------
+__global__ void __launch_bounds__(512)
+topk_kernel(const uint32_t *__restrict__ short_id, const float *__restrict__ exact,
+            const uint32_t *__restrict__ n_short, uint32_t probe_topk,
+            uint32_t n_pad, uint32_t topk, float *__restrict__ out_s,
+            uint32_t *__restrict__ out_id) {
+  extern __shared__ uint64_t keys[];
+  const uint32_t b = blockIdx.x;
+  const uint32_t n = n_short[b];
+  for (uint32_t i = threadIdx.x; i < n_pad; i += blockDim.x)
+    keys[i] = i < n ? make_key(exact[(size_t)b * probe_topk + i], short_id[(size_t)b * probe_topk + i]) : 0ull;
+  __syncthreads();
+  for (uint32_t k = 2; k <= n_pad; k <<= 1) {
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      for (uint32_t i = threadIdx.x; i < n_pad; i += blockDim.x) {
+        const uint32_t l = i ^ j;
+        if (l > i) {
+          const uint64_t a = keys[i], c = keys[l];
+          const bool desc = (i & k) == 0;
+          if (desc ? (a < c) : (a > c)) { keys[i] = c; keys[l] = a; }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (uint32_t i = threadIdx.x; i < topk; i += blockDim.x) {
+    if (i < n) {
+      out_s[(size_t)b * topk + i] = key_score(keys[i]);
+      out_id[(size_t)b * topk + i] = key_id(keys[i]);
+    } else {
+      out_s[(size_t)b * topk + i] = -INFINITY;
+      out_id[(size_t)b * topk + i] = 0xffffffffu;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------
+// host-side launchers
+// ---------------------------------------------------------------------
+size_t rerank_smem_bytes(int n_bit) {
+  return (size_t)(kDim * kRerankTile + kDim * kMaxQueryTok + 256 * (8 / n_bit)) * sizeof(float) +
+         (size_t)kMaxQueryTok * kRerankDocs * sizeof(int);
+}
+
+cudaError_t configure_kernels() {
+  cudaError_t e = cudaFuncSetAttribute(probe_topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kProbeSmem);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(rerank_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rerank_smem_bytes(1));
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(rerank_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rerank_smem_bytes(2));
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(rerank_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rerank_smem_bytes(4));
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(rerank_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rerank_smem_bytes(8));
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)(kMaxShort * sizeof(uint64_t)));
+}
+
+int probe_splits(uint32_t n_tok, uint32_t n_cent_pad, int n_sm) {
+  const uint32_t tok_tiles = (n_tok + kProbeTokTile - 1) / kProbeTokTile;
+  const uint32_t cen_tiles = n_cent_pad / kProbeCenTile;
+  uint32_t want = (uint32_t)(2 * n_sm + tok_tiles - 1) / tok_tiles;  // ~2 waves
+  if (want < 1) want = 1;
+  if (want > cen_tiles) want = cen_tiles;
+  return (int)want;
+}
+
+cudaError_t launch_probe(const DevIndex &ix, const float *q, uint32_t n_tok,
+                         uint32_t nprobe, int n_split, uint32_t *part_id,
+                         float *part_s, uint32_t *out_id, float *out_s,
+                         cudaStream_t st, int *n_launch) {
+  const uint32_t cen_tiles = ix.n_centroid_pad / kProbeCenTile;
+  const uint32_t per = (cen_tiles + n_split - 1) / n_split;
+  const uint32_t splits = (cen_tiles + per - 1) / per;
+  dim3 grid(splits, (n_tok + kProbeTokTile - 1) / kProbeTokTile);
+  if (splits == 1) {
+    probe_topk_kernel<<<grid, 256, kProbeSmem, st>>>(q, n_tok, ix.centroid_t, ix.n_centroid,
+                                                    ix.n_centroid_pad, nprobe, per, out_id, out_s);
+    *n_launch += 1;
+    return cudaGetLastError();
+  }
+  probe_topk_kernel<<<grid, 256, kProbeSmem, st>>>(q, n_tok, ix.centroid_t, ix.n_centroid,
+                                                  ix.n_centroid_pad, nprobe, per, part_id, part_s);
+  probe_merge_kernel<<<(n_tok + 7) / 8, 256, 0, st>>>(part_id, part_s, splits, n_tok, nprobe,
+                                                      out_id, out_s);
+  *n_launch += 2;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_filter(const DevIndex &ix, const uint32_t *probe_id,
+                          const float *probe_s, uint32_t nprobe,
+                          const uint64_t *q_off, uint32_t n_query,
+                          uint32_t probe_topk, const FilterScratch &scr,
+                          uint32_t epoch, uint32_t *short_id,
+                          float *short_approx, uint32_t *n_short,
+                          uint32_t *qstat, cudaStream_t st, int *n_launch) {
+  filter_kernel<<<n_query, kFilterThreads, 0, st>>>(ix, probe_id, probe_s, nprobe, q_off, probe_topk,
+                                                    scr, epoch, short_id, short_approx, n_short, qstat);
+  *n_launch += 1;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rerank(const DevIndex &ix, const float *q, const uint64_t *q_off,
+                          uint32_t n_query, const uint32_t *short_id,
+                          const uint32_t *n_short, uint32_t probe_topk,
+                          int semantics, float *exact, cudaStream_t st,
+                          int *n_launch) {
+  dim3 grid((probe_topk + kRerankDocs - 1) / kRerankDocs, n_query);
+  const size_t sm = rerank_smem_bytes((int)ix.n_bit);
+  switch (ix.n_bit) {
+    case 1: rerank_kernel<1><<<grid, 256, sm, st>>>(ix, q, q_off, short_id, n_short, probe_topk, semantics, exact); break;
+    case 2: rerank_kernel<2><<<grid, 256, sm, st>>>(ix, q, q_off, short_id, n_short, probe_topk, semantics, exact); break;
+    case 4: rerank_kernel<4><<<grid, 256, sm, st>>>(ix, q, q_off, short_id, n_short, probe_topk, semantics, exact); break;
+    case 8: rerank_kernel<8><<<grid, 256, sm, st>>>(ix, q, q_off, short_id, n_short, probe_topk, semantics, exact); break;
+    default: return cudaErrorInvalidValue;
+  }
+  *n_launch += 1;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_topk(const uint32_t *short_id, const float *exact,
+                        const uint32_t *n_short, uint32_t n_query,
+                        uint32_t probe_topk, uint32_t topk, float *out_s,
+                        uint32_t *out_id, cudaStream_t st, int *n_launch) {
+  uint32_t n_pad = 1;
+  while (n_pad < probe_topk) n_pad <<= 1;
+  topk_kernel<<<n_query, 512, n_pad * sizeof(uint64_t), st>>>(short_id, exact, n_short, probe_topk,
+                                                            n_pad, topk, out_s, out_id);
+  *n_launch += 1;
+  return cudaGetLastError();
+}
+
+}  // namespace mvr

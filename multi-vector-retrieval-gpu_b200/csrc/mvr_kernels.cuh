@@ -1,0 +1,43 @@
+// mvr_kernels.cuh -- launchers of the plain FP32 search kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include "mvr_common.cuh"
+
+namespace mvr {
+
+// Per-query-slot scratch of the candidate filter (one slot per CTA of a
+// filter launch).  stamp starts at 0, rank at 0xff; the filter restores rank.
+struct FilterScratch {
+  uint32_t *stamp;       // [slots][n_item] epoch of last visit
+  uint8_t *rank;         // [slots][n_item][rank_stride] best probe rank
+  uint64_t *key;         // [slots][n_item] candidate (score, id) keys
+  uint32_t n_item;
+  uint32_t rank_stride;  // 32 or 64 (>= query tokens, multiple of 16)
+};
+
+cudaError_t configure_kernels();
+int probe_splits(uint32_t n_tok, uint32_t n_cent_pad, int n_sm);
+cudaError_t launch_probe(const DevIndex &ix, const float *q, uint32_t n_tok,
+                         uint32_t nprobe, int n_split, uint32_t *part_id,
+                         float *part_s, uint32_t *out_id, float *out_s,
+                         cudaStream_t st, int *n_launch);
+cudaError_t launch_filter(const DevIndex &ix, const uint32_t *probe_id,
+                          const float *probe_s, uint32_t nprobe,
+                          const uint64_t *q_off, uint32_t n_query,
+                          uint32_t probe_topk, const FilterScratch &scr,
+                          uint32_t epoch, uint32_t *short_id,
+                          float *short_approx, uint32_t *n_short,
+                          uint32_t *qstat /*[n_query][3]: n_cand, list entries
+                                            visited, shortlist tokens*/,
+                          cudaStream_t st, int *n_launch);
+cudaError_t launch_rerank(const DevIndex &ix, const float *q, const uint64_t *q_off,
+                          uint32_t n_query, const uint32_t *short_id,
+                          const uint32_t *n_short, uint32_t probe_topk,
+                          int semantics, float *exact, cudaStream_t st,
+                          int *n_launch);
+cudaError_t launch_topk(const uint32_t *short_id, const float *exact,
+                        const uint32_t *n_short, uint32_t n_query,
+                        uint32_t probe_topk, uint32_t topk, float *out_s,
+                        uint32_t *out_id, cudaStream_t st, int *n_launch);
+
+}  // namespace mvr

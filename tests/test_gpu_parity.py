@@ -1,0 +1,197 @@
+"""CUDA path vs the oracle, through the C ABI: probed centroid ids, candidate
+sets, approximate scores, shortlists, decompressed vectors / bucket indices,
+exact MaxSim scores and final top-k are all compared bit-for-bit (the path's
+canonical FP32 arithmetic is specified in oracle/mvr_oracle.h); FP32 exact
+scores are additionally checked within 1e-5 relative of FP64."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import pyoracle
+from helpers import make_queries, oracle_of, tiny_index
+from mvr import SEM_BASIC, SEM_PP, Index, MvrError, _lib
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "codec_*d128.npz")))
+
+
+def gpu_index(ix):
+    return Index.from_arrays(ix["item_n_vec"], ix["centroid"], ix["vq_code"], ix["ivf_off"],
+                             ix["ivf_size"], ix["ivf_ids"], ix["weight"], ix["n_bit"],
+                             ix["residual"])
+
+
+@pytest.fixture(scope="module", params=[1, 2, 4, 8], ids=lambda b: f"b{b}")
+def pair(request):
+    ix = tiny_index(n_doc=400, n_centroid=96, n_bit=request.param, seed=request.param)
+    g = gpu_index(ix)
+    yield ix, g, oracle_of(ix)
+    g.close()
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[6:-4] for p in GOLDEN])
+def test_decode_matches_reference_golden(path):
+    c = np.load(path)
+    g = Index.from_arrays(c["item_n_vec"], c["centroid"], c["code"], c["ivf_off"], c["ivf_size"],
+                          c["ivf_ids"], c["weight"], int(c["n_bit"]), c["residual"])
+    ids = np.arange(len(c["code"]), dtype=np.uint64)
+    np.testing.assert_array_equal(g.decompress(ids), c["decoded"])
+    np.testing.assert_array_equal(
+        g.unpack_buckets(ids),
+        pyoracle.unpack_buckets(c["residual"], len(c["code"]), 128, int(c["n_bit"])))
+    g.close()
+
+
+def compare_trace(t, r):
+    np.testing.assert_array_equal(t["probe_id"], r["probe_id"])
+    np.testing.assert_array_equal(t["probe_score"], r["probe_score"])
+    np.testing.assert_array_equal(t["cand_id"], r["cand_id"])
+    np.testing.assert_array_equal(t["cand_score"], r["cand_score"])
+    o = np.argsort(r["short_id"])
+    np.testing.assert_array_equal(t["short_id"], r["short_id"][o])
+    np.testing.assert_array_equal(t["short_approx"], r["short_approx"][o])
+    np.testing.assert_array_equal(t["short_exact"], r["short_exact"][o])
+    np.testing.assert_array_equal(t["id"], r["id"])
+    np.testing.assert_array_equal(t["score"], r["score"])
+
+
+@pytest.mark.parametrize("sem", [SEM_PP, SEM_BASIC], ids=["pp", "basic"])
+def test_stage_trace_bit_exact(pair, sem):
+    ix, g, o = pair
+    q, off = make_queries(ix, 4, 32, seed=21)
+    for i in range(4):
+        qi = q[off[i]:off[i + 1]]
+        for nprobe, ptk, k in ((4, 100, 10), (8, 300, 100)):
+            compare_trace(g.trace(qi, k, nprobe, ptk, sem), o.search_one(qi, k, nprobe, ptk, sem))
+
+
+def test_batched_ragged_search_bit_exact(pair):
+    ix, g, o = pair
+    q, off = make_queries(ix, 37, (1, 64), seed=5)
+    g.set_batch(8)  # several batches incl. a partial one
+    s, i, st = g.search(q, 10, 6, 120, tok_off=off, with_stats=True)
+    g.set_batch(0)
+    rs, ri = o.search(q, off, 10, 6, 120)
+    np.testing.assert_array_equal(i, ri)
+    np.testing.assert_array_equal(s, rs)
+    assert st["n_batch"] == 5 and st["gpu_launches"] >= 4 * 5
+
+
+def test_uniform_and_device_entry_points_agree(pair):
+    import torch
+    ix, g, o = pair
+    q, off = make_queries(ix, 12, 32, seed=8)
+    s1, i1 = g.search(q.reshape(12, 32, 128), 10, 4, 100)
+    dq = torch.from_numpy(q).cuda()
+    ds = torch.empty((12, 10), dtype=torch.float32, device="cuda")
+    di = torch.empty((12, 10), dtype=torch.int32, device="cuda")
+    st = g.search_device(dq.data_ptr(), None, 12, 32, 10, 4, 100, ds.data_ptr(), di.data_ptr())
+    np.testing.assert_array_equal(ds.cpu().numpy(), s1)
+    np.testing.assert_array_equal(di.cpu().numpy().view(np.uint32), i1)
+    assert st.h2d_bytes < 4096 and st.d2h_bytes == 0
+
+
+def test_exact_scores_within_fp64_tolerance(pair):
+    ix, g, o = pair
+    q, off = make_queries(ix, 3, 32, seed=9)
+    dec = o.decompress_all().astype(np.float64)
+    toff = np.concatenate([[0], np.cumsum(ix["item_n_vec"].astype(np.int64))])
+    for k in range(3):
+        qi = q[off[k]:off[k + 1]]
+        t = g.trace(qi, 10, 4, 100)
+        for d, s in zip(t["short_id"], t["short_exact"]):
+            ref = (qi.astype(np.float64) @ dec[toff[d]:toff[d + 1]].T).max(1).sum()
+            assert abs(s - ref) <= TOL * abs(ref), (d, s, ref)
+
+
+def test_edge_cases():
+    ix = tiny_index(n_doc=60, n_centroid=40, n_bit=2, seed=7, len_hi=12, len_lo=1)
+    g, o = gpu_index(ix), oracle_of(ix)
+    assert ix["item_n_vec"].min() <= 2
+    q, off = make_queries(ix, 3, 64, seed=3)
+    cases = [dict(k=5, nprobe=32, ptk=5),       # nprobe = max, topk = probe_topk
+             dict(k=10, nprobe=1, ptk=8000),    # shortlist larger than candidate set
+             dict(k=60, nprobe=2, ptk=60)]      # topk beyond candidates -> padded tail
+    for c in cases:
+        for i in range(3):
+            qi = q[off[i]:off[i + 1]]
+            for nq in (1, 7, 64):
+                compare_trace(g.trace(qi[:nq], c["k"], c["nprobe"], c["ptk"]),
+                              o.search_one(qi[:nq], c["k"], c["nprobe"], c["ptk"]))
+    r = g.trace(q[:4], 60, 1, 60)
+    pad = r["id"] == 0xFFFFFFFF
+    assert np.all(np.isneginf(r["score"][pad]))
+    g.close()
+
+
+def test_invalid_arguments_rejected(pair):
+    ix, g, o = pair
+    q = np.zeros((1, 32, 128), np.float32)
+    bad = [dict(k=10, nprobe=4, ptk=5), dict(k=10, nprobe=0, ptk=50),
+           dict(k=10, nprobe=10_000, ptk=50), dict(k=2000, nprobe=4, ptk=4000),
+           dict(k=10, nprobe=4, ptk=9000)]
+    for b in bad:
+        with pytest.raises(MvrError) as e:
+            g.search(q, b["k"], b["nprobe"], b["ptk"])
+        assert e.value.code in (_lib.MVR_ERR_INVALID_ARG, _lib.MVR_ERR_UNSUPPORTED)
+    with pytest.raises(MvrError):
+        g.search(np.zeros((1, 65, 128), np.float32), 10, 4, 50)
+    with pytest.raises(MvrError):
+        g.search(np.zeros((2, 128), np.float32), 10, 4, 50, tok_off=np.array([0, 2, 1], np.uint64))
+
+
+def test_gpu_builder_matches_oracle_codec():
+    import torch
+    from mvr import build, synth
+    spec = synth.CorpusSpec(800, seed=4, n_latent=300)
+    tok = synth.tokens(spec, "cuda")
+    ix = build.build_index(tok, spec.item_n_vec, 128, 2, kmeans_iter=3)
+    h = build.to_host(ix)
+    tn = tok.cpu().numpy()
+    np.testing.assert_array_equal(h["vq_code"], pyoracle.assign(tn, h["centroid"]))
+    np.testing.assert_array_equal(
+        h["residual"], pyoracle.pack_residual(tn, h["centroid"], h["vq_code"], ix["cutoff"], 2))
+    off, size, ids = pyoracle.ivf_build(h["vq_code"], spec.item_n_vec, 128)
+    np.testing.assert_array_equal(h["ivf_off"], off)
+    np.testing.assert_array_equal(h["ivf_size"], size)
+    np.testing.assert_array_equal(h["ivf_ids"], ids)
+    # quantile parameters: exact order statistics of the k-means sample residuals
+    pids = build.sample_items(len(spec.item_n_vec))
+    toff = np.concatenate([[0], np.cumsum(spec.item_n_vec.astype(np.int64))])
+    sidx = np.concatenate([np.arange(toff[p], toff[p + 1]) for p in pids])
+    samp = tn[sidx]
+    cut, w = pyoracle.quantize(samp, h["centroid"], pyoracle.assign(samp, h["centroid"]), 2)
+    np.testing.assert_array_equal(ix["cutoff"], cut)
+    np.testing.assert_array_equal(h["weight"], w)
+    g = build.load_built(ix)
+    assert g.info()["n_vec"] == len(tn)
+    g.close()
+    del tok
+    torch.cuda.empty_cache()
+
+
+def test_config1_scale_gpu_built_index_bit_exact():
+    """10,000 docs / 8,192 centroids / nbits 2 (the small synthetic config),
+    built on the GPU; 16 queries x (nprobe 4, k 10 and 100) vs the oracle."""
+    import torch
+    from mvr import build, synth
+    spec = synth.CorpusSpec(10_000, seed=1)
+    tok = synth.tokens(spec, "cuda")
+    ix = build.build_index(tok, spec.item_n_vec, 8192, 2, kmeans_iter=2)
+    g = build.load_built(ix)
+    h = build.to_host(ix)
+    o = pyoracle.Oracle(h["item_n_vec"], h["centroid"], h["vq_code"], h["residual"], h["weight"],
+                        h["ivf_off"], h["ivf_size"], h["ivf_ids"], 2)
+    q, off = synth.queries(spec, 16, 32, "cpu", seed=3)
+    q = q.numpy()
+    for k, ptk in ((10, 200), (100, 1000)):
+        s, i = g.search(q.reshape(16, 32, 128), k, 4, ptk)
+        rs, ri = o.search(q, off, k, 4, ptk)
+        np.testing.assert_array_equal(i, ri)
+        np.testing.assert_array_equal(s, rs)
+    g.close()
+    del tok
+    torch.cuda.empty_cache()
