@@ -1,0 +1,417 @@
+#!/usr/bin/env python
+"""bench.py -- throughput of the GPU multi-vector search path on B200.
+
+One step = one search pass over the workload's query set (10,000 queries x 32
+tokens for the default "medium" workload: 1M synthetic docs / ~70M tokens,
+65,536 centroids, nbits 2, nprobe 8, k 10).  The index is built on the GPU
+from the seeded synthetic corpus before anything is timed.
+
+  value : queries/s with queries resident in HBM (mvr_search_device), device
+          time by CUDA events on the launching stream, L2 flushed between
+          steps, max over ranks
+  e2e   : queries/s through mvr_search with pinned HOST query/result buffers
+          (copies inside the timed region), wall clock around each call
+  roofline : the dominant stage's algorithmic work / its CUDA-event time
+  cpu_baseline : the oracle's multi-threaded CPU port of the same path on a
+          bounded query sample (rank 0, N=1)
+
+--impl reference times that CPU port alone (all host threads) as the
+reference arm.  N>1 (torchrun): each rank serves its own query set against its
+own replica of the index (weak scaling, no data-path collective).
+"""
+import argparse
+import hashlib
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "multi-vector-retrieval-gpu_b200"))
+
+METRIC = ("QPS & p99 ms at recall@10>=0.99 vs exact MaxSim: learned+BF16/FP8 vs plain, "
+          "1 B200")
+CACHE_VERSION = "mvr-index-v1"
+
+WORKLOADS = {
+    # 1M docs, 65,536 centroids, nbits 2, 10,000 queries
+    "medium": dict(n_doc=1_000_000, n_centroid=65536, n_bit=2, n_query=10_000, n_tok=32,
+                   nprobe=8, topk=10, probe_topk=1000, kmeans_iter=4, seed=0, n_gt=100),
+    # 10k docs, 8,192 centroids, nbits 2, 1,000 queries
+    "small": dict(n_doc=10_000, n_centroid=8192, n_bit=2, n_query=1000, n_tok=32, nprobe=4,
+                  topk=10, probe_topk=200, kmeans_iter=8, seed=0, n_gt=200),
+}
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        p = json.load(open(path))
+        return dict(hbm=p["hbm_gbs"], tc=p["bf16_tflops"], tc_sus=p["bf16_tflops_sustained"],
+                    src="measured")
+    return dict(hbm=6650.0, tc=1590.0, tc_sus=1400.0, src="fallback")
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cache_dir(w):
+    key = json.dumps({k: w[k] for k in ("n_doc", "n_centroid", "n_bit", "kmeans_iter", "seed")},
+                     sort_keys=True) + CACHE_VERSION
+    return os.path.join("/tmp", "mvr_bench_cache", hashlib.sha1(key.encode()).hexdigest()[:16])
+
+
+def get_index(w, device, rank, want_tokens):
+    """GPU-built index (cached on local disk so both bench arms build once)."""
+    import torch
+    from mvr import build, formats, synth
+    spec = synth.CorpusSpec(w["n_doc"], seed=w["seed"])
+    cdir = cache_dir(w)
+    tok = None
+    t0 = time.time()
+    if os.path.exists(os.path.join(cdir, "DONE")):
+        host = formats.read_index_dir(cdir)
+        host["n_bit"] = w["n_bit"]
+        built_s = None
+    else:
+        tok = synth.tokens(spec, device)
+        ix = build.build_index(tok, spec.item_n_vec, w["n_centroid"], w["n_bit"],
+                               kmeans_iter=w["kmeans_iter"], seed=123 + w["seed"])
+        host = build.to_host(ix)
+        del ix
+        built_s = time.time() - t0
+        if rank == 0:
+            tmp = cdir + f".tmp{os.getpid()}"
+            try:
+                formats.write_index_dir(tmp, host["item_n_vec"], host["centroid"],
+                                        host["vq_code"], host["weight"], host["residual"],
+                                        host["ivf_off"], host["ivf_size"], host["ivf_ids"])
+                open(os.path.join(tmp, "DONE"), "w").close()
+                os.replace(tmp, cdir)
+            except OSError:
+                pass
+    if want_tokens and tok is None:
+        tok = synth.tokens(spec, device)
+    torch.cuda.empty_cache()
+    return spec, host, tok, built_s
+
+
+def load_gpu_index(host, device_idx):
+    from mvr import Index
+    return Index.from_arrays(host["item_n_vec"], host["centroid"], host["vq_code"],
+                             host["ivf_off"], host["ivf_size"], host["ivf_ids"], host["weight"],
+                             host["n_bit"], host["residual"], device=device_idx)
+
+
+def cpu_port_qps(host, q_np, off, w, n_threads, budget_s=15.0):
+    """The oracle's CPU port of the path (test infrastructure) on a bounded
+    query sample; returns (qps, sample size, seconds)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    o = pyoracle.Oracle(host["item_n_vec"], host["centroid"], host["vq_code"], host["residual"],
+                        host["weight"], host["ivf_off"], host["ivf_size"], host["ivf_ids"],
+                        host["n_bit"])
+    probe_n = min(len(off) - 1, max(2 * n_threads, 8))
+    t = time.perf_counter()
+    o.search(q_np[: off[probe_n]], off[: probe_n + 1], w["topk"], w["nprobe"], w["probe_topk"],
+             n_threads=n_threads)
+    per_q = (time.perf_counter() - t) / probe_n
+    n = int(min(len(off) - 1, max(probe_n, budget_s / max(per_q, 1e-6))))
+    t = time.perf_counter()
+    o.search(q_np[: off[n]], off[: n + 1], w["topk"], w["nprobe"], w["probe_topk"],
+             n_threads=n_threads)
+    dt = time.perf_counter() - t
+    return n / dt, n, dt, o
+
+
+def run_reference(args, w):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    from mvr import synth
+    spec, host, _, _ = get_index(w, f"cuda:{local}", rank, want_tokens=False)
+    q, off = synth.queries(spec, w["n_query"], w["n_tok"], f"cuda:{local}", seed=100)
+    q_np = q.cpu().numpy()
+    del q
+    n_threads = os.cpu_count()
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    o = pyoracle.Oracle(host["item_n_vec"], host["centroid"], host["vq_code"], host["residual"],
+                        host["weight"], host["ivf_off"], host["ivf_size"], host["ivf_ids"],
+                        host["n_bit"])
+    # size each step to a bounded sample (~8 s of CPU work)
+    t = time.perf_counter()
+    m = min(w["n_query"], 2 * n_threads)
+    o.search(q_np[: off[m]], off[: m + 1], w["topk"], w["nprobe"], w["probe_topk"],
+             n_threads=n_threads)
+    per_q = (time.perf_counter() - t) / m
+    n = int(max(m, min(w["n_query"], 8.0 / max(per_q, 1e-6))))
+    for _ in range(args.warmup):
+        o.search(q_np[: off[m]], off[: m + 1], w["topk"], w["nprobe"], w["probe_topk"],
+                 n_threads=n_threads)
+    t = time.perf_counter()
+    for s in range(args.steps):
+        a = (s * n) % max(1, w["n_query"] - n + 1)
+        o.search(q_np[off[a]: off[a + n]], off[a: a + n + 1] - off[a], w["topk"], w["nprobe"],
+                 w["probe_topk"], n_threads=n_threads)
+    dt = time.perf_counter() - t
+    qps = args.steps * n / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": qps, "unit": "queries/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(w, "CPU port of the reference path (oracle)"),
+        "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": n_threads, "kind": "port",
+                         "sample": f"{n} queries per step of the {w['n_query']}-query workload"},
+        "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def workload_config(w, path):
+    return {"workload": (f"{path}: {w['n_doc']:,} synthetic docs (lognormal 70/35, clipped 8..180), "
+                         f"{w['n_centroid']:,} centroids, nbits {w['n_bit']}, "
+                         f"{w['n_query']:,} queries x {w['n_tok']} tok, nprobe {w['nprobe']}, "
+                         f"k {w['topk']}, probe_topk {w['probe_topk']}"),
+            "n_doc": w["n_doc"], "n_centroid": w["n_centroid"], "n_bit": w["n_bit"],
+            "queries_per_step": w["n_query"], "query_tokens": w["n_tok"], "nprobe": w["nprobe"],
+            "topk": w["topk"], "probe_topk": w["probe_topk"], "kmeans_iter": w["kmeans_iter"],
+            "l2": "flushed (256 MiB write) between timed steps"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["mvr", "reference"], default="mvr")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="medium")
+    ap.add_argument("--probe-topk", type=int, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--recall-sweep", default="",
+                    help="extra nprobe:probe_topk settings whose recall@k is reported, "
+                         "e.g. 4:100,8:500")
+    args = ap.parse_args()
+    w = dict(WORKLOADS[args.workload])
+    if args.probe_topk:
+        w["probe_topk"] = args.probe_topk
+    if args.impl == "reference":
+        return run_reference(args, w)
+
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = f"cuda:{local}"
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(minutes=20))
+
+    from mvr import exhaustive, formats, synth
+    spec, host, tok, built_s = get_index(w, dev, rank, want_tokens=(rank == 0))
+    g = load_gpu_index(host, local)
+    q, off = synth.queries(spec, w["n_query"], w["n_tok"], dev, seed=100 + rank)
+    n_query, T = w["n_query"], q.shape[0]
+    k, nprobe, ptk = w["topk"], w["nprobe"], w["probe_topk"]
+    stream = torch.cuda.current_stream()
+    out_s = torch.empty((n_query, k), dtype=torch.float32, device=dev)
+    out_i = torch.empty((n_query, k), dtype=torch.int32, device=dev)
+
+    def step():
+        return g.search_device(q.data_ptr(), None, n_query, w["n_tok"], k, nprobe, ptk,
+                               out_s.data_ptr(), out_i.data_ptr(), stream.cuda_stream)
+
+    # recall@10 against exhaustive FP64 MaxSim over the raw tokens (rank 0)
+    recall = None
+    sweep = {}
+    if rank == 0:
+        step()
+        n_gt = w["n_gt"]
+        qg = q[: n_gt * w["n_tok"]]
+        gs, gi = exhaustive.exhaustive_topk(qg, off[: n_gt + 1], tok, spec.item_n_vec, k)
+        est = out_i[:n_gt].cpu().numpy().view(np.uint32)
+        recall = float(formats.recall_at_k(gi, est, k).mean())
+        qg_np = qg.cpu().numpy()
+        for item in filter(None, args.recall_sweep.split(",")):
+            npb, ptk_s = (int(x) for x in item.split(":"))
+            _, si = g.search(qg_np.reshape(n_gt, w["n_tok"], 128), k, npb, ptk_s)
+            sweep[item] = float(formats.recall_at_k(gi, si, k).mean())
+        del tok
+        torch.cuda.empty_cache()
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    stage = np.zeros(5)
+    launches = n_cand = n_tok_rr = n_ent = 0
+    with ClockSampler(local) as clk:
+        for s in range(args.steps):
+            flush.fill_(s & 0xFF)
+            ev[s][0].record(stream)
+            st = step()
+            ev[s][1].record(stream)
+            stage += np.asarray(list(st.stage_ms))
+            launches += st.gpu_launches
+            n_cand += st.n_cand_total
+            n_tok_rr += st.n_rerank_tok
+            n_ent += st.n_list_ent
+        torch.cuda.synchronize()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = float(sum(step_ms))
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    value = world * n_query * args.steps / (total_ms / 1e3)
+
+    # end to end: pinned host buffers, copies inside every step
+    hq = q.cpu().pin_memory()
+    hs = torch.empty((n_query, k), dtype=torch.float32).pin_memory()
+    hi = torch.empty((n_query, k), dtype=torch.int32).pin_memory()
+    qtime = np.zeros(n_query)
+    e2e_dt = []
+    for s in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st_e = g.search_host_ptr(hq.data_ptr(), None, n_query, w["n_tok"], k, nprobe, ptk,
+                                 hs.data_ptr(), hi.data_ptr(), qtime=qtime)
+        if s >= args.warmup:
+            e2e_dt.append(time.perf_counter() - t0)
+    e2e_s = float(sum(e2e_dt))
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = world * n_query * args.steps / e2e_s
+    p50, p99 = (float(np.percentile(qtime, p)) * 1e3 for p in (50, 99))
+
+    if rank != 0:
+        dist.destroy_process_group()
+        return
+
+    # roofline of the dominant stage (stage_ms: copy, probe, filter, rerank+topk, copy)
+    pk = peaks()
+    S = args.steps
+    C, D = w["n_centroid"], 128
+    bpv = D * w["n_bit"] // 8
+    probe_flop = 2.0 * T * C * D * S
+    rerank_flop = 2.0 * w["n_tok"] * D * n_tok_rr
+    rerank_bytes = (4.0 + bpv) * n_tok_rr
+    filter_bytes = 4.0 * n_ent + (4 + 32 + 8) * n_cand
+    kern = {1: ("probe_topk_kernel", "tensor", probe_flop / 1e12, pk["tc_sus"], "TFLOP/s"),
+            2: ("filter_kernel", "hbm", filter_bytes / 1e9, pk["hbm"], "GB/s"),
+            3: ("rerank_kernel", "tensor", rerank_flop / 1e12, pk["tc_sus"], "TFLOP/s")}
+    dom = max((1, 2, 3), key=lambda i: stage[i])
+    name, bound, work, peak, unit = kern[dom]
+    achieved = work / (stage[dom] / 1e3)
+    roof = {"kernel": name, "bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
+            "frac": achieved / peak, "traffic": None,
+            "peak_source": f"{pk['src']} ({'bf16 sustained' if bound == 'tensor' else 'HBM copy'})",
+            "stage_share": {n: float(stage[i] / stage.sum()) for i, n in
+                            ((0, "query_copy"), (1, "probe"), (2, "filter"), (3, "rerank_topk"),
+                             (4, "result_copy"))},
+            "per_stage": {kern[i][0]: {"ms_per_step": float(stage[i] / S),
+                                       "achieved": kern[i][2] / (stage[i] / 1e3),
+                                       "unit": kern[i][4]} for i in (1, 2, 3)}}
+
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        qps_cpu, n_s, dt_s, _ = cpu_port_qps(host, hq.numpy(), off, w, os.cpu_count())
+        cpu = {"value": qps_cpu, "unit": "queries/s", "cores": os.cpu_count(), "kind": "port",
+               "sample": f"first {n_s} of the {n_query} queries ({dt_s:.1f} s)"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": S,
+        "warmup": args.warmup, "ms_per_step": total_ms / S, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": dict(workload_config(w, "plain FP32 CUDA path"),
+                       **{"recall@10": recall, "recall_queries": w["n_gt"],
+                          "recall_sweep": sweep,
+                          "p50_ms": p50, "p99_ms": p99, "latency": "per query = its batch's "
+                          "device latency incl. copies (e2e run)",
+                          "parallelism": f"replica x{world}, queries split by rank",
+                          "index_build_s": built_s, "cand_per_query": n_cand / (S * n_query),
+                          "rerank_tok_per_query": n_tok_rr / (S * n_query)}),
+        "e2e": {"value": e2e, "unit": "queries/s",
+                "h2d_bytes_per_step": int(st_e.h2d_bytes), "d2h_bytes_per_step": int(st_e.d2h_bytes)},
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "clocks": clk.summary(),
+        "gpu_launches": int(launches),
+        "p99_ms": p99,
+    }
+    print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -38,6 +38,11 @@ typedef enum {
 #define MVR_SEM_BASIC 1u /* rerank over docs zero-padded to the longest doc,
                             i.e. max(0, .) per query token for shorter docs
                             (Rerank.hpp:166-179,287-306) */
+#define MVR_PREC_BF16 2u /* mixed precision: the shortlist is scored by the
+                            BF16 tensor-core (tcgen05) MaxSim kernel with FP32
+                            accumulation, and its best R docs are re-scored by
+                            the exact FP32 kernel (R: mvr_index_set_rescore).
+                            Returned scores are always exact FP32 MaxSim. */
 
 typedef struct mvr_index mvr_index;
 
@@ -59,8 +64,9 @@ typedef struct {
   uint64_t n_cand_total;  /* sum over queries of candidate-set sizes */
   uint64_t n_rerank_tok;  /* sum over queries of reranked doc tokens */
   uint64_t n_list_ent;    /* sum over queries of probed IVF entries read */
-  double stage_ms[5];     /* CUDA-event time summed over batches: query
-                             copy, scoring + probe, filter, rerank + top-k,
+  double stage_ms[6];     /* CUDA-event time summed over batches: query
+                             copy, scoring + probe, filter, rerank (FP32 or
+                             BF16 tensor-core), FP32 re-score + top-k,
                              result copy */
 } mvr_stats;
 
@@ -141,6 +147,10 @@ int mvr_index_get_info(const mvr_index *h, mvr_index_info *info);
 /* Queries per device batch (default chosen from the index size). */
 int mvr_index_set_batch(mvr_index *h, uint32_t max_batch_queries);
 
+/* Docs per query that the MVR_PREC_BF16 path re-scores exactly in FP32
+ * (0 = default 4 * topk; clamped to [topk, probe_topk]). */
+int mvr_index_set_rescore(mvr_index *h, uint32_t n_rescore);
+
 /* Batched search with HOST buffers (queries in, results out; copies inside).
  * query_l: float32 tokens, query i = rows [tok_off[i], tok_off[i+1]) of a
  * [*, dim] matrix; tok_off == NULL means every query has query_n_vec tokens
@@ -158,9 +168,10 @@ int mvr_search(mvr_index *h, const float *query_l, const uint64_t *tok_off,
                double *query_time_s, mvr_stats *stats);
 
 /* mvr_search plus per-query stage times (seconds, of the query's batch):
- * stage_time_s[i*5 + k], k = 0 query copy, 1 centroid scoring + probe,
- * 2 candidate filter + shortlist, 3 rerank + top-k, 4 result copy -- the
- * stage columns of the reference's performance TSV (IGPGPUBasic.cpp:183-204). */
+ * stage_time_s[i*6 + k], k = 0 query copy, 1 centroid scoring + probe,
+ * 2 candidate filter + shortlist, 3 rerank, 4 re-score + top-k, 5 result
+ * copy -- the stage columns of the reference's performance TSV
+ * (IGPGPUBasic.cpp:183-204). */
 int mvr_search_staged(mvr_index *h, const float *query_l,
                       const uint64_t *tok_off, uint32_t n_query,
                       uint32_t query_n_vec, uint32_t topk, uint32_t nprobe,

@@ -55,7 +55,7 @@ void IndexBase::run(const float *query_l, uint32_t n_query, uint32_t query_n_vec
   score.assign((size_t)n_query * topk, 0.f);
   id.assign((size_t)n_query * topk, 0u);
   qtime.assign(n_query, 0.0);
-  if (stage) stage->assign((size_t)n_query * 5, 0.0);
+  if (stage) stage->assign((size_t)n_query * 6, 0.0);
   mvr_stats st{};
   if (mvr_search_staged(h_, query_l, nullptr, n_query, query_n_vec, topk, nprobe, probe_topk,
                         flags, score.data(), id.data(), qtime.data(),
@@ -83,14 +83,14 @@ IGPGPUBasicResult IGPGPUBasic::search(const float *query_l, uint32_t n_query,
   r.rerank_transmit_time_l.resize(n_query);
   r.rerank_compute_time_l.resize(n_query);
   for (uint32_t i = 0; i < n_query; i++) {
-    const double *s = stage.data() + (size_t)i * 5;
+    const double *s = stage.data() + (size_t)i * 6;
     r.transmit_query_time_l[i] = s[0];
     r.cand_gen_time_l[i] = s[1];
     r.filter_time_l[i] = s[2];
     r.filter_compute_time_l[i] = s[2];
-    r.rerank_compute_time_l[i] = s[3];
-    r.rerank_transmit_time_l[i] = s[4];
-    r.rerank_time_l[i] = s[3] + s[4];
+    r.rerank_compute_time_l[i] = s[3] + s[4];
+    r.rerank_transmit_time_l[i] = s[5];
+    r.rerank_time_l[i] = s[3] + s[4] + s[5];
   }
   return r;
 }

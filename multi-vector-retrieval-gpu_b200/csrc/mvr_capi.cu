@@ -17,6 +17,7 @@
 #include "mvr_common.cuh"
 #include "mvr_io.hpp"
 #include "mvr_kernels.cuh"
+#include "mvr_tc.cuh"
 
 using namespace mvr;
 
@@ -115,6 +116,9 @@ struct Workspace {
   float *short_approx = nullptr, *exact = nullptr;
   float *out_s = nullptr;
   uint32_t *out_id = nullptr;
+  uint32_t r_cap = 0;             // FP32 re-score of the top-R (BF16 path)
+  uint32_t *r_id = nullptr, *n_r = nullptr;
+  float *r_score = nullptr, *r_exact = nullptr;
   // per call
   size_t off_cap = 0, stat_cap = 0;
   uint64_t *q_off = nullptr;    // device, all batches' relative offsets
@@ -133,13 +137,18 @@ struct mvr_index {
   cudaStream_t stream = nullptr;
   std::vector<cudaEvent_t> events;
   uint32_t batch_cap = 0;
+  uint32_t rescore = 0;          // FP32 re-score count of the BF16 path (0: 4 * topk)
   uint32_t epoch = 0;
+  void *cen_bf16 = nullptr;      // [C][128] BF16 centroid rows
+  void *lut_bf16 = nullptr;      // [256][8/b] BF16 decode table
+  unsigned *d_err = nullptr;     // device error flags of the tensor-core kernels
   Workspace ws;
 
   ~mvr_index() {
     DeviceGuard g(device);
     if (stream) cudaStreamSynchronize(stream);
     for (void *p : bufs) dfree(p);
+    dfree(d_err);
     free_scratch();
     free_batch();
     dfree(ws.q_off);
@@ -157,8 +166,12 @@ struct mvr_index {
   void free_batch() {
     for (void *p : {(void *)ws.q, (void *)ws.probe_id, (void *)ws.part_id, (void *)ws.probe_s,
                     (void *)ws.part_s, (void *)ws.short_id, (void *)ws.n_short,
-                    (void *)ws.short_approx, (void *)ws.exact, (void *)ws.out_s, (void *)ws.out_id})
+                    (void *)ws.short_approx, (void *)ws.exact, (void *)ws.out_s, (void *)ws.out_id,
+                    (void *)ws.r_id, (void *)ws.n_r, (void *)ws.r_score, (void *)ws.r_exact})
       dfree(p);
+    ws.r_id = ws.n_r = nullptr;
+    ws.r_score = ws.r_exact = nullptr;
+    ws.r_cap = 0;
     ws.q = nullptr; ws.probe_id = ws.part_id = nullptr; ws.probe_s = ws.part_s = nullptr;
     ws.short_id = ws.n_short = nullptr; ws.short_approx = ws.exact = nullptr;
     ws.out_s = nullptr; ws.out_id = nullptr;
@@ -197,11 +210,13 @@ int ensure_scratch(mvr_index *h, uint32_t slots, uint32_t rank_stride) {
 }
 
 int ensure_batch(mvr_index *h, uint32_t slots, uint32_t tok_cap, uint32_t nprobe,
-                 uint32_t short_cap, uint32_t topk, size_t part_need) {
+                 uint32_t short_cap, uint32_t topk, size_t part_need, uint32_t r_cap) {
   Workspace &w = h->ws;
   if (w.batch_slots >= slots && w.tok_cap >= tok_cap && w.np_cap >= nprobe &&
-      w.short_cap >= short_cap && w.topk_cap >= topk && w.part_cap >= part_need)
+      w.short_cap >= short_cap && w.topk_cap >= topk && w.part_cap >= part_need &&
+      w.r_cap >= r_cap)
     return MVR_OK;
+  r_cap = std::max(r_cap, w.r_cap);
   const uint32_t s = std::max(slots, w.batch_slots);
   tok_cap = std::max(tok_cap, w.tok_cap);
   nprobe = std::max(nprobe, w.np_cap);
@@ -220,6 +235,11 @@ int ensure_batch(mvr_index *h, uint32_t slots, uint32_t tok_cap, uint32_t nprobe
   MVR_TRY(dalloc(&w.n_short, (size_t)s));
   MVR_TRY(dalloc(&w.out_s, (size_t)s * topk));
   MVR_TRY(dalloc(&w.out_id, (size_t)s * topk));
+  MVR_TRY(dalloc(&w.r_id, (size_t)s * r_cap));
+  MVR_TRY(dalloc(&w.r_score, (size_t)s * r_cap));
+  MVR_TRY(dalloc(&w.r_exact, (size_t)s * r_cap));
+  MVR_TRY(dalloc(&w.n_r, (size_t)s));
+  w.r_cap = r_cap;
   w.batch_slots = s;
   w.tok_cap = tok_cap;
   w.np_cap = nprobe;
@@ -307,10 +327,12 @@ int build_offsets(const uint64_t *tok_off, uint32_t n_query, uint32_t query_n_ve
 
 // The shared batched pipeline.  host_io: queries/results are host buffers
 // (copied per batch inside the call); otherwise device buffers.
-// Events: 5 per batch (start, query copied, probed, filtered, reranked) plus
-// one closing event; stage_s (nullable) receives per query the 5 stage times
-// of its batch: query copy, centroid scoring + probe, filter, rerank + top-k,
-// result copy.
+// Events: kStages+0 per batch at the stage boundaries plus one closing event;
+// stage k of a batch = events[bt*kStages+k] .. events[bt*kStages+k+1]:
+//   0 query copy, 1 centroid scoring + probe, 2 candidate filter + shortlist,
+//   3 rerank (FP32, or BF16 tensor-core), 4 FP32 re-score + top-k, 5 result copy.
+constexpr int kStages = 6;
+
 int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, uint32_t n_query,
                 uint32_t query_n_vec, uint32_t topk, uint32_t nprobe, uint32_t probe_topk,
                 uint32_t flags, float *out_s, uint32_t *out_id, double *query_time_s,
@@ -322,7 +344,12 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
     return MVR_OK;
   }
   if (!query || !out_s || !out_id) return set_err(MVR_ERR_INVALID_ARG, "null query/result buffer");
-  if (flags > MVR_SEM_BASIC) return set_err(MVR_ERR_INVALID_ARG, "unknown flags %u", flags);
+  if (flags & ~(MVR_SEM_BASIC | MVR_PREC_BF16))
+    return set_err(MVR_ERR_INVALID_ARG, "unknown flags %u", flags);
+  const int sem = (flags & MVR_SEM_BASIC) ? 1 : 0;
+  const bool bf16 = (flags & MVR_PREC_BF16) != 0;
+  uint32_t R = h->rescore ? h->rescore : 4 * topk;
+  R = std::min(std::max(R, topk), probe_topk);
   std::vector<uint64_t> off;
   uint32_t nq_max = 0;
   MVR_TRY(build_offsets(tok_off_in, n_query, query_n_vec, off, &nq_max));
@@ -341,8 +368,9 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
   }
   const uint32_t rank_stride = nq_max <= 32 ? 32u : 64u;
   MVR_TRY(ensure_scratch(h, std::min(B, n_query), rank_stride));
-  MVR_TRY(ensure_batch(h, std::min(B, n_query), tok_cap, nprobe, probe_topk, topk, part_need));
-  MVR_TRY(ensure_call(h, (size_t)n_query + n_batch, (size_t)n_query * 3, 5 * n_batch + 1));
+  MVR_TRY(ensure_batch(h, std::min(B, n_query), tok_cap, nprobe, probe_topk, topk, part_need, R));
+  MVR_TRY(ensure_call(h, (size_t)n_query + n_batch, (size_t)n_query * 3,
+                      (size_t)kStages * n_batch + 1));
   Workspace &w = h->ws;
 
   // relative token offsets of every batch, uploaded once
@@ -356,9 +384,10 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
   FilterScratch scr{w.stamp, w.rank, w.key, h->dix.n_item, w.rank_stride};
   int launches = 0;
   uint64_t h2d = ((size_t)n_query + n_batch) * sizeof(uint64_t), d2h = 0;
+  auto ev = [&](uint32_t bt, int k) { return h->events[(size_t)bt * kStages + k]; };
   for (uint32_t bt = 0; bt < n_batch; bt++) {
     const uint32_t s = bt * B, e = std::min(n_query, s + B), nb = e - s;
-    CUDA_TRY(cudaEventRecord(h->events[bt * 5 + 0], st));
+    CUDA_TRY(cudaEventRecord(ev(bt, 0), st));
     const uint32_t T = (uint32_t)(off[e] - off[s]);
     const uint64_t *qo = w.q_off + (size_t)s + bt;
     const float *qp;
@@ -370,12 +399,12 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
     } else {
       qp = query + off[s] * kDim;
     }
-    CUDA_TRY(cudaEventRecord(h->events[bt * 5 + 1], st));
+    CUDA_TRY(cudaEventRecord(ev(bt, 1), st));
     int splits;
     part_entries(h, T, nprobe, &splits);
     CUDA_TRY(launch_probe(h->dix, qp, T, nprobe, splits, w.part_id, w.part_s, w.probe_id,
                           w.probe_s, st, &launches));
-    CUDA_TRY(cudaEventRecord(h->events[bt * 5 + 2], st));
+    CUDA_TRY(cudaEventRecord(ev(bt, 2), st));
     if (++h->epoch == 0) {  // stamps wrapped: clear them
       CUDA_TRY(cudaMemsetAsync(w.stamp, 0, (size_t)w.slots * h->dix.n_item * sizeof(uint32_t), st));
       h->epoch = 1;
@@ -383,13 +412,27 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
     CUDA_TRY(launch_filter(h->dix, w.probe_id, w.probe_s, nprobe, qo, nb, probe_topk, scr, h->epoch,
                            w.short_id, w.short_approx, w.n_short, w.qstat + (size_t)s * 3, st,
                            &launches));
-    CUDA_TRY(cudaEventRecord(h->events[bt * 5 + 3], st));
-    CUDA_TRY(launch_rerank(h->dix, qp, qo, nb, w.short_id, w.n_short, probe_topk, (int)flags,
-                           w.exact, st, &launches));
+    CUDA_TRY(cudaEventRecord(ev(bt, 3), st));
     float *os = host_io ? w.out_s : out_s + (size_t)s * topk;
     uint32_t *oi = host_io ? w.out_id : out_id + (size_t)s * topk;
-    CUDA_TRY(launch_topk(w.short_id, w.exact, w.n_short, nb, probe_topk, topk, os, oi, st, &launches));
-    CUDA_TRY(cudaEventRecord(h->events[bt * 5 + 4], st));
+    if (bf16) {
+      // BF16 tensor-core MaxSim over the whole shortlist, then the exact FP32
+      // kernel re-scores its best R docs
+      CUDA_TRY(launch_rerank_tc(h->dix, h->cen_bf16, h->lut_bf16, qp, qo, nb, w.short_id,
+                                w.n_short, probe_topk, sem, w.exact, h->d_err, st, &launches));
+      CUDA_TRY(cudaEventRecord(ev(bt, 4), st));
+      CUDA_TRY(launch_topk(w.short_id, w.exact, w.n_short, nb, probe_topk, R, w.r_score, w.r_id,
+                           w.n_r, st, &launches));
+      CUDA_TRY(launch_rerank(h->dix, qp, qo, nb, w.r_id, w.n_r, R, sem, w.r_exact, st, &launches));
+      CUDA_TRY(launch_topk(w.r_id, w.r_exact, w.n_r, nb, R, topk, os, oi, nullptr, st, &launches));
+    } else {
+      CUDA_TRY(launch_rerank(h->dix, qp, qo, nb, w.short_id, w.n_short, probe_topk, sem, w.exact,
+                             st, &launches));
+      CUDA_TRY(cudaEventRecord(ev(bt, 4), st));
+      CUDA_TRY(launch_topk(w.short_id, w.exact, w.n_short, nb, probe_topk, topk, os, oi, nullptr,
+                           st, &launches));
+    }
+    CUDA_TRY(cudaEventRecord(ev(bt, 5), st));
     if (host_io) {
       CUDA_TRY(cudaMemcpyAsync(out_s + (size_t)s * topk, w.out_s, (size_t)nb * topk * sizeof(float),
                                cudaMemcpyDeviceToHost, st));
@@ -398,25 +441,34 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
       d2h += (size_t)nb * topk * 8;
     }
   }
-  CUDA_TRY(cudaEventRecord(h->events[n_batch * 5], st));
+  CUDA_TRY(cudaEventRecord(h->events[(size_t)n_batch * kStages], st));
   CUDA_TRY(cudaMemcpyAsync(w.h_qstat, w.qstat, (size_t)n_query * 3 * sizeof(uint32_t),
                            cudaMemcpyDeviceToHost, st));
+  unsigned herr = 0;
+  if (bf16) CUDA_TRY(cudaMemcpyAsync(&herr, h->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
   CUDA_TRY(cudaStreamSynchronize(st));
   CUDA_TRY(cudaGetLastError());
+  if (herr) {
+    CUDA_TRY(cudaMemset(h->d_err, 0, sizeof(unsigned)));
+    return set_err(MVR_ERR_CUDA, "tensor-core rerank: an MMA completion wait timed out");
+  }
 
   float total_ms = 0.f, max_ms = 0.f;
-  CUDA_TRY(cudaEventElapsedTime(&total_ms, h->events[0], h->events[n_batch * 5]));
+  CUDA_TRY(cudaEventElapsedTime(&total_ms, h->events[0], h->events[(size_t)n_batch * kStages]));
+  double stage_tot[kStages] = {0};
   for (uint32_t bt = 0; bt < n_batch; bt++) {
-    float ms = 0.f, st_ms[5];
-    CUDA_TRY(cudaEventElapsedTime(&ms, h->events[bt * 5], h->events[(bt + 1) * 5]));
-    for (int k = 0; k < 5; k++)
-      CUDA_TRY(cudaEventElapsedTime(&st_ms[k], h->events[bt * 5 + k], h->events[bt * 5 + k + 1]));
+    float ms = 0.f, st_ms[kStages];
+    CUDA_TRY(cudaEventElapsedTime(&ms, ev(bt, 0), h->events[(size_t)(bt + 1) * kStages]));
+    for (int k = 0; k < kStages; k++) {
+      CUDA_TRY(cudaEventElapsedTime(&st_ms[k], ev(bt, k), h->events[(size_t)bt * kStages + k + 1]));
+      stage_tot[k] += st_ms[k];
+    }
     max_ms = std::max(max_ms, ms);
     const uint32_t s = bt * B, e = std::min(n_query, s + B);
     for (uint32_t i = s; i < e; i++) {
       if (query_time_s) query_time_s[i] = ms * 1e-3;
       if (stage_s)
-        for (int k = 0; k < 5; k++) stage_s[(size_t)i * 5 + k] = st_ms[k] * 1e-3;
+        for (int k = 0; k < kStages; k++) stage_s[(size_t)i * kStages + k] = st_ms[k] * 1e-3;
     }
   }
   if (stats) {
@@ -432,12 +484,7 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
       stats->n_list_ent += w.h_qstat[i * 3 + 1];
       stats->n_rerank_tok += w.h_qstat[i * 3 + 2];
     }
-    for (uint32_t bt = 0; bt < n_batch; bt++)
-      for (int k = 0; k < 5; k++) {
-        float ms = 0.f;
-        CUDA_TRY(cudaEventElapsedTime(&ms, h->events[bt * 5 + k], h->events[bt * 5 + k + 1]));
-        stats->stage_ms[k] += ms;
-      }
+    for (int k = 0; k < kStages; k++) stats->stage_ms[k] = stage_tot[k];
     stats->wall_s =
         std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
   }
@@ -458,6 +505,13 @@ int finish_index(mvr_index *h, const uint32_t *item_n_vec_host, const uint32_t *
   MVR_TRY(dalloc(&dl, lut.size(), &h->bufs));
   CUDA_TRY(cudaMemcpy(dl, lut.data(), lut.size() * sizeof(float), cudaMemcpyHostToDevice));
   d.lut = dl;
+  uint16_t *cb, *lb;
+  MVR_TRY(dalloc(&cb, (size_t)d.n_centroid * kDim, &h->bufs));
+  MVR_TRY(dalloc(&lb, lut.size(), &h->bufs));
+  CUDA_TRY(make_bf16(d.centroid, (size_t)d.n_centroid * kDim, cb, h->stream));
+  CUDA_TRY(make_bf16(dl, lut.size(), lb, h->stream));
+  h->cen_bf16 = cb;
+  h->lut_bf16 = lb;
   float *ct;
   MVR_TRY(dalloc(&ct, (size_t)kDim * d.n_centroid_pad, &h->bufs));
   CUDA_TRY(launch_transpose_centroid(d.centroid, d.n_centroid, d.n_centroid_pad, ct, h->stream));
@@ -508,7 +562,10 @@ int new_handle(int device, std::unique_ptr<mvr_index> &h) {
   CUDA_TRY(cudaSetDevice(device));
   CUDA_TRY(cudaDeviceGetAttribute(&h->n_sm, cudaDevAttrMultiProcessorCount, device));
   CUDA_TRY(configure_kernels());
+  CUDA_TRY(configure_tc_kernels());
   CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  MVR_TRY(dalloc(&h->d_err, 1));
+  CUDA_TRY(cudaMemset(h->d_err, 0, sizeof(unsigned)));
   return MVR_OK;
 }
 
@@ -720,6 +777,12 @@ int mvr_index_get_info(const mvr_index *h, mvr_index_info *info) {
 int mvr_index_set_batch(mvr_index *h, uint32_t max_batch_queries) {
   if (!h) return set_err(MVR_ERR_INVALID_ARG, "null index handle");
   h->batch_cap = max_batch_queries;
+  return MVR_OK;
+}
+
+int mvr_index_set_rescore(mvr_index *h, uint32_t n_rescore) {
+  if (!h) return set_err(MVR_ERR_INVALID_ARG, "null index handle");
+  h->rescore = n_rescore;
   return MVR_OK;
 }
 

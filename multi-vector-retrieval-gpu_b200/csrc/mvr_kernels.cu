@@ -550,10 +550,11 @@ __global__ void __launch_bounds__(512)
 topk_kernel(const uint32_t *__restrict__ short_id, const float *__restrict__ exact,
             const uint32_t *__restrict__ n_short, uint32_t probe_topk,
             uint32_t n_pad, uint32_t topk, float *__restrict__ out_s,
-            uint32_t *__restrict__ out_id) {
+            uint32_t *__restrict__ out_id, uint32_t *__restrict__ n_out) {
   extern __shared__ uint64_t keys[];
   const uint32_t b = blockIdx.x;
   const uint32_t n = n_short[b];
+  if (n_out && threadIdx.x == 0) n_out[b] = min(n, topk);
   for (uint32_t i = threadIdx.x; i < n_pad; i += blockDim.x)
     keys[i] = i < n ? make_key(exact[(size_t)b * probe_topk + i], short_id[(size_t)b * probe_topk + i]) : 0ull;
   __syncthreads();
@@ -670,11 +671,11 @@ cudaError_t launch_rerank(const DevIndex &ix, const float *q, const uint64_t *q_
 cudaError_t launch_topk(const uint32_t *short_id, const float *exact,
                         const uint32_t *n_short, uint32_t n_query,
                         uint32_t probe_topk, uint32_t topk, float *out_s,
-                        uint32_t *out_id, cudaStream_t st, int *n_launch) {
+                        uint32_t *out_id, uint32_t *n_out, cudaStream_t st, int *n_launch) {
   uint32_t n_pad = 1;
   while (n_pad < probe_topk) n_pad <<= 1;
   topk_kernel<<<n_query, 512, n_pad * sizeof(uint64_t), st>>>(short_id, exact, n_short, probe_topk,
-                                                            n_pad, topk, out_s, out_id);
+                                                            n_pad, topk, out_s, out_id, n_out);
   *n_launch += 1;
   return cudaGetLastError();
 }

@@ -38,6 +38,7 @@ cudaError_t launch_rerank(const DevIndex &ix, const float *q, const uint64_t *q_
 cudaError_t launch_topk(const uint32_t *short_id, const float *exact,
                         const uint32_t *n_short, uint32_t n_query,
                         uint32_t probe_topk, uint32_t topk, float *out_s,
-                        uint32_t *out_id, cudaStream_t st, int *n_launch);
+                        uint32_t *out_id, uint32_t *n_out /*nullable: min(n, topk)*/,
+                        cudaStream_t st, int *n_launch);
 
 }  // namespace mvr

@@ -18,12 +18,13 @@ MVR_ERR_OOM = 4
 MVR_ERR_UNSUPPORTED = 5
 MVR_SEM_PP = 0
 MVR_SEM_BASIC = 1
+MVR_PREC_BF16 = 2
 
 # every symbol include/mvr.h declares
 EXPORTS = (
     "mvr_last_error", "mvr_device_count", "mvr_index_load", "mvr_index_load_files",
     "mvr_index_from_arrays", "mvr_index_from_device_arrays", "mvr_index_free",
-    "mvr_index_get_info", "mvr_index_set_batch", "mvr_search", "mvr_search_staged",
+    "mvr_index_get_info", "mvr_index_set_batch", "mvr_index_set_rescore", "mvr_search", "mvr_search_staged",
     "mvr_search_device", "mvr_search_trace", "mvr_decompress", "mvr_unpack_buckets",
     "mvr_assign_device", "mvr_pack_residual_device", "mvr_kmeans_accumulate_device",
 )
@@ -47,7 +48,7 @@ class Stats(C.Structure):
                 ("n_batch", C.c_uint32), ("gpu_launches", C.c_uint32),
                 ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64),
                 ("n_cand_total", C.c_uint64), ("n_rerank_tok", C.c_uint64),
-                ("n_list_ent", C.c_uint64), ("stage_ms", C.c_double * 5)]
+                ("n_list_ent", C.c_uint64), ("stage_ms", C.c_double * 6)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_}
@@ -88,6 +89,7 @@ def lib():
         "mvr_index_free": [vp],
         "mvr_index_get_info": [vp, C.POINTER(IndexInfo)],
         "mvr_index_set_batch": [vp, u32],
+        "mvr_index_set_rescore": [vp, u32],
         "mvr_search": [vp, vp, vp, u32, u32, u32, u32, u32, u32, vp, vp, vp, C.POINTER(Stats)],
         "mvr_search_staged": [vp, vp, vp, u32, u32, u32, u32, u32, u32, vp, vp, vp, vp,
                               C.POINTER(Stats)],

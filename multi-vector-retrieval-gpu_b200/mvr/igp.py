@@ -60,8 +60,8 @@ class IGPGPUBasic(_Base):
             compute_time_l=st["query_time_s"], reset_time_l=zero,
             transmit_query_time_l=stg[:, 0], cand_gen_time_l=stg[:, 1], filter_time_l=stg[:, 2],
             filter_transmit_time_l=zero, filter_compute_time_l=stg[:, 2],
-            rerank_time_l=stg[:, 3] + stg[:, 4], rerank_transmit_time_l=stg[:, 4],
-            rerank_compute_time_l=stg[:, 3], n_query=n_query, topk=topk)
+            rerank_time_l=stg[:, 3] + stg[:, 4] + stg[:, 5], rerank_transmit_time_l=stg[:, 5],
+            rerank_compute_time_l=stg[:, 3] + stg[:, 4], n_query=n_query, topk=topk)
 
 
 class IGPGPUPP(_Base):

@@ -14,6 +14,7 @@ from ._lib import check, lib
 
 SEM_PP = _lib.MVR_SEM_PP
 SEM_BASIC = _lib.MVR_SEM_BASIC
+PREC_BF16 = _lib.MVR_PREC_BF16
 
 
 def _ptr(a):
@@ -112,6 +113,9 @@ class Index:
     def set_batch(self, max_batch_queries):
         check(lib().mvr_index_set_batch(self._h, max_batch_queries))
 
+    def set_rescore(self, n_rescore):
+        check(lib().mvr_index_set_rescore(self._h, n_rescore))
+
     # -- search ----------------------------------------------------------
     def search(self, queries, k, nprobe, probe_topk, tok_off=None, semantics=SEM_PP,
                with_stats=False, with_stages=False):
@@ -121,7 +125,7 @@ class Index:
         qtime = np.zeros(n_query, np.float64)
         st = _lib.Stats()
         if with_stages:
-            stages = np.zeros((n_query, 5), np.float64)
+            stages = np.zeros((n_query, 6), np.float64)
             check(lib().mvr_search_staged(self._h, _ptr(q), _ptr(off), n_query, n_vec, k, nprobe,
                                           probe_topk, semantics, _ptr(scores), _ptr(ids),
                                           _ptr(qtime), _ptr(stages), C.byref(st)))
@@ -138,12 +142,14 @@ class Index:
         return scores, ids, out
 
     def search_host_ptr(self, q_ptr, off, n_query, n_vec, k, nprobe, probe_topk, scores_ptr,
-                        ids_ptr, semantics=SEM_PP):
-        """Raw-pointer host search (e.g. pinned torch tensors); returns Stats."""
+                        ids_ptr, semantics=SEM_PP, qtime=None):
+        """Raw-pointer host search (e.g. pinned torch tensors); returns Stats.
+        qtime (float64 [n_query], optional) receives per-query batch latency."""
         st = _lib.Stats()
+        off = _c(off, np.uint64) if off is not None else None
         check(lib().mvr_search(self._h, C.c_void_p(q_ptr), _ptr(off), n_query, n_vec, k, nprobe,
                                probe_topk, semantics, C.c_void_p(scores_ptr),
-                               C.c_void_p(ids_ptr), None, C.byref(st)))
+                               C.c_void_p(ids_ptr), _ptr(qtime), C.byref(st)))
         return st
 
     def search_device(self, q_ptr, off, n_query, n_vec, k, nprobe, probe_topk, scores_ptr,

@@ -6,8 +6,13 @@ Generator: n_latent cluster means uniform on the unit sphere S^127; each doc
 draws 5..15 of them; doc lengths ~ lognormal with mean 70 / sd 35, rounded and
 clipped to [8, 180]; token = normalize(mu_c + 0.45 * N(0, I)) with c one of the
 doc's clusters; a query token = normalize(mu_c + 0.55 * N(0, I)) with c one of
-a random doc's clusters.  torch RNG on the requested device (CPU and CUDA
-streams differ but each is deterministic for a seed).
+a random doc's clusters.  The noise vector is N(0, I/128) scaled by 0.45
+(0.55): its expected norm is 0.45 (0.55), so a token keeps cos ~0.91 (~0.87)
+with its cluster mean.  (Per-dimension unit variance would give a noise norm
+of ~5.1 and cos ~0.19 with the mean, under which exact-MaxSim rankings are
+noise-dominated and no IVF method reaches meaningful recall.)  torch RNG on
+the requested device (CPU and CUDA streams differ but each is deterministic
+for a seed).
 """
 import math
 
@@ -61,7 +66,8 @@ def tokens(spec, device="cpu", noise=0.45, chunk=1 << 22, out=None):
         d = doc_of[s:e]
         slot = (torch.rand(e - s, device=dev, generator=gen) * doc_k[d]).long().clamp_max_(14)
         c = clusters[d, slot]
-        x = latent[c] + noise * torch.randn((e - s, DIM), device=dev, generator=gen)
+        x = latent[c] + (noise / math.sqrt(DIM)) * torch.randn((e - s, DIM), device=dev,
+                                                              generator=gen)
         out[s:e] = _normalize_(x)
     return out
 
@@ -86,5 +92,5 @@ def queries(spec, n_query, n_tok=32, device="cpu", noise=0.55, seed=1):
     dev = torch.device(device)
     gen = torch.Generator(device=dev).manual_seed(seed * 7 + spec.seed)
     x = torch.from_numpy(spec.latent[cl]).to(dev)
-    x = x + noise * torch.randn(x.shape, device=dev, generator=gen)
+    x = x + (noise / math.sqrt(DIM)) * torch.randn(x.shape, device=dev, generator=gen)
     return _normalize_(x).contiguous(), off

@@ -14,8 +14,12 @@ import pyoracle  # noqa: E402
 from mvr import synth  # noqa: E402
 
 
-def tiny_index(n_doc=300, n_centroid=64, n_bit=2, seed=0, len_hi=180, n_latent=200, len_lo=8):
-    spec = synth.CorpusSpec(n_doc, seed=seed, n_latent=n_latent, len_hi=len_hi, len_lo=len_lo)
+def tiny_index(n_doc=300, n_centroid=64, n_bit=2, seed=0, len_hi=180, n_latent=200, lengths=None):
+    spec = synth.CorpusSpec(n_doc, seed=seed, n_latent=n_latent, len_hi=len_hi)
+    if lengths is not None:  # explicit doc lengths (edge cases)
+        spec.item_n_vec = np.asarray(lengths, np.uint32)
+        spec.item_off = np.zeros(n_doc, np.uint64)
+        spec.item_off[1:] = np.cumsum(spec.item_n_vec[:-1], dtype=np.uint64)
     tok = synth.tokens(spec, "cpu").numpy()
     rng = np.random.default_rng(seed + 5)
     cen = tok[rng.choice(len(tok), n_centroid, replace=False)]

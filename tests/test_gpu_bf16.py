@@ -1,0 +1,94 @@
+"""Mixed-precision path (MVR_PREC_BF16): the BF16 tensor-core (tcgen05)
+MaxSim over the shortlist followed by the exact FP32 re-score of its best R
+docs.  Checked against the oracle: the BF16 scores lie within BF16 rounding
+of the exact FP32 MaxSim, every returned score is bit-identical to the
+oracle's FP32 MaxSim of that doc, and the top-k equals the plain path's
+wherever the plain path's exact ranking survives the BF16 pre-selection."""
+import numpy as np
+import pytest
+
+import pyoracle
+from helpers import make_queries, oracle_of, tiny_index
+from mvr import PREC_BF16, SEM_BASIC, SEM_PP, Index
+
+pytestmark = pytest.mark.gpu
+
+
+def gpu_index(ix):
+    return Index.from_arrays(ix["item_n_vec"], ix["centroid"], ix["vq_code"], ix["ivf_off"],
+                             ix["ivf_size"], ix["ivf_ids"], ix["weight"], ix["n_bit"],
+                             ix["residual"])
+
+
+@pytest.fixture(scope="module", params=[1, 2, 4, 8], ids=lambda b: f"b{b}")
+def pair(request):
+    ix = tiny_index(n_doc=500, n_centroid=96, n_bit=request.param, seed=10 + request.param)
+    g = gpu_index(ix)
+    yield ix, g, oracle_of(ix)
+    g.close()
+
+
+@pytest.mark.parametrize("sem", [SEM_PP, SEM_BASIC], ids=["pp", "basic"])
+def test_bf16_scores_close_to_exact(pair, sem):
+    ix, g, o = pair
+    q, off = make_queries(ix, 4, (8, 64), seed=31)
+    rel = []
+    for i in range(4):
+        qi = q[off[i]:off[i + 1]]
+        t = g.trace(qi, 10, 6, 200, sem | PREC_BF16)
+        r = o.search_one(qi, 10, 6, 200, sem)
+        np.testing.assert_array_equal(t["short_id"], np.sort(r["short_id"]))
+        exact = np.array([o.maxsim_item(qi, d, sem) for d in t["short_id"]])
+        err = np.abs(t["short_exact"] - exact) / np.maximum(np.abs(exact), 1e-3)
+        rel.append(err)
+        assert err.max() < 3e-2, err.max()
+    assert np.concatenate(rel).mean() < 5e-3
+
+
+@pytest.mark.parametrize("sem", [SEM_PP, SEM_BASIC], ids=["pp", "basic"])
+def test_bf16_topk_scores_are_exact_fp32(pair, sem):
+    ix, g, o = pair
+    q, off = make_queries(ix, 24, 32, seed=33)
+    s_bf, i_bf = g.search(q.reshape(24, 32, 128), 10, 6, 200, semantics=sem | PREC_BF16)
+    s_pl, i_pl = g.search(q.reshape(24, 32, 128), 10, 6, 200, semantics=sem)
+    same = 0
+    for k in range(24):
+        qk = q[off[k]:off[k + 1]]
+        for d, s in zip(i_bf[k], s_bf[k]):
+            if d != 0xFFFFFFFF:
+                assert s == o.maxsim_item(qk, d, sem)  # bit-exact FP32 re-score
+        same += np.array_equal(i_bf[k], i_pl[k])
+        # order is by exact score: (score desc, id asc)
+        assert all((s_bf[k][j] > s_bf[k][j + 1]) or
+                   (s_bf[k][j] == s_bf[k][j + 1] and i_bf[k][j] < i_bf[k][j + 1])
+                   for j in range(9))
+    assert same >= 22, same
+
+
+def test_bf16_rescore_width_and_batches(pair):
+    ix, g, o = pair
+    q, off = make_queries(ix, 30, (1, 64), seed=35)
+    ref_s, ref_i = g.search(q, 10, 4, 150, tok_off=off)
+    g.set_rescore(150)  # re-score the whole shortlist: identical to the plain path
+    g.set_batch(7)
+    s, i = g.search(q, 10, 4, 150, tok_off=off, semantics=PREC_BF16)
+    g.set_rescore(0)
+    g.set_batch(0)
+    np.testing.assert_array_equal(i, ref_i)
+    np.testing.assert_array_equal(s, ref_s)
+
+
+def test_bf16_small_shortlists():
+    lens = np.random.default_rng(1).integers(1, 20, 80)
+    ix = tiny_index(n_doc=80, n_centroid=30, n_bit=2, seed=5, lengths=lens)
+    g, o = gpu_index(ix), oracle_of(ix)
+    q, off = make_queries(ix, 5, 32, seed=2)
+    for i in range(5):
+        qi = q[off[i]:off[i + 1]]
+        for nq in (1, 32):
+            t = g.trace(qi[:nq], 10, 1, 12, PREC_BF16)
+            r = o.search_one(qi[:nq], 10, 1, 12)
+            assert len(t["short_id"]) == len(r["short_id"])
+            ok = t["id"] != 0xFFFFFFFF
+            assert ok.sum() == min(10, len(r["short_id"]))
+    g.close()

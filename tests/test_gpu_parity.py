@@ -18,6 +18,18 @@ TOL = 1e-5
 GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "codec_*d128.npz")))
 
 
+def with_orphan_centroids(ix, n_orphan):
+    """Appends centroids that no token is closest to (negated copies), so
+    their IVF lists are empty, and rebuilds codes / residuals / lists."""
+    cen = np.concatenate([ix["centroid"], -ix["centroid"][np.arange(n_orphan) % len(ix["centroid"])]])
+    code = pyoracle.assign(ix["tokens"], cen)
+    cut, w = pyoracle.quantize(ix["tokens"], cen, code, ix["n_bit"])
+    res = pyoracle.pack_residual(ix["tokens"], cen, code, cut, ix["n_bit"])
+    off, size, ids = pyoracle.ivf_build(code, ix["item_n_vec"], len(cen))
+    return dict(ix, centroid=cen, vq_code=code, weight=w, residual=res, ivf_off=off,
+                ivf_size=size, ivf_ids=ids)
+
+
 def gpu_index(ix):
     return Index.from_arrays(ix["item_n_vec"], ix["centroid"], ix["vq_code"], ix["ivf_off"],
                              ix["ivf_size"], ix["ivf_ids"], ix["weight"], ix["n_bit"],
@@ -108,9 +120,11 @@ def test_exact_scores_within_fp64_tolerance(pair):
 
 
 def test_edge_cases():
-    ix = tiny_index(n_doc=60, n_centroid=40, n_bit=2, seed=7, len_hi=12, len_lo=1)
+    lens = np.random.default_rng(3).integers(1, 13, 60)
+    lens[:3] = 1  # single-token docs
+    ix = tiny_index(n_doc=60, n_centroid=40, n_bit=2, seed=7, lengths=lens)
     g, o = gpu_index(ix), oracle_of(ix)
-    assert ix["item_n_vec"].min() <= 2
+    assert ix["item_n_vec"].min() == 1
     q, off = make_queries(ix, 3, 64, seed=3)
     cases = [dict(k=5, nprobe=32, ptk=5),       # nprobe = max, topk = probe_topk
              dict(k=10, nprobe=1, ptk=8000),    # shortlist larger than candidate set
@@ -125,6 +139,15 @@ def test_edge_cases():
     pad = r["id"] == 0xFFFFFFFF
     assert np.all(np.isneginf(r["score"][pad]))
     g.close()
+    # 80 orphan centroids own no token: empty IVF lists get probed
+    ix2 = with_orphan_centroids(tiny_index(n_doc=60, n_centroid=20, n_bit=4, seed=8,
+                                           lengths=lens), 80)
+    assert (ix2["ivf_size"] == 0).sum() >= 40
+    g2, o2 = gpu_index(ix2), oracle_of(ix2)
+    for i in range(3):
+        qi = q[off[i]:off[i + 1]]
+        compare_trace(g2.trace(qi, 10, 32, 40), o2.search_one(qi, 10, 32, 40))
+    g2.close()
 
 
 def test_invalid_arguments_rejected(pair):

@@ -1,0 +1,65 @@
+"""Host-side logic on the CPU: synthetic generator statistics, the GPU
+builder's pure-host helpers (sample selection, centroid-count formula, exact
+order statistics by bisection, IVF build), and the exhaustive ground truth
+(torch, CPU tensors here) against the oracle's FP64 exhaustive MaxSim."""
+import numpy as np
+import torch
+
+import pyoracle
+from helpers import tiny_index
+from mvr import build, exhaustive, synth
+
+
+def test_generator_shapes_and_stats():
+    spec = synth.CorpusSpec(2000, seed=3)
+    assert spec.item_n_vec.min() >= 8 and spec.item_n_vec.max() <= 180
+    assert 60 < spec.item_n_vec.mean() < 80
+    tok = synth.tokens(spec, "cpu")
+    assert tok.shape == (spec.n_vec, 128)
+    np.testing.assert_allclose(torch.linalg.vector_norm(tok, dim=1).numpy(), 1.0, atol=1e-5)
+    q, off = synth.queries(spec, 10, (8, 32), "cpu", seed=2)
+    assert len(off) == 11 and q.shape[0] == off[-1]
+    assert all(8 <= d <= 32 for d in np.diff(off))
+    tok2 = synth.tokens(spec, "cpu")
+    assert torch.equal(tok, tok2)  # deterministic
+
+
+def test_sample_and_centroid_formula():
+    assert build.n_centroid_default(700_000) == 8192
+    assert build.n_centroid_default(70_000_000) == 131072
+    s = build.sample_items(10_000)
+    assert len(s) == min(1 + int(8 * np.sqrt(120 * 10_000)), 10_000)
+    assert s == sorted(set(s))
+
+
+def test_order_statistics_exact():
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal(100_001).astype(np.float32)
+    x[::7] = 0.25  # ties
+    x[::11] = -0.0
+    keys = build._ord_keys(torch.from_numpy(x))
+    srt = np.sort(x)
+    for r in (0, 1, 500, 50_000, 99_999, 100_000):
+        assert build.order_statistic(keys, r) == srt[r]
+    cut, w = build.quantize_params(torch.from_numpy(x), 2)
+    nq = 4
+    np.testing.assert_array_equal(cut, [srt[int(np.floor((i + 1) / nq * len(x)))] for i in range(3)])
+
+
+def test_ivf_build_torch_matches_oracle():
+    ix = tiny_index(n_doc=150, n_centroid=50, seed=2)
+    off, size, ids = build.ivf_build(torch.from_numpy(ix["vq_code"].astype(np.int32)),
+                                     ix["item_n_vec"], 50)
+    np.testing.assert_array_equal(off.numpy(), ix["ivf_off"])
+    np.testing.assert_array_equal(size.numpy(), ix["ivf_size"])
+    np.testing.assert_array_equal(ids.numpy().view(np.uint32), ix["ivf_ids"])
+
+
+def test_exhaustive_topk_matches_oracle_f64():
+    ix = tiny_index(n_doc=120, n_centroid=16, seed=4)
+    q, off = synth.queries(ix["spec"], 3, 12, "cpu", seed=9)
+    s, i = exhaustive.exhaustive_topk(q, off, torch.from_numpy(ix["tokens"]), ix["item_n_vec"], 7,
+                                      chunk_tokens=300)
+    rs, ri = pyoracle.exhaustive_f64(q.numpy(), off, ix["tokens"], ix["item_n_vec"], 7)
+    np.testing.assert_array_equal(i, ri)
+    np.testing.assert_allclose(s, rs, rtol=1e-12)
