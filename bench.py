@@ -247,6 +247,7 @@ def main():
     ap.add_argument("--impl", choices=["mvr", "reference"], default="mvr")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="medium")
     ap.add_argument("--probe-topk", type=int, default=None)
+    ap.add_argument("--rescore", type=int, default=0, help="FP32 re-score width (0: 4*k)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--recall-sweep", default="",
                     help="extra nprobe:probe_topk settings whose recall@k is reported, "
@@ -260,6 +261,7 @@ def main():
 
     import torch
     import torch.distributed as dist
+    from mvr import PREC_BF16, exhaustive, formats, synth
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -269,30 +271,32 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(minutes=20))
 
-    from mvr import exhaustive, formats, synth
     spec, host, tok, built_s = get_index(w, dev, rank, want_tokens=(rank == 0))
     g = load_gpu_index(host, local)
+    g.set_rescore(args.rescore)
     q, off = synth.queries(spec, w["n_query"], w["n_tok"], dev, seed=100 + rank)
     n_query, T = w["n_query"], q.shape[0]
     k, nprobe, ptk = w["topk"], w["nprobe"], w["probe_topk"]
     stream = torch.cuda.current_stream()
     out_s = torch.empty((n_query, k), dtype=torch.float32, device=dev)
     out_i = torch.empty((n_query, k), dtype=torch.int32, device=dev)
+    FAST, PLAIN = PREC_BF16, 0
 
-    def step():
+    def step(flags):
         return g.search_device(q.data_ptr(), None, n_query, w["n_tok"], k, nprobe, ptk,
-                               out_s.data_ptr(), out_i.data_ptr(), stream.cuda_stream)
+                               out_s.data_ptr(), out_i.data_ptr(), stream.cuda_stream,
+                               semantics=flags)
 
-    # recall@10 against exhaustive FP64 MaxSim over the raw tokens (rank 0)
-    recall = None
-    sweep = {}
+    # recall@k against exhaustive FP64 MaxSim over the raw tokens (rank 0)
+    recall, sweep = {}, {}
     if rank == 0:
-        step()
         n_gt = w["n_gt"]
         qg = q[: n_gt * w["n_tok"]]
         gs, gi = exhaustive.exhaustive_topk(qg, off[: n_gt + 1], tok, spec.item_n_vec, k)
-        est = out_i[:n_gt].cpu().numpy().view(np.uint32)
-        recall = float(formats.recall_at_k(gi, est, k).mean())
+        for name, fl in (("bf16", FAST), ("plain", PLAIN)):
+            step(fl)
+            est = out_i[:n_gt].cpu().numpy().view(np.uint32)
+            recall[name] = float(formats.recall_at_k(gi, est, k).mean())
         qg_np = qg.cpu().numpy()
         for item in filter(None, args.recall_sweep.split(",")):
             npb, ptk_s = (int(x) for x in item.split(":"))
@@ -302,35 +306,41 @@ def main():
         torch.cuda.empty_cache()
 
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in range(args.steps)]
-    stage = np.zeros(5)
-    launches = n_cand = n_tok_rr = n_ent = 0
-    with ClockSampler(local) as clk:
+
+    def measure(flags, clk=None):
+        for _ in range(args.warmup):
+            step(flags)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(args.steps)]
+        acc = dict(stage=np.zeros(6), launches=0, n_cand=0, n_tok=0, n_ent=0)
         for s in range(args.steps):
             flush.fill_(s & 0xFF)
             ev[s][0].record(stream)
-            st = step()
+            st = step(flags)
             ev[s][1].record(stream)
-            stage += np.asarray(list(st.stage_ms))
-            launches += st.gpu_launches
-            n_cand += st.n_cand_total
-            n_tok_rr += st.n_rerank_tok
-            n_ent += st.n_list_ent
+            acc["stage"] += np.asarray(list(st.stage_ms))
+            acc["launches"] += st.gpu_launches
+            acc["n_cand"] += st.n_cand_total
+            acc["n_tok"] += st.n_rerank_tok
+            acc["n_ent"] += st.n_list_ent
         torch.cuda.synchronize()
-    step_ms = [a.elapsed_time(b) for a, b in ev]
-    total_ms = float(sum(step_ms))
-    if world > 1:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-        dist.barrier()
-    value = world * n_query * args.steps / (total_ms / 1e3)
+        total_ms = float(sum(a.elapsed_time(b) for a, b in ev))
+        if world > 1:
+            t = torch.tensor([total_ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            total_ms = float(t.item())
+            dist.barrier()
+        acc["total_ms"] = total_ms
+        acc["qps"] = world * n_query * args.steps / (total_ms / 1e3)
+        return acc
+
+    plain = measure(PLAIN)
+    with ClockSampler(local) as clk:
+        fast = measure(FAST)
+    value = fast["qps"]
 
     # end to end: pinned host buffers, copies inside every step
     hq = q.cpu().pin_memory()
@@ -342,7 +352,7 @@ def main():
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         st_e = g.search_host_ptr(hq.data_ptr(), None, n_query, w["n_tok"], k, nprobe, ptk,
-                                 hs.data_ptr(), hi.data_ptr(), qtime=qtime)
+                                 hs.data_ptr(), hi.data_ptr(), semantics=FAST, qtime=qtime)
         if s >= args.warmup:
             e2e_dt.append(time.perf_counter() - t0)
     e2e_s = float(sum(e2e_dt))
@@ -357,30 +367,33 @@ def main():
         dist.destroy_process_group()
         return
 
-    # roofline of the dominant stage (stage_ms: copy, probe, filter, rerank+topk, copy)
+    # roofline of the dominant stage of the headline (mixed-precision) path;
+    # stage_ms: 0 query copy, 1 probe, 2 filter, 3 rerank, 4 re-score+top-k, 5 copy
     pk = peaks()
     S = args.steps
     C, D = w["n_centroid"], 128
     bpv = D * w["n_bit"] // 8
+    stage = fast["stage"]
     probe_flop = 2.0 * T * C * D * S
-    rerank_flop = 2.0 * w["n_tok"] * D * n_tok_rr
-    rerank_bytes = (4.0 + bpv) * n_tok_rr
-    filter_bytes = 4.0 * n_ent + (4 + 32 + 8) * n_cand
+    rerank_flop = 2.0 * w["n_tok"] * D * fast["n_tok"]
+    rerank_bytes = (4.0 + bpv) * fast["n_tok"]
+    filter_bytes = 4.0 * fast["n_ent"] + (4 + 32 + 8) * fast["n_cand"]
     kern = {1: ("probe_topk_kernel", "tensor", probe_flop / 1e12, pk["tc_sus"], "TFLOP/s"),
             2: ("filter_kernel", "hbm", filter_bytes / 1e9, pk["hbm"], "GB/s"),
-            3: ("rerank_kernel", "tensor", rerank_flop / 1e12, pk["tc_sus"], "TFLOP/s")}
+            3: ("rerank_tc_kernel", "tensor", rerank_flop / 1e12, pk["tc_sus"], "TFLOP/s")}
     dom = max((1, 2, 3), key=lambda i: stage[i])
     name, bound, work, peak, unit = kern[dom]
     achieved = work / (stage[dom] / 1e3)
+    names = ("query_copy", "probe", "filter", "rerank", "rescore_topk", "result_copy")
     roof = {"kernel": name, "bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
             "frac": achieved / peak, "traffic": None,
             "peak_source": f"{pk['src']} ({'bf16 sustained' if bound == 'tensor' else 'HBM copy'})",
-            "stage_share": {n: float(stage[i] / stage.sum()) for i, n in
-                            ((0, "query_copy"), (1, "probe"), (2, "filter"), (3, "rerank_topk"),
-                             (4, "result_copy"))},
+            "stage_share": {n: float(stage[i] / stage.sum()) for i, n in enumerate(names)},
             "per_stage": {kern[i][0]: {"ms_per_step": float(stage[i] / S),
                                        "achieved": kern[i][2] / (stage[i] / 1e3),
-                                       "unit": kern[i][4]} for i in (1, 2, 3)}}
+                                       "unit": kern[i][4]} for i in (1, 2, 3)},
+            "rerank_tc_hbm_gbs": rerank_bytes / 1e9 / (stage[3] / 1e3),
+            "rescore_topk_ms_per_step": float(stage[4] / S)}
 
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
@@ -388,24 +401,28 @@ def main():
         cpu = {"value": qps_cpu, "unit": "queries/s", "cores": os.cpu_count(), "kind": "port",
                "sample": f"first {n_s} of the {n_query} queries ({dt_s:.1f} s)"}
 
+    R = args.rescore or 4 * k
     line = {
         "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": S,
-        "warmup": args.warmup, "ms_per_step": total_ms / S, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": dict(workload_config(w, "plain FP32 CUDA path"),
-                       **{"recall@10": recall, "recall_queries": w["n_gt"],
-                          "recall_sweep": sweep,
+        "warmup": args.warmup, "ms_per_step": fast["total_ms"] / S, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "bf16", "data": "synthetic",
+        "config": dict(workload_config(w, "BF16 tensor-core MaxSim + FP32 re-score"),
+                       **{"rescore": R, "recall@10": recall.get("bf16"),
+                          "recall@10_plain": recall.get("plain"), "recall_queries": w["n_gt"],
+                          "recall_sweep_plain": sweep, "plain_fp32_qps": plain["qps"],
+                          "speedup_vs_plain": value / plain["qps"],
+                          "plain_stage_ms_per_step": [float(x / S) for x in plain["stage"]],
                           "p50_ms": p50, "p99_ms": p99, "latency": "per query = its batch's "
                           "device latency incl. copies (e2e run)",
                           "parallelism": f"replica x{world}, queries split by rank",
-                          "index_build_s": built_s, "cand_per_query": n_cand / (S * n_query),
-                          "rerank_tok_per_query": n_tok_rr / (S * n_query)}),
+                          "index_build_s": built_s, "cand_per_query": fast["n_cand"] / (S * n_query),
+                          "rerank_tok_per_query": fast["n_tok"] / (S * n_query)}),
         "e2e": {"value": e2e, "unit": "queries/s",
                 "h2d_bytes_per_step": int(st_e.h2d_bytes), "d2h_bytes_per_step": int(st_e.d2h_bytes)},
         "roofline": roof,
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
-        "gpu_launches": int(launches),
+        "gpu_launches": int(fast["launches"]),
         "p99_ms": p99,
     }
     print(json.dumps(line))
