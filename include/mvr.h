@@ -197,6 +197,29 @@ int mvr_search_trace(mvr_index *h, const float *query, uint32_t nq,
                      uint32_t topk, uint32_t nprobe, uint32_t probe_topk,
                      uint32_t flags, mvr_trace *trace);
 
+/* Candidate filter for ONE query with no device allocation in the call: the
+ * probe lists -> candidate set -> approximate scores -> top-probe_topk
+ * shortlist stage of mvr_search, its scratch held in a fixed array compiled
+ * into libmvr (about 11 MB on every GPU that loads the library, kept until
+ * the process exits).  No counterpart in the reference: it is for callers
+ * that cannot allocate device memory while serving (a plugin inside a host
+ * whose GPU memory is all reserved by the host's own pool allocator, or a
+ * latency-critical caller that cannot afford cudaMalloc's implicit device
+ * synchronisation).  Inputs and outputs are the caller's DEVICE buffers:
+ * d_probe_id / d_probe_score [nq*nprobe], the token-major probe lists sorted
+ * best-first as mvr_search_trace returns them; d_short_id /
+ * d_short_approx [probe_topk] (unordered) and d_n_short [1].  Limits:
+ * index of at most 262,144 docs, 1..32 query tokens; larger sizes fail with
+ * MVR_ERR_INVALID_ARG.  Runs asynchronously on cuda_stream.  All calls on a
+ * device share the array: calls whose GPU work overlaps race -- serialise
+ * them.  The first call on a device does the one-time set-up (looks up the
+ * array's device address); make it before any stream capture. */
+int mvr_filter_noalloc(mvr_index *h, const uint32_t *d_probe_id,
+                       const float *d_probe_score, uint32_t nq,
+                       uint32_t nprobe, uint32_t probe_topk,
+                       uint32_t *d_short_id, float *d_short_approx,
+                       uint32_t *d_n_short, void *cuda_stream);
+
 /* Decompressed token vectors x = centroid[code] + W[bucket] for the given
  * global token ids (host in/out, out: float32 [n, dim]); the decoder of
  * decompressAndAddResidual (RerankPP.hpp:65-113). */

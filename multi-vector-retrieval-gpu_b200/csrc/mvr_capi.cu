@@ -658,6 +658,17 @@ bool npy_u32(const NpyArray &a, std::vector<uint32_t> &out) {
 
 }  // namespace
 
+// Read access to a handle's device and HBM-resident index arrays for other
+// translation units of the library (not part of the C ABI).
+namespace mvr {
+const DevIndex *handle_index(const mvr_index *h, int *device) {
+  if (device) *device = h->device;
+  return &h->dix;
+}
+// Sets the calling thread's mvr_last_error() text; returns code.
+int record_error(int code, const char *msg) { return set_err(code, "%s", msg); }
+}  // namespace mvr
+
 // ----------------------------------------------------------------------
 // C ABI
 // ----------------------------------------------------------------------
