@@ -262,6 +262,7 @@ def main():
     import torch
     import torch.distributed as dist
     from mvr import PREC_BF16, exhaustive, formats, synth
+    from mvr import dist as mdist
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -327,11 +328,8 @@ def main():
             acc["n_tok"] += st.n_rerank_tok
             acc["n_ent"] += st.n_list_ent
         torch.cuda.synchronize()
-        total_ms = float(sum(a.elapsed_time(b) for a, b in ev))
+        total_ms = mdist.max_over_ranks(sum(a.elapsed_time(b) for a, b in ev), dev)
         if world > 1:
-            t = torch.tensor([total_ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            total_ms = float(t.item())
             dist.barrier()
         acc["total_ms"] = total_ms
         acc["qps"] = world * n_query * args.steps / (total_ms / 1e3)
@@ -355,11 +353,7 @@ def main():
                                  hs.data_ptr(), hi.data_ptr(), semantics=FAST, qtime=qtime)
         if s >= args.warmup:
             e2e_dt.append(time.perf_counter() - t0)
-    e2e_s = float(sum(e2e_dt))
-    if world > 1:
-        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = mdist.max_over_ranks(sum(e2e_dt), dev)
     e2e = world * n_query * args.steps / e2e_s
     p50, p99 = (float(np.percentile(qtime, p)) * 1e3 for p in (50, 99))
 

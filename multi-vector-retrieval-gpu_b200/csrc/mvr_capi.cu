@@ -116,6 +116,8 @@ struct Workspace {
   float *short_approx = nullptr, *exact = nullptr;
   float *out_s = nullptr;
   uint32_t *out_id = nullptr;
+  size_t cand_cap = 0;            // tensor-core probe candidates (BF16 path)
+  uint32_t *cand = nullptr;
   uint32_t r_cap = 0;             // FP32 re-score of the top-R (BF16 path)
   uint32_t *r_id = nullptr, *n_r = nullptr;
   float *r_score = nullptr, *r_exact = nullptr;
@@ -141,6 +143,7 @@ struct mvr_index {
   uint32_t epoch = 0;
   void *cen_bf16 = nullptr;      // [C][128] BF16 centroid rows
   void *lut_bf16 = nullptr;      // [256][8/b] BF16 decode table
+  void *cen_sw = nullptr;        // [C_pad/128][32 KB] swizzled BF16 centroid tiles
   unsigned *d_err = nullptr;     // device error flags of the tensor-core kernels
   Workspace ws;
 
@@ -167,8 +170,11 @@ struct mvr_index {
     for (void *p : {(void *)ws.q, (void *)ws.probe_id, (void *)ws.part_id, (void *)ws.probe_s,
                     (void *)ws.part_s, (void *)ws.short_id, (void *)ws.n_short,
                     (void *)ws.short_approx, (void *)ws.exact, (void *)ws.out_s, (void *)ws.out_id,
-                    (void *)ws.r_id, (void *)ws.n_r, (void *)ws.r_score, (void *)ws.r_exact})
+                    (void *)ws.r_id, (void *)ws.n_r, (void *)ws.r_score, (void *)ws.r_exact,
+                    (void *)ws.cand})
       dfree(p);
+    ws.cand = nullptr;
+    ws.cand_cap = 0;
     ws.r_id = ws.n_r = nullptr;
     ws.r_score = ws.r_exact = nullptr;
     ws.r_cap = 0;
@@ -210,13 +216,15 @@ int ensure_scratch(mvr_index *h, uint32_t slots, uint32_t rank_stride) {
 }
 
 int ensure_batch(mvr_index *h, uint32_t slots, uint32_t tok_cap, uint32_t nprobe,
-                 uint32_t short_cap, uint32_t topk, size_t part_need, uint32_t r_cap) {
+                 uint32_t short_cap, uint32_t topk, size_t part_need, uint32_t r_cap,
+                 size_t cand_need) {
   Workspace &w = h->ws;
   if (w.batch_slots >= slots && w.tok_cap >= tok_cap && w.np_cap >= nprobe &&
       w.short_cap >= short_cap && w.topk_cap >= topk && w.part_cap >= part_need &&
-      w.r_cap >= r_cap)
+      w.r_cap >= r_cap && w.cand_cap >= cand_need)
     return MVR_OK;
   r_cap = std::max(r_cap, w.r_cap);
+  cand_need = std::max(cand_need, w.cand_cap);
   const uint32_t s = std::max(slots, w.batch_slots);
   tok_cap = std::max(tok_cap, w.tok_cap);
   nprobe = std::max(nprobe, w.np_cap);
@@ -239,6 +247,8 @@ int ensure_batch(mvr_index *h, uint32_t slots, uint32_t tok_cap, uint32_t nprobe
   MVR_TRY(dalloc(&w.r_score, (size_t)s * r_cap));
   MVR_TRY(dalloc(&w.r_exact, (size_t)s * r_cap));
   MVR_TRY(dalloc(&w.n_r, (size_t)s));
+  MVR_TRY(dalloc(&w.cand, cand_need));
+  w.cand_cap = cand_need;
   w.r_cap = r_cap;
   w.batch_slots = s;
   w.tok_cap = tok_cap;
@@ -358,17 +368,23 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
   const uint32_t B = h->batch_cap ? h->batch_cap : default_batch(h);
   const uint32_t n_batch = (n_query + B - 1) / B;
   uint32_t tok_cap = 0;
-  size_t part_need = 1;
+  size_t part_need = 1, cand_need = 1;
+  const bool tc_probe = bf16 && nprobe <= 16;  // tensor-core scoring + exact re-score
+  const uint32_t n_ctile = h->dix.n_centroid_pad / 128;
   for (uint32_t bt = 0; bt < n_batch; bt++) {
     const uint32_t s = bt * B, e = std::min(n_query, s + B);
     const uint32_t T = (uint32_t)(off[e] - off[s]);
     tok_cap = std::max(tok_cap, T);
     int sp;
     part_need = std::max(part_need, part_entries(h, T, nprobe, &sp));
+    uint32_t tsp;
+    if (tc_probe)
+      cand_need = std::max(cand_need, (size_t)T * probe_tc_cand_per_token(T, n_ctile, h->n_sm, &tsp));
   }
   const uint32_t rank_stride = nq_max <= 32 ? 32u : 64u;
   MVR_TRY(ensure_scratch(h, std::min(B, n_query), rank_stride));
-  MVR_TRY(ensure_batch(h, std::min(B, n_query), tok_cap, nprobe, probe_topk, topk, part_need, R));
+  MVR_TRY(ensure_batch(h, std::min(B, n_query), tok_cap, nprobe, probe_topk, topk, part_need, R,
+                       cand_need));
   MVR_TRY(ensure_call(h, (size_t)n_query + n_batch, (size_t)n_query * 3,
                       (size_t)kStages * n_batch + 1));
   Workspace &w = h->ws;
@@ -400,10 +416,17 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
       qp = query + off[s] * kDim;
     }
     CUDA_TRY(cudaEventRecord(ev(bt, 1), st));
-    int splits;
-    part_entries(h, T, nprobe, &splits);
-    CUDA_TRY(launch_probe(h->dix, qp, T, nprobe, splits, w.part_id, w.part_s, w.probe_id,
-                          w.probe_s, st, &launches));
+    if (tc_probe) {
+      uint32_t tsp;
+      probe_tc_cand_per_token(T, n_ctile, h->n_sm, &tsp);
+      CUDA_TRY(launch_probe_tc(qp, T, h->cen_sw, h->dix.centroid, h->dix.n_centroid, nprobe, tsp,
+                               w.cand, w.probe_id, w.probe_s, h->d_err, st, &launches));
+    } else {
+      int splits;
+      part_entries(h, T, nprobe, &splits);
+      CUDA_TRY(launch_probe(h->dix, qp, T, nprobe, splits, w.part_id, w.part_s, w.probe_id,
+                            w.probe_s, st, &launches));
+    }
     CUDA_TRY(cudaEventRecord(ev(bt, 2), st));
     if (++h->epoch == 0) {  // stamps wrapped: clear them
       CUDA_TRY(cudaMemsetAsync(w.stamp, 0, (size_t)w.slots * h->dix.n_item * sizeof(uint32_t), st));
@@ -419,7 +442,8 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
       // BF16 tensor-core MaxSim over the whole shortlist, then the exact FP32
       // kernel re-scores its best R docs
       CUDA_TRY(launch_rerank_tc(h->dix, h->cen_bf16, h->lut_bf16, qp, qo, nb, w.short_id,
-                                w.n_short, probe_topk, sem, w.exact, h->d_err, st, &launches));
+                                w.n_short, probe_topk, sem, nq_max, w.exact, h->d_err, st,
+                                &launches));
       CUDA_TRY(cudaEventRecord(ev(bt, 4), st));
       CUDA_TRY(launch_topk(w.short_id, w.exact, w.n_short, nb, probe_topk, R, w.r_score, w.r_id,
                            w.n_r, st, &launches));
@@ -450,7 +474,8 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
   CUDA_TRY(cudaGetLastError());
   if (herr) {
     CUDA_TRY(cudaMemset(h->d_err, 0, sizeof(unsigned)));
-    return set_err(MVR_ERR_CUDA, "tensor-core rerank: an MMA completion wait timed out");
+    return set_err(MVR_ERR_CUDA, "tensor-core %s: a completion wait timed out",
+                   (herr & 2u) ? "centroid scoring" : "rerank");
   }
 
   float total_ms = 0.f, max_ms = 0.f;
@@ -512,6 +537,10 @@ int finish_index(mvr_index *h, const uint32_t *item_n_vec_host, const uint32_t *
   CUDA_TRY(make_bf16(dl, lut.size(), lb, h->stream));
   h->cen_bf16 = cb;
   h->lut_bf16 = lb;
+  uint8_t *sw;
+  MVR_TRY(dalloc(&sw, (size_t)d.n_centroid_pad * 256, &h->bufs));
+  CUDA_TRY(make_centroid_tiles(d.centroid, d.n_centroid, d.n_centroid_pad / 128, sw, h->stream));
+  h->cen_sw = sw;
   float *ct;
   MVR_TRY(dalloc(&ct, (size_t)kDim * d.n_centroid_pad, &h->bufs));
   CUDA_TRY(launch_transpose_centroid(d.centroid, d.n_centroid, d.n_centroid_pad, ct, h->stream));

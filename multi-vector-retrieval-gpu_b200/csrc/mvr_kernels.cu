@@ -247,6 +247,8 @@ filter_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
   __shared__ float ps[kMaxQueryTok * kMaxProbe];
   __shared__ uint32_t pid[kMaxQueryTok * kMaxProbe];
   __shared__ uint32_t pref[kMaxQueryTok + 1];
+  __shared__ uint32_t lsz[kMaxQueryTok * kMaxProbe];
+  __shared__ uint64_t lof[kMaxQueryTok * kMaxProbe];
   __shared__ uint32_t hist[256];
   __shared__ uint32_t s_ncand, s_sel, s_digit, s_need, s_done, s_entries, s_stok;
 
@@ -266,32 +268,60 @@ filter_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
   if (tid == 0) { s_ncand = 0; s_entries = 0; s_stok = 0; }
   __syncthreads();
 
+  // list sizes / offsets of every probe (probe id 0xffffffff = no finite score)
+  for (uint32_t i = tid; i < nq * nprobe; i += blockDim.x) {
+    const uint32_t c = pid[i];
+    lsz[i] = c < ix.n_centroid ? ix.ivf_size[c] : 0u;
+    lof[i] = c < ix.n_centroid ? ix.ivf_off[c] : 0ull;
+  }
+  __syncthreads();
+
   // ---- phase A: scatter probed lists rank by rank ----
   for (uint32_t j = 0; j < nprobe; j++) {
-    if (tid == 0) {
-      uint32_t acc = 0;
-      for (uint32_t t = 0; t < nq; t++) {
-        pref[t] = acc;
-        const uint32_t c = pid[t * nprobe + j];  // 0xffffffff if no finite score
-        acc += c < ix.n_centroid ? ix.ivf_size[c] : 0u;
+    if (warp == 0) {  // exclusive prefix of the nq list sizes of rank j
+      const uint32_t s0 = (uint32_t)lane < nq ? lsz[lane * nprobe + j] : 0u;
+      const uint32_t s1 = (uint32_t)lane + 32 < nq ? lsz[(lane + 32) * nprobe + j] : 0u;
+      uint32_t i0 = s0, i1 = s1;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v0 = __shfl_up_sync(kFull, i0, o), v1 = __shfl_up_sync(kFull, i1, o);
+        if (lane >= o) { i0 += v0; i1 += v1; }
       }
-      pref[nq] = acc;
-      s_entries += acc;
+      const uint32_t tot0 = __shfl_sync(kFull, i0, 31);
+      if ((uint32_t)lane < nq) pref[lane] = i0 - s0;
+      if ((uint32_t)lane + 32 < nq) pref[lane + 32] = tot0 + i1 - s1;
+      if (lane == 31) {
+        const uint32_t total = tot0 + i1;
+        pref[nq] = total;
+        s_entries += total;
+      }
     }
     __syncthreads();
     const uint32_t total = pref[nq];
-    for (uint32_t e0 = warp * 32; e0 < total; e0 += n_warp * 32) {
-      const uint32_t e = e0 + lane;
-      if (e < total) {
-        const uint32_t t = find_seg(pref, (int)nq, e);
-        const uint32_t c = pid[t * nprobe + j];
-        const uint32_t item = ix.ivf_ids[ix.ivf_off[c] + (e - pref[t])];
-        uint8_t *r = rank + (size_t)item * scr.rank_stride + t;
-        if (*r == 0xff) {
-          *r = (uint8_t)j;
-          if (atomicExch(stamp + item, epoch) != epoch) {
+    // 4 entries per lane in flight: independent list-id and rank-byte loads
+    for (uint32_t e0 = warp * 128; e0 < total; e0 += n_warp * 128) {
+      uint32_t item[4], tt[4];
+      uint8_t rv[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const uint32_t e = e0 + u * 32 + lane;
+        tt[u] = 0xffffffffu;
+        if (e < total) {
+          const uint32_t t = find_seg(pref, (int)nq, e);
+          tt[u] = t;
+          item[u] = ix.ivf_ids[lof[t * nprobe + j] + (e - pref[t])];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+        if (tt[u] != 0xffffffffu) rv[u] = rank[(size_t)item[u] * scr.rank_stride + tt[u]];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        if (tt[u] != 0xffffffffu && rv[u] == 0xff) {
+          rank[(size_t)item[u] * scr.rank_stride + tt[u]] = (uint8_t)j;
+          if (atomicExch(stamp + item[u], epoch) != epoch) {
             const uint32_t pos = atomicAdd(&s_ncand, 1u);
-            key[pos] = item;
+            key[pos] = item[u];
           }
         }
       }
@@ -300,22 +330,41 @@ filter_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
   }
   const uint32_t n_cand = s_ncand;
 
-  // ---- phase B: approximate score, restore rank rows ----
-  for (uint32_t i = tid; i < n_cand; i += blockDim.x) {
-    const uint32_t item = (uint32_t)key[i];
-    uint8_t *row = rank + (size_t)item * scr.rank_stride;
-    float s = 0.0f;
-    for (uint32_t t0 = 0; t0 < nq; t0 += 16) {
-      uint4 w = *reinterpret_cast<uint4 *>(row + t0);
-      const uint8_t *bytes = reinterpret_cast<const uint8_t *>(&w);
+  // ---- phase B: approximate score, restore rank rows (2 candidates in flight) ----
+  for (uint32_t i0 = tid; i0 < n_cand; i0 += 2 * blockDim.x) {
+    float ps_acc[2] = {0.0f, 0.0f};
+    uint32_t item[2];
+    uint8_t *row[2];
 #pragma unroll
-      for (int u = 0; u < 16; u++) {
-        const uint32_t t = t0 + u;
-        if (t < nq && bytes[u] != 0xff) s = __fadd_rn(s, ps[t * nprobe + bytes[u]]);
-      }
-      *reinterpret_cast<uint4 *>(row + t0) = make_uint4(~0u, ~0u, ~0u, ~0u);
+    for (int u = 0; u < 2; u++) {
+      const uint32_t i = i0 + u * blockDim.x;
+      item[u] = i < n_cand ? (uint32_t)key[i] : 0u;
+      row[u] = rank + (size_t)item[u] * scr.rank_stride;
     }
-    key[i] = make_key(s, item);
+    for (uint32_t t0 = 0; t0 < nq; t0 += 16) {
+      uint4 w[2];
+#pragma unroll
+      for (int u = 0; u < 2; u++)
+        if (i0 + u * blockDim.x < n_cand) w[u] = *reinterpret_cast<uint4 *>(row[u] + t0);
+#pragma unroll
+      for (int u = 0; u < 2; u++) {
+        if (i0 + u * blockDim.x >= n_cand) continue;
+        const uint8_t *bytes = reinterpret_cast<const uint8_t *>(&w[u]);
+        float s = t0 == 0 ? 0.0f : ps_acc[u];
+#pragma unroll
+        for (int v = 0; v < 16; v++) {
+          const uint32_t t = t0 + v;
+          if (t < nq && bytes[v] != 0xff) s = __fadd_rn(s, ps[t * nprobe + bytes[v]]);
+        }
+        ps_acc[u] = s;
+        *reinterpret_cast<uint4 *>(row[u] + t0) = make_uint4(~0u, ~0u, ~0u, ~0u);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      const uint32_t i = i0 + u * blockDim.x;
+      if (i < n_cand) key[i] = make_key(ps_acc[u], item[u]);
+    }
   }
   __syncthreads();
 

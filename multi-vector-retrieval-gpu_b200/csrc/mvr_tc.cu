@@ -17,6 +17,8 @@
 
 #include <cuda_bf16.h>
 
+#include <algorithm>
+
 namespace mvr {
 
 namespace {
@@ -105,37 +107,86 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 }
 
-__device__ __forceinline__ uint32_t find_doc(const uint32_t *pref, int n, uint32_t e) {
-  int lo = 0, hi = n - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (pref[mid] <= e) lo = mid; else hi = mid - 1;
-  }
-  return (uint32_t)lo;
-}
 
 }  // namespace
 
-// smem layout (dynamic, 1024-aligned inside): A[2] 2 x 32 KB, B 16 KB,
-// lut (bf16) <= 4 KB, best [64][kTcDocs] ints 8 KB
-constexpr size_t kTcSmem = 1024 + 2 * 32768 + 16384 + 4096 + 64 * kTcDocs * 4;
+// Decompress 8 dims (one 16-byte chunk of a BF16 row): centroid chunk +
+// per-byte decode-table rows (VPB BF16 weights per residual byte).
+template <int NBIT>
+__device__ __forceinline__ uint4 decode_chunk(uint4 cen, const uint8_t *rb,
+                                              const __nv_bfloat16 *lut, const uint32_t *nib,
+                                              int lane) {
+  constexpr int VPB = 8 / NBIT;
+  uint32_t w[4];
+  if constexpr (NBIT == 2) {         // 2 bytes = 4 nibbles -> 4 x (2 weights)
+    // nib[(nibble * 32 + lane)]: bf16x2 of the nibble's two codes, one copy
+    // per lane so that the 32 lanes read 32 different banks
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const uint32_t byte = rb[u >> 1];
+      const uint32_t nb = (u & 1) ? (byte & 0xfu) : (byte >> 4);
+      w[u] = nib[nb * 32 + lane];
+    }
+  } else if constexpr (NBIT == 1) {  // 1 byte = 2 nibbles -> 2 x (4 weights)
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      const uint32_t nb = u ? (rb[0] & 0xfu) : (rb[0] >> 4);
+      const uint2 t = reinterpret_cast<const uint2 *>(nib)[nb * 32 + lane];
+      w[2 * u] = t.x;
+      w[2 * u + 1] = t.y;
+    }
+  } else if constexpr (VPB == 8) {   // (unused) 1 byte -> 8 weights
+    const uint4 t = *reinterpret_cast<const uint4 *>(lut + rb[0] * 8);
+    w[0] = t.x; w[1] = t.y; w[2] = t.z; w[3] = t.w;
+  } else if constexpr (VPB == 4) {   // 2 bytes -> 2 x 4 weights
+    const uint2 t0 = *reinterpret_cast<const uint2 *>(lut + rb[0] * 4);
+    const uint2 t1 = *reinterpret_cast<const uint2 *>(lut + rb[1] * 4);
+    w[0] = t0.x; w[1] = t0.y; w[2] = t1.x; w[3] = t1.y;
+  } else if constexpr (VPB == 2) {   // 4 bytes -> 4 x 2 weights
+#pragma unroll
+    for (int u = 0; u < 4; u++) w[u] = *reinterpret_cast<const uint32_t *>(lut + rb[u] * 2);
+  } else {                           // 8 bytes -> 8 x 1 weight
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const uint32_t lo = *reinterpret_cast<const uint16_t *>(lut + rb[2 * u]);
+      const uint32_t hi = *reinterpret_cast<const uint16_t *>(lut + rb[2 * u + 1]);
+      w[u] = lo | (hi << 16);
+    }
+  }
+  uint32_t c[4] = {cen.x, cen.y, cen.z, cen.w};
+#pragma unroll
+  for (int u = 0; u < 4; u++) {
+    __nv_bfloat162 r = __hadd2(*reinterpret_cast<__nv_bfloat162 *>(&c[u]),
+                               *reinterpret_cast<__nv_bfloat162 *>(&w[u]));
+    c[u] = *reinterpret_cast<uint32_t *>(&r);
+  }
+  return make_uint4(c[0], c[1], c[2], c[3]);
+}
+
+// Dynamic shared memory of rerank_tc_kernel for a query-token tile of N rows.
+__host__ __device__ constexpr size_t tc_smem_bytes(int nbit, uint32_t n) {
+  return 1024 + 32768 /*A*/ + (size_t)n * 256 /*B*/ + 64 * kTcDocs * 4 /*best*/ +
+         (nbit <= 2 ? 16 * 32 * 4 * (nbit == 1 ? 2 : 1) : 256 * (8 / nbit) * 2) /*decode table*/;
+}
 
 template <int NBIT>
-__global__ void __launch_bounds__(kTcThreads, 1)
+__global__ void __launch_bounds__(kTcThreads, 4)
 rerank_tc_kernel(DevIndex ix, const __nv_bfloat16 *__restrict__ cen_bf16,
                  const __nv_bfloat16 *__restrict__ lut_bf16, const float *__restrict__ q,
                  const uint64_t *__restrict__ q_off, const uint32_t *__restrict__ short_id,
                  const uint32_t *__restrict__ n_short, uint32_t probe_topk, int semantics,
-                 float *__restrict__ approx, unsigned *__restrict__ err) {
+                 uint32_t n_max, float *__restrict__ approx, unsigned *__restrict__ err) {
   constexpr int VPB = 8 / NBIT;
-  constexpr int HALF_BYTES = 64 / VPB;
+  constexpr int HALF_BYTES = 64 / VPB;  // residual bytes of 64 dims
+  constexpr int NRW = HALF_BYTES / 8;   // uint2 words per half row
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  uint8_t *A0 = smem;              // [2][2 K-blocks][128 rows][128 B]
-  uint8_t *Bq = smem + 2 * 32768;  // [2 K-blocks][64 rows][128 B]
-  __nv_bfloat16 *lut = reinterpret_cast<__nv_bfloat16 *>(Bq + 16384);  // [256][VPB]
-  int *best = reinterpret_cast<int *>(Bq + 16384 + 4096);             // [64][kTcDocs]
-  __shared__ uint64_t bars[2];
+  uint8_t *Ad = smem;                                          // [2 K-blocks][128 rows][128 B]
+  uint8_t *Bq = smem + 32768;                                  // [2 K-blocks][n_max rows][128 B]
+  int *best = reinterpret_cast<int *>(Bq + n_max * 256);       // [64][kTcDocs]
+  uint32_t *nib = reinterpret_cast<uint32_t *>(best + 64 * kTcDocs);  // b<=2: [16][32](x2)
+  __nv_bfloat16 *lut = reinterpret_cast<__nv_bfloat16 *>(nib);        // b>=4: [256][VPB]
+  __shared__ uint64_t bar;
   __shared__ uint32_t tmem_base_s;
   __shared__ uint32_t d_len[kTcDocs], d_pref[kTcDocs + 1];
   __shared__ uint64_t d_off[kTcDocs];
@@ -150,18 +201,17 @@ rerank_tc_kernel(DevIndex ix, const __nv_bfloat16 *__restrict__ cen_bf16,
   const uint32_t nd = min((uint32_t)kTcDocs, ns - d0);
   const uint64_t tok0 = q_off[b];
   const uint32_t nq = (uint32_t)(q_off[b + 1] - tok0);
-  const uint32_t N = nq <= 32 ? 32u : 64u;
+  const uint32_t N = nq <= 32 ? 32u : 64u;  // <= n_max (host sizes smem by the batch)
   const uint32_t idesc = idesc_bf16(kTcTile, (int)N);
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
                      smem_u32(&tmem_base_s)),
-                 "r"(128u));
+                 "r"(64u));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
   }
   if (tid == 0) {
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
+    mbar_init(&bar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     s_abort = 0;
   }
@@ -170,10 +220,26 @@ rerank_tc_kernel(DevIndex ix, const __nv_bfloat16 *__restrict__ cen_bf16,
     d_len[tid] = ix.item_n_vec[it];
     d_off[tid] = ix.item_off[it];
   }
-  for (int i = tid; i < 256 * VPB; i += kTcThreads) lut[i] = lut_bf16[i];
+  if constexpr (NBIT <= 2) {
+    // nibble n is the top nibble of byte (n << 4): its codes' weights are the
+    // first 4 / NBIT entries of that byte's decode-table row; one copy per
+    // lane so the 32 lanes of a warp read 32 different banks
+    for (int i = tid; i < 16 * 32; i += kTcThreads) {
+      const int n = i >> 5, ln = i & 31;
+      const uint16_t *row = reinterpret_cast<const uint16_t *>(lut_bf16) + (n << 4) * VPB;
+      if constexpr (NBIT == 2) {
+        nib[n * 32 + ln] = (uint32_t)row[0] | ((uint32_t)row[1] << 16);
+      } else {
+        reinterpret_cast<uint2 *>(nib)[n * 32 + ln] =
+            make_uint2((uint32_t)row[0] | ((uint32_t)row[1] << 16), (uint32_t)row[2] | ((uint32_t)row[3] << 16));
+      }
+    }
+  } else {
+    for (int i = tid; i < 256 * VPB; i += kTcThreads) lut[i] = lut_bf16[i];
+  }
   for (int i = tid; i < 64 * kTcDocs; i += kTcThreads) best[i] = f2si(-INFINITY);
   // query tokens -> B operand (BF16, swizzled, rows >= nq zero)
-  for (int i = tid; i < 64 * 16; i += kTcThreads) {
+  for (int i = tid; i < (int)N * 16; i += kTcThreads) {
     const int row = i >> 4, ch = i & 15;  // 16 chunks of 8 dims
     uint4 v = make_uint4(0, 0, 0, 0);
     if ((uint32_t)row < nq) {
@@ -186,8 +252,7 @@ rerank_tc_kernel(DevIndex ix, const __nv_bfloat16 *__restrict__ cen_bf16,
       v.z = *reinterpret_cast<uint32_t *>(&p2);
       v.w = *reinterpret_cast<uint32_t *>(&p3);
     }
-    if ((uint32_t)row < N)
-      *reinterpret_cast<uint4 *>(Bq + (ch >> 3) * (N * 128) + sw128_off(row, ch & 7)) = v;
+    *reinterpret_cast<uint4 *>(Bq + (ch >> 3) * (N * 128) + sw128_off(row, ch & 7)) = v;
   }
   __syncthreads();
   if (tid == 0) {
@@ -201,85 +266,86 @@ rerank_tc_kernel(DevIndex ix, const __nv_bfloat16 *__restrict__ cen_bf16,
   const uint32_t tmem = tmem_base_s;
   const uint32_t n_tok = d_pref[nd];
   const uint32_t n_tiles = (n_tok + kTcTile - 1) / kTcTile;
-  const uint32_t a_base = smem_u32(A0), b_base = smem_u32(Bq);
+  const uint32_t a_base = smem_u32(Ad), b_base = smem_u32(Bq);
+  const uint32_t row = tid & (kTcTile - 1), half = tid >> 7;
+  uint8_t *kb = Ad + half * 16384;
+
+  // next tile's row data (doc, centroid id, residual bytes); the doc index
+  // only moves forward as the tiles advance
+  uint32_t di = 0;
+  int p_doc = -1;
+  uint32_t p_code = 0;
+  uint2 p_res[NRW];
+  auto prefetch = [&](uint32_t tile) {
+    const uint32_t s = tile * kTcTile + row;
+    p_doc = -1;
+    if (tile < n_tiles && s < n_tok) {
+      while (d_pref[di + 1] <= s) di++;
+      const uint64_t v = d_off[di] + (s - d_pref[di]);
+      p_doc = (int)di;
+      p_code = __ldg(ix.vq_code + v);
+      const uint2 *res = reinterpret_cast<const uint2 *>(ix.residual + v * ix.bytes_per_vec + half * HALF_BYTES);
+#pragma unroll
+      for (int u = 0; u < NRW; u++) p_res[u] = __ldg(res + u);
+    }
+  };
 
   auto epilogue = [&](uint32_t tile) {
-    const int buf = tile & 1;
-    const bool ok = __all_sync(kFull, mbar_wait(&bars[buf], (tile >> 1) & 1));
-    if (!ok) {  // warp-uniform: record, skip this tile, stop after the next barrier
+    const bool ok = __all_sync(kFull, mbar_wait(&bar, tile & 1));
+    if (!ok) {  // warp-uniform: record, skip, stop after the next barrier
       if (lane == 0) { atomicOr(err, 1u); s_abort = 1; }
       return;
     }
     tc_fence_after();
-    const uint32_t row = 32 * (warp & 3) + lane;
-    const int doc = tok_doc[buf][row];
+    const uint32_t r = 32 * (warp & 3) + lane;
+    const int doc = tok_doc[tile & 1][r];
     const unsigned grp = __match_any_sync(kFull, doc);
     const bool leader = lane == __ffs(grp) - 1;
-    for (uint32_t c0 = (warp >> 2) * (N / 2); c0 < (warp >> 2) * (N / 2) + N / 2; c0 += 16) {
-      uint32_t r[16];
-      tmem_ld16(tmem + ((32u * (warp & 3)) << 16) + buf * N + c0, r);
+    for (uint32_t c0 = half * (N / 2); c0 < half * (N / 2) + N / 2; c0 += 16) {
+      uint32_t v[16];
+      tmem_ld16(tmem + ((32u * (warp & 3)) << 16) + c0, v);
 #pragma unroll
       for (int j = 0; j < 16; j++) {
-        const int m = __reduce_max_sync(grp, f2si(__uint_as_float(r[j])));
+        const int m = __reduce_max_sync(grp, f2si(__uint_as_float(v[j])));
         if (leader && doc >= 0 && c0 + j < nq) atomicMax(&best[(c0 + j) * kTcDocs + doc], m);
       }
     }
     tc_fence_before();
   };
 
+  prefetch(0);
   for (uint32_t tile = 0; tile < n_tiles; tile++) {
-    const int buf = tile & 1;
-    uint8_t *Ab = A0 + buf * 32768;
-    // -- decompress 128 tokens to BF16: thread = (row tid&127, half tid>>7) --
-    {
-      const uint32_t row = tid & (kTcTile - 1), half = tid >> 7;
-      const uint32_t s = tile * kTcTile + row;
-      uint8_t *kb = Ab + half * 16384;
-      if (s < n_tok) {
-        const uint32_t di = find_doc(d_pref, (int)nd, s);
-        const uint64_t v = d_off[di] + (s - d_pref[di]);
-        if (half == 0) tok_doc[buf][row] = (int)di;
-        const uint4 *cen = reinterpret_cast<const uint4 *>(cen_bf16 + (size_t)ix.vq_code[v] * kDim + half * 64);
-        const uint8_t *res = ix.residual + v * ix.bytes_per_vec + half * HALF_BYTES;
-        uint8_t rb[HALF_BYTES];
+    if (tile > 0) epilogue(tile - 1);  // MMA(tile-1) done: A reusable, D readable
+    const int doc = p_doc;
+    const uint32_t code = p_code;
+    uint8_t rb[HALF_BYTES];
 #pragma unroll
-        for (int u = 0; u < HALF_BYTES / 8; u++)
-          *reinterpret_cast<uint2 *>(rb + 8 * u) = __ldg(reinterpret_cast<const uint2 *>(res) + u);
+    for (int u = 0; u < NRW; u++) *reinterpret_cast<uint2 *>(rb + 8 * u) = p_res[u];
+    if (half == 0) tok_doc[tile & 1][row] = doc;
+    prefetch(tile + 1);
+    if (doc >= 0) {
+      const uint4 *cen = reinterpret_cast<const uint4 *>(cen_bf16 + (size_t)code * kDim + half * 64);
 #pragma unroll
-        for (int c = 0; c < 8; c++) {  // 8 dims per 16-byte chunk
-          uint4 cv = __ldg(cen + c);
-          __nv_bfloat162 *cp = reinterpret_cast<__nv_bfloat162 *>(&cv);
+      for (int c = 0; c < 8; c++)
+        *reinterpret_cast<uint4 *>(kb + sw128_off(row, c)) =
+            decode_chunk<NBIT>(__ldg(cen + c), rb + c * (8 / VPB), lut, nib, lane);
+    } else {
 #pragma unroll
-          for (int u = 0; u < 4; u++) {
-            const int d = c * 8 + 2 * u;
-            const __nv_bfloat16 w0 = lut[(uint32_t)rb[d / VPB] * VPB + (d % VPB)];
-            const __nv_bfloat16 w1 = lut[(uint32_t)rb[(d + 1) / VPB] * VPB + ((d + 1) % VPB)];
-            cp[u] = __hadd2(cp[u], __halves2bfloat162(w0, w1));
-          }
-          *reinterpret_cast<uint4 *>(kb + sw128_off(row, c)) = cv;
-        }
-      } else {
-        if (half == 0) tok_doc[buf][row] = -1;
-#pragma unroll
-        for (int c = 0; c < 8; c++) *reinterpret_cast<uint4 *>(kb + sw128_off(row, c)) = make_uint4(0, 0, 0, 0);
-      }
+      for (int c = 0; c < 8; c++) *reinterpret_cast<uint4 *>(kb + sw128_off(row, c)) = make_uint4(0, 0, 0, 0);
     }
     fence_async_smem();
     __syncthreads();
     if (s_abort) break;
     if (tid == 0) {
       tc_fence_after();
-      const uint32_t a_tile = a_base + buf * 32768;
 #pragma unroll
       for (int kk = 0; kk < 8; kk++) {
-        const uint64_t ad = sw128_desc(a_tile + (kk >> 2) * 16384 + (kk & 3) * 32);
+        const uint64_t ad = sw128_desc(a_base + (kk >> 2) * 16384 + (kk & 3) * 32);
         const uint64_t bd = sw128_desc(b_base + (kk >> 2) * (N * 128) + (kk & 3) * 32);
-        mma_bf16(tmem + buf * N, ad, bd, idesc, kk > 0 ? 1u : 0u);
+        mma_bf16(tmem, ad, bd, idesc, kk > 0 ? 1u : 0u);
       }
-      mma_commit(&bars[buf]);
+      mma_commit(&bar);
     }
-    if (tile > 0) epilogue(tile - 1);
-    __syncthreads();
   }
   if (!s_abort && n_tiles > 0) epilogue(n_tiles - 1);
   __syncthreads();
@@ -298,8 +364,335 @@ rerank_tc_kernel(DevIndex ix, const __nv_bfloat16 *__restrict__ cen_bf16,
   __syncthreads();
   if (warp == 0) {
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(128u));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(64u));
   }
+}
+
+// ---------------------------------------------------------------------
+// Centroid scoring on tensor cores.
+//
+// probe_tc_kernel: CTA = 128 query tokens (operand A, M = 128, BF16
+// swizzled in smem) x a range of 128-centroid tiles (operand B, N = 128).
+// Centroid tiles are stored pre-swizzled in HBM (cen_sw, 32 KB per tile) and
+// streamed with cp.async.bulk into a double buffer, completion tracked by
+// mbarrier transaction counts; one thread issues 8 tcgen05.mma per tile into
+// a double-buffered TMEM accumulator (2 x 128 columns).  Epilogue: thread
+// (token row r, column half h) reads its 64 scores with tcgen05.ld and keeps
+// the best kCand (score desc, id asc) in shared memory.  Candidate ids per
+// token per split go to `cand`; probe_rescore_kernel recomputes their scores
+// exactly (canonical FP32 fma chain) and selects the top nprobe.
+// ---------------------------------------------------------------------
+constexpr int kPtTok = 128;     // tokens per CTA (M)
+constexpr int kPtCen = 128;     // centroids per tile (N)
+constexpr int kCand = 16;       // candidates kept per (token, column half)
+constexpr size_t kPtSmem = 1024 + 32768 /*A*/ + 2 * 32768 /*B*/ + 2 * kCand * 256 * 4 /*lists*/ +
+                           256 * 33 * 4 /*per-thread staging of 32 scores*/;
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,"
+      "%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
+        "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),
+        "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+}
+
+// Insert (v, c) into thread column `col` of the [kCand][256] candidate lists
+// (sorted best-first); returns the new worst entry.  Out of line on purpose:
+// inserting is rare after the first tiles, and inlining it into the unrolled
+// epilogue blows the kernel past the instruction cache.
+__device__ __noinline__ void cand_insert(float *ls, uint32_t *lid, int col, float v, uint32_t c,
+                                         float *thr_s, uint32_t *thr_id) {
+  int pos = kCand - 1;
+  while (pos > 0 && better(v, c, ls[(pos - 1) * 256 + col], lid[(pos - 1) * 256 + col])) {
+    ls[pos * 256 + col] = ls[(pos - 1) * 256 + col];
+    lid[pos * 256 + col] = lid[(pos - 1) * 256 + col];
+    pos--;
+  }
+  ls[pos * 256 + col] = v;
+  lid[pos * 256 + col] = c;
+  *thr_s = ls[(kCand - 1) * 256 + col];
+  *thr_id = lid[(kCand - 1) * 256 + col];
+}
+
+__global__ void __launch_bounds__(256, 1)
+probe_tc_kernel(const float *__restrict__ q, uint32_t n_tok, const uint8_t *__restrict__ cen_sw,
+                uint32_t n_cent, uint32_t tiles_per_split, uint32_t n_tiles,
+                uint32_t *__restrict__ cand, unsigned *__restrict__ err) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint8_t *Aq = smem;                  // [2 K-blocks][128 rows][128 B]
+  uint8_t *Bc = smem + 32768;          // [2 bufs][2 K-blocks][128 rows][128 B]
+  float *ls = reinterpret_cast<float *>(smem + 32768 + 65536);   // [kCand][256]
+  uint32_t *lid = reinterpret_cast<uint32_t *>(ls + kCand * 256);  // [kCand][256]
+  __shared__ uint64_t full[2], done[2];
+  __shared__ uint32_t tmem_base_s;
+  __shared__ int s_abort;
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t t0 = blockIdx.y * kPtTok;
+  const uint32_t tile_begin = blockIdx.x * tiles_per_split;
+  const uint32_t tile_end = min(n_tiles, tile_begin + tiles_per_split);
+  if (tile_begin >= tile_end) return;
+  const uint32_t idesc = idesc_bf16(kPtTok, kPtCen);
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     smem_u32(&tmem_base_s)),
+                 "r"(256u));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  if (tid == 0) {
+    mbar_init(&full[0], 1);
+    mbar_init(&full[1], 1);
+    mbar_init(&done[0], 1);
+    mbar_init(&done[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    s_abort = 0;
+  }
+  // query tokens -> A (BF16, swizzled; rows >= n_tok zero)
+  for (int i = tid; i < kPtTok * 16; i += 256) {
+    const int row = i >> 4, ch = i & 15;
+    uint4 v = make_uint4(0, 0, 0, 0);
+    if (t0 + row < n_tok) {
+      const float4 *src = reinterpret_cast<const float4 *>(q + (size_t)(t0 + row) * kDim + ch * 8);
+      const float4 a = __ldg(src), c = __ldg(src + 1);
+      __nv_bfloat162 p0 = __floats2bfloat162_rn(a.x, a.y), p1 = __floats2bfloat162_rn(a.z, a.w);
+      __nv_bfloat162 p2 = __floats2bfloat162_rn(c.x, c.y), p3 = __floats2bfloat162_rn(c.z, c.w);
+      v.x = *reinterpret_cast<uint32_t *>(&p0);
+      v.y = *reinterpret_cast<uint32_t *>(&p1);
+      v.z = *reinterpret_cast<uint32_t *>(&p2);
+      v.w = *reinterpret_cast<uint32_t *>(&p3);
+    }
+    *reinterpret_cast<uint4 *>(Aq + (ch >> 3) * 16384 + sw128_off(row, ch & 7)) = v;
+  }
+  for (int i = 0; i < kCand; i++) {
+    ls[i * 256 + tid] = -INFINITY;
+    lid[i * 256 + tid] = 0xffffffffu;
+  }
+  fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_s;
+  const uint32_t a_base = smem_u32(Aq), b_base = smem_u32(Bc);
+  if (tid == 0) {
+    mbar_expect_tx(&full[0], 32768);
+    bulk_g2s(Bc, cen_sw + (size_t)tile_begin * 32768, 32768, &full[0]);
+  }
+  float thr_s = -INFINITY;
+  uint32_t thr_id = 0xffffffffu;
+  const uint32_t half = tid >> 7;
+
+  auto epilogue = [&](uint32_t j) {  // tile j = tile_begin + j
+    const int buf = j & 1;
+    const bool ok = __all_sync(kFull, mbar_wait(&done[buf], (j >> 1) & 1));
+    if (!ok) {
+      if (lane == 0) { atomicOr(err, 2u); s_abort = 1; }
+      return;
+    }
+    tc_fence_after();
+    const uint32_t cbase = (tile_begin + j) * kPtCen + half * 64;
+#pragma unroll
+    for (int part = 0; part < 2; part++) {
+      uint32_t r[32];
+      tmem_ld32(tmem + ((32u * (warp & 3)) << 16) + buf * kPtCen + half * 64 + part * 32, r);
+      // candidates better than the current worst kept entry (compare only)
+      uint32_t m = 0;
+#pragma unroll
+      for (int i = 0; i < 32; i++) {
+        const uint32_t c = cbase + part * 32 + i;
+        m |= (uint32_t)(c < n_cent && better(__uint_as_float(r[i]), c, thr_s, thr_id)) << i;
+      }
+      if (m) {  // rare after the first tiles: spill this chunk and insert
+        float *stage = ls + kCand * 256 * 2 + tid * 33;  // per-thread staging row
+#pragma unroll
+        for (int i = 0; i < 32; i++) stage[i] = __uint_as_float(r[i]);
+        while (m) {
+          const int i = __ffs(m) - 1;
+          m &= m - 1;
+          const uint32_t c = cbase + part * 32 + i;
+          const float v = stage[i];
+          if (better(v, c, thr_s, thr_id)) cand_insert(ls, lid, tid, v, c, &thr_s, &thr_id);
+        }
+      }
+    }
+    tc_fence_before();
+  };
+
+  const uint32_t n_local = tile_end - tile_begin;
+  for (uint32_t j = 0; j < n_local; j++) {
+    const int buf = j & 1;
+    if (tid == 0) {
+      bool ok = mbar_wait(&full[buf], (j >> 1) & 1);  // tile j landed in B[buf]
+      if (ok) {
+        tc_fence_after();
+        const uint32_t bt = b_base + buf * 32768;
+#pragma unroll
+        for (int kk = 0; kk < 8; kk++) {
+          const uint64_t ad = sw128_desc(a_base + (kk >> 2) * 16384 + (kk & 3) * 32);
+          const uint64_t bd = sw128_desc(bt + (kk >> 2) * 16384 + (kk & 3) * 32);
+          mma_bf16(tmem + buf * kPtCen, ad, bd, idesc, kk > 0 ? 1u : 0u);
+        }
+        mma_commit(&done[buf]);
+        // B[buf ^ 1] is free once MMA j-1 completed; stream tile j+1 into it
+        if (j >= 1) ok = mbar_wait(&done[buf ^ 1], ((j - 1) >> 1) & 1);
+        if (ok && j + 1 < n_local) {
+          mbar_expect_tx(&full[buf ^ 1], 32768);
+          bulk_g2s(Bc + (buf ^ 1) * 32768, cen_sw + (size_t)(tile_begin + j + 1) * 32768, 32768,
+                   &full[buf ^ 1]);
+        }
+      }
+      if (!ok) { atomicOr(err, 2u); s_abort = 1; }
+    }
+    if (j >= 1) epilogue(j - 1);
+    __syncthreads();
+    if (s_abort) break;
+  }
+  if (!s_abort) epilogue(n_local - 1);
+  __syncthreads();
+  // candidates of this split: [token][split][2 halves][kCand]
+  const uint32_t row = 32 * (warp & 3) + lane;
+  if (t0 + row < n_tok && !s_abort) {
+    uint32_t *dst = cand + ((size_t)(t0 + row) * gridDim.x + blockIdx.x) * (2 * kCand) + half * kCand;
+    for (int i = 0; i < kCand; i++) dst[i] = lid[i * 256 + tid];
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(256u));
+  }
+}
+
+// One warp per token: exact FP32 scores (sequential fma over d, + 1.0f) of
+// the token's BF16 candidates, top nprobe by (score desc, id asc).
+__global__ void __launch_bounds__(256)
+probe_rescore_kernel(const float *__restrict__ q, uint32_t n_tok, const float *__restrict__ cen,
+                     uint32_t n_cent, const uint32_t *__restrict__ cand, uint32_t n_cand,
+                     uint32_t nprobe, uint32_t *__restrict__ out_id, float *__restrict__ out_s) {
+  __shared__ float qs[8][kDim];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint32_t t = blockIdx.x * 8 + w;
+  if (t >= n_tok) return;
+  for (int d = lane; d < kDim; d += 32) qs[w][d] = q[(size_t)t * kDim + d];
+  __syncwarp();
+  const int np = (int)nprobe;
+  float ls = -INFINITY, thr_s = -INFINITY;
+  uint32_t lid = 0xffffffffu, thr_id = 0xffffffffu;
+  const uint32_t *cl = cand + (size_t)t * n_cand;
+  for (uint32_t c0 = 0; c0 < n_cand; c0 += 32) {
+    const uint32_t i = c0 + lane;
+    uint32_t c = i < n_cand ? cl[i] : 0xffffffffu;
+    float s = -INFINITY;
+    if (c < n_cent) {
+      const float4 *row = reinterpret_cast<const float4 *>(cen + (size_t)c * kDim);
+      float acc = 0.0f;
+#pragma unroll 8
+      for (int d4 = 0; d4 < kDim / 4; d4++) {
+        const float4 x = __ldg(row + d4);
+        acc = __fmaf_rn(qs[w][4 * d4 + 0], x.x, acc);
+        acc = __fmaf_rn(qs[w][4 * d4 + 1], x.y, acc);
+        acc = __fmaf_rn(qs[w][4 * d4 + 2], x.z, acc);
+        acc = __fmaf_rn(qs[w][4 * d4 + 3], x.w, acc);
+      }
+      s = __fadd_rn(acc, 1.0f);
+    } else {
+      c = 0xffffffffu;
+    }
+    unsigned m = __ballot_sync(kFull, c != 0xffffffffu && better(s, c, thr_s, thr_id));
+    while (m) {
+      const int src = __ffs(m) - 1;
+      m &= m - 1;
+      const float ns = __shfl_sync(kFull, s, src);
+      const uint32_t nid = __shfl_sync(kFull, c, src);
+      if (better(ns, nid, thr_s, thr_id)) {
+        const bool ahead = lane < np && better(ls, lid, ns, nid);
+        const int pos = __popc(__ballot_sync(kFull, ahead));
+        const float up_s = __shfl_up_sync(kFull, ls, 1);
+        const uint32_t up_id = __shfl_up_sync(kFull, lid, 1);
+        if (lane > pos) { ls = up_s; lid = up_id; }
+        else if (lane == pos) { ls = ns; lid = nid; }
+        thr_s = __shfl_sync(kFull, ls, np - 1);
+        thr_id = __shfl_sync(kFull, lid, np - 1);
+      }
+    }
+  }
+  if (lane < np) {
+    out_id[(size_t)t * nprobe + lane] = lid;
+    out_s[(size_t)t * nprobe + lane] = ls;
+  }
+}
+
+// cen_sw[tile][kb][row][128 B] = swizzled BF16 centroid rows (rows >= C zero)
+__global__ void swizzle_centroid_kernel(const float *__restrict__ cen, uint32_t n_cent,
+                                        uint32_t n_tiles, uint8_t *__restrict__ out) {
+  const size_t n_chunks = (size_t)n_tiles * 128 * 16;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_chunks;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t tile = (uint32_t)(i / (128 * 16));
+    const uint32_t row = (uint32_t)((i / 16) % 128), ch = (uint32_t)(i % 16);
+    const uint32_t c = tile * 128 + row;
+    uint4 v = make_uint4(0, 0, 0, 0);
+    if (c < n_cent) {
+      const float *src = cen + (size_t)c * kDim + ch * 8;
+      __nv_bfloat162 p0 = __floats2bfloat162_rn(src[0], src[1]), p1 = __floats2bfloat162_rn(src[2], src[3]);
+      __nv_bfloat162 p2 = __floats2bfloat162_rn(src[4], src[5]), p3 = __floats2bfloat162_rn(src[6], src[7]);
+      v.x = *reinterpret_cast<uint32_t *>(&p0);
+      v.y = *reinterpret_cast<uint32_t *>(&p1);
+      v.z = *reinterpret_cast<uint32_t *>(&p2);
+      v.w = *reinterpret_cast<uint32_t *>(&p3);
+    }
+    *reinterpret_cast<uint4 *>(out + (size_t)tile * 32768 + (ch >> 3) * 16384 + sw128_off(row, ch & 7)) = v;
+  }
+}
+
+cudaError_t make_centroid_tiles(const float *cen, uint32_t n_cent, uint32_t n_tiles, void *out,
+                                cudaStream_t st) {
+  swizzle_centroid_kernel<<<592, 256, 0, st>>>(cen, n_cent, n_tiles, reinterpret_cast<uint8_t *>(out));
+  return cudaGetLastError();
+}
+
+uint32_t probe_tc_cand_per_token(uint32_t n_tok, uint32_t n_tiles, int n_sm, uint32_t *splits) {
+  const uint32_t tok_tiles = (n_tok + kPtTok - 1) / kPtTok;
+  uint32_t s = ((uint32_t)n_sm + tok_tiles - 1) / tok_tiles;  // ~1 wave of 1-CTA/SM
+  s = std::max(1u, std::min(s, n_tiles));
+  const uint32_t per = (n_tiles + s - 1) / s;
+  *splits = (n_tiles + per - 1) / per;
+  return *splits * 2 * kCand;
+}
+
+cudaError_t launch_probe_tc(const float *q, uint32_t n_tok, const void *cen_sw, const float *cen,
+                            uint32_t n_cent, uint32_t nprobe, uint32_t splits, uint32_t *cand,
+                            uint32_t *out_id, float *out_s, unsigned *err, cudaStream_t st,
+                            int *n_launch) {
+  const uint32_t n_tiles = (n_cent + kPtCen - 1) / kPtCen;
+  const uint32_t per = (n_tiles + splits - 1) / splits;
+  dim3 grid(splits, (n_tok + kPtTok - 1) / kPtTok);
+  probe_tc_kernel<<<grid, 256, kPtSmem, st>>>(q, n_tok, reinterpret_cast<const uint8_t *>(cen_sw),
+                                              n_cent, per, n_tiles, cand, err);
+  probe_rescore_kernel<<<(n_tok + 7) / 8, 256, 0, st>>>(q, n_tok, cen, n_cent, cand,
+                                                       splits * 2 * kCand, nprobe, out_id, out_s);
+  *n_launch += 2;
+  return cudaGetLastError();
 }
 
 // BF16 tables: centroid rows and the byte -> per-value weight table.
@@ -315,28 +708,32 @@ cudaError_t make_bf16(const float *in, size_t n, void *out, cudaStream_t st) {
 
 cudaError_t configure_tc_kernels() {
   cudaError_t e;
-  e = cudaFuncSetAttribute(rerank_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
+  e = cudaFuncSetAttribute(rerank_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem_bytes(1, 64));
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(rerank_tc_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
+  e = cudaFuncSetAttribute(rerank_tc_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem_bytes(2, 64));
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(rerank_tc_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
+  e = cudaFuncSetAttribute(rerank_tc_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem_bytes(4, 64));
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(rerank_tc_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
+  e = cudaFuncSetAttribute(probe_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPtSmem);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(rerank_tc_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem_bytes(8, 64));
 }
 
 cudaError_t launch_rerank_tc(const DevIndex &ix, const void *cen_bf16, const void *lut_bf16,
                              const float *q, const uint64_t *q_off, uint32_t n_query,
                              const uint32_t *short_id, const uint32_t *n_short,
-                             uint32_t probe_topk, int semantics, float *approx, unsigned *err,
-                             cudaStream_t st, int *n_launch) {
+                             uint32_t probe_topk, int semantics, uint32_t nq_max, float *approx,
+                             unsigned *err, cudaStream_t st, int *n_launch) {
   dim3 grid((probe_topk + kTcDocs - 1) / kTcDocs, n_query);
+  const uint32_t n_max = nq_max <= 32 ? 32u : 64u;
+  const size_t sm = tc_smem_bytes((int)ix.n_bit, n_max);
   const __nv_bfloat16 *c = reinterpret_cast<const __nv_bfloat16 *>(cen_bf16);
   const __nv_bfloat16 *l = reinterpret_cast<const __nv_bfloat16 *>(lut_bf16);
   switch (ix.n_bit) {
-    case 1: rerank_tc_kernel<1><<<grid, kTcThreads, kTcSmem, st>>>(ix, c, l, q, q_off, short_id, n_short, probe_topk, semantics, approx, err); break;
-    case 2: rerank_tc_kernel<2><<<grid, kTcThreads, kTcSmem, st>>>(ix, c, l, q, q_off, short_id, n_short, probe_topk, semantics, approx, err); break;
-    case 4: rerank_tc_kernel<4><<<grid, kTcThreads, kTcSmem, st>>>(ix, c, l, q, q_off, short_id, n_short, probe_topk, semantics, approx, err); break;
-    case 8: rerank_tc_kernel<8><<<grid, kTcThreads, kTcSmem, st>>>(ix, c, l, q, q_off, short_id, n_short, probe_topk, semantics, approx, err); break;
+    case 1: rerank_tc_kernel<1><<<grid, kTcThreads, sm, st>>>(ix, c, l, q, q_off, short_id, n_short, probe_topk, semantics, n_max, approx, err); break;
+    case 2: rerank_tc_kernel<2><<<grid, kTcThreads, sm, st>>>(ix, c, l, q, q_off, short_id, n_short, probe_topk, semantics, n_max, approx, err); break;
+    case 4: rerank_tc_kernel<4><<<grid, kTcThreads, sm, st>>>(ix, c, l, q, q_off, short_id, n_short, probe_topk, semantics, n_max, approx, err); break;
+    case 8: rerank_tc_kernel<8><<<grid, kTcThreads, sm, st>>>(ix, c, l, q, q_off, short_id, n_short, probe_topk, semantics, n_max, approx, err); break;
     default: return cudaErrorInvalidValue;
   }
   *n_launch += 1;

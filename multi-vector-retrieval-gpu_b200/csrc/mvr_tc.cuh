@@ -10,7 +10,16 @@ cudaError_t make_bf16(const float *in, size_t n, void *out, cudaStream_t st);
 cudaError_t launch_rerank_tc(const DevIndex &ix, const void *cen_bf16, const void *lut_bf16,
                              const float *q, const uint64_t *q_off, uint32_t n_query,
                              const uint32_t *short_id, const uint32_t *n_short,
-                             uint32_t probe_topk, int semantics, float *approx, unsigned *err,
-                             cudaStream_t st, int *n_launch);
+                             uint32_t probe_topk, int semantics, uint32_t nq_max, float *approx,
+                             unsigned *err, cudaStream_t st, int *n_launch);
+
+// tensor-core centroid scoring: candidates per token = splits * 32
+uint32_t probe_tc_cand_per_token(uint32_t n_tok, uint32_t n_tiles, int n_sm, uint32_t *splits);
+cudaError_t make_centroid_tiles(const float *cen, uint32_t n_cent, uint32_t n_tiles, void *out,
+                                cudaStream_t st);
+cudaError_t launch_probe_tc(const float *q, uint32_t n_tok, const void *cen_sw, const float *cen,
+                            uint32_t n_cent, uint32_t nprobe, uint32_t splits, uint32_t *cand,
+                            uint32_t *out_id, float *out_s, unsigned *err, cudaStream_t st,
+                            int *n_launch);
 
 }  // namespace mvr

@@ -92,3 +92,26 @@ def test_bf16_small_shortlists():
             ok = t["id"] != 0xFFFFFFFF
             assert ok.sum() == min(10, len(r["short_id"]))
     g.close()
+
+
+@pytest.mark.parametrize("n_centroid", [96, 700])
+def test_tensor_core_probe_matches_exact(n_centroid):
+    """nprobe <= 16 under MVR_PREC_BF16 scores centroids on the tensor cores
+    and re-scores the candidates in exact FP32: probe ids and scores must be
+    the plain path's, bit for bit."""
+    ix = tiny_index(n_doc=700, n_centroid=n_centroid, n_bit=2, seed=n_centroid)
+    g, o = gpu_index(ix), oracle_of(ix)
+    q, off = make_queries(ix, 6, (1, 64), seed=41)
+    for i in range(6):
+        qi = q[off[i]:off[i + 1]]
+        for nprobe in (1, 8, 16):
+            t = g.trace(qi, 10, nprobe, 100, PREC_BF16)
+            r = o.search_one(qi, 10, nprobe, 100)
+            np.testing.assert_array_equal(t["probe_id"], r["probe_id"])
+            np.testing.assert_array_equal(t["probe_score"], r["probe_score"])
+            np.testing.assert_array_equal(t["cand_id"], r["cand_id"])
+    # a multi-batch run exercises several token tiles and centroid splits
+    s, i = g.search(q, 10, 8, 100, tok_off=off, semantics=PREC_BF16)
+    s2, i2 = g.search(q, 10, 8, 100, tok_off=off)
+    assert (i == i2).all(axis=1).sum() >= 5
+    g.close()
