@@ -370,7 +370,6 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
   uint32_t tok_cap = 0;
   size_t part_need = 1, cand_need = 1;
   const bool tc_probe = bf16 && nprobe <= 16;  // tensor-core scoring + exact re-score
-  const uint32_t n_ctile = h->dix.n_centroid_pad / 128;
   for (uint32_t bt = 0; bt < n_batch; bt++) {
     const uint32_t s = bt * B, e = std::min(n_query, s + B);
     const uint32_t T = (uint32_t)(off[e] - off[s]);
@@ -379,7 +378,7 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
     part_need = std::max(part_need, part_entries(h, T, nprobe, &sp));
     uint32_t tsp;
     if (tc_probe)
-      cand_need = std::max(cand_need, (size_t)T * probe_tc_cand_per_token(T, n_ctile, h->n_sm, &tsp));
+      cand_need = std::max(cand_need, (size_t)T * probe_tc_cand_per_token(T, h->dix.n_centroid, h->n_sm, &tsp));
   }
   const uint32_t rank_stride = nq_max <= 32 ? 32u : 64u;
   MVR_TRY(ensure_scratch(h, std::min(B, n_query), rank_stride));
@@ -418,7 +417,7 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
     CUDA_TRY(cudaEventRecord(ev(bt, 1), st));
     if (tc_probe) {
       uint32_t tsp;
-      probe_tc_cand_per_token(T, n_ctile, h->n_sm, &tsp);
+      probe_tc_cand_per_token(T, h->dix.n_centroid, h->n_sm, &tsp);
       CUDA_TRY(launch_probe_tc(qp, T, h->cen_sw, h->dix.centroid, h->dix.n_centroid, nprobe, tsp,
                                w.cand, w.probe_id, w.probe_s, h->d_err, st, &launches));
     } else {
@@ -539,7 +538,7 @@ int finish_index(mvr_index *h, const uint32_t *item_n_vec_host, const uint32_t *
   h->lut_bf16 = lb;
   uint8_t *sw;
   MVR_TRY(dalloc(&sw, (size_t)d.n_centroid_pad * 256, &h->bufs));
-  CUDA_TRY(make_centroid_tiles(d.centroid, d.n_centroid, d.n_centroid_pad / 128, sw, h->stream));
+  CUDA_TRY(make_centroid_tiles(d.centroid, d.n_centroid, d.n_centroid_pad / 64, sw, h->stream));
   h->cen_sw = sw;
   float *ct;
   MVR_TRY(dalloc(&ct, (size_t)kDim * d.n_centroid_pad, &h->bufs));

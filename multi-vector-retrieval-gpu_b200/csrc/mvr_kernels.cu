@@ -221,11 +221,23 @@ probe_merge_kernel(const uint32_t *__restrict__ part_id,
 // (doc, token) carries the max over probes; the rank j is recorded in a
 // per-slot byte table rank[doc][token] (0xff = unvisited).  A doc enters the
 // candidate set the first time any token visits it (per-slot epoch stamps,
-// no O(n_item) reset).  Phase B sums the per-token maxima in token order and
-// restores the touched rank rows to 0xff.  Phase C/D radix-select the top
+// no O(n_item) reset).  Phase B sums the per-token maxima exactly (2^-32
+// fixed point, rounded once to FP32) and restores the touched rank rows to
+// 0xff.  Phase C/D radix-select the top
 // probe_topk candidates by the 64-bit key (score desc, id asc).
 // ---------------------------------------------------------------------
 constexpr int kFilterThreads = 1024;
+
+// v * 2^32 rounded to nearest-even, clamped to +-2^62 (exact for |v| >= 2^-9):
+// the approximate score is the exact sum of these terms, rounded once to FP32
+__device__ __forceinline__ long long to_fixed(float v) {
+  double x = (double)v * 4294967296.0;
+  x = fmin(fmax(x, -4611686018427387904.0), 4611686018427387904.0);
+  return __double2ll_rn(x);
+}
+__device__ __forceinline__ float from_fixed(long long a) {
+  return __ll2float_rn(a) * (1.0f / 4294967296.0f);
+}
 
 __device__ __forceinline__ uint32_t find_seg(const uint32_t *pref, int n, uint32_t e) {
   // largest i in [0, n) with pref[i] <= e   (pref[0] = 0, non-decreasing)
@@ -244,8 +256,7 @@ filter_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
               FilterScratch scr, uint32_t epoch,
               uint32_t *__restrict__ short_id, float *__restrict__ short_approx,
               uint32_t *__restrict__ n_short_out, uint32_t *__restrict__ qstat) {
-  __shared__ float ps[kMaxQueryTok * kMaxProbe];
-  __shared__ uint32_t pid[kMaxQueryTok * kMaxProbe];
+  __shared__ long long pfix[kMaxQueryTok * kMaxProbe];
   __shared__ uint32_t pref[kMaxQueryTok + 1];
   __shared__ uint32_t lsz[kMaxQueryTok * kMaxProbe];
   __shared__ uint64_t lof[kMaxQueryTok * kMaxProbe];
@@ -261,19 +272,15 @@ filter_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
   uint8_t *rank = scr.rank + (size_t)b * scr.n_item * scr.rank_stride;
   uint64_t *key = scr.key + (size_t)b * scr.n_item;
 
+  // probe scores (fixed point) and list sizes / offsets of every probe
+  // (probe id 0xffffffff = no finite score)
   for (uint32_t i = tid; i < nq * nprobe; i += blockDim.x) {
-    pid[i] = probe_id[tok0 * nprobe + i];
-    ps[i] = probe_s[tok0 * nprobe + i];
-  }
-  if (tid == 0) { s_ncand = 0; s_entries = 0; s_stok = 0; }
-  __syncthreads();
-
-  // list sizes / offsets of every probe (probe id 0xffffffff = no finite score)
-  for (uint32_t i = tid; i < nq * nprobe; i += blockDim.x) {
-    const uint32_t c = pid[i];
+    const uint32_t c = probe_id[tok0 * nprobe + i];
+    pfix[i] = to_fixed(probe_s[tok0 * nprobe + i]);
     lsz[i] = c < ix.n_centroid ? ix.ivf_size[c] : 0u;
     lof[i] = c < ix.n_centroid ? ix.ivf_off[c] : 0ull;
   }
+  if (tid == 0) { s_ncand = 0; s_entries = 0; s_stok = 0; }
   __syncthreads();
 
   // ---- phase A: scatter probed lists rank by rank ----
@@ -332,7 +339,7 @@ filter_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
 
   // ---- phase B: approximate score, restore rank rows (2 candidates in flight) ----
   for (uint32_t i0 = tid; i0 < n_cand; i0 += 2 * blockDim.x) {
-    float ps_acc[2] = {0.0f, 0.0f};
+    long long ps_acc[2] = {0, 0};
     uint32_t item[2];
     uint8_t *row[2];
 #pragma unroll
@@ -350,11 +357,11 @@ filter_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
       for (int u = 0; u < 2; u++) {
         if (i0 + u * blockDim.x >= n_cand) continue;
         const uint8_t *bytes = reinterpret_cast<const uint8_t *>(&w[u]);
-        float s = t0 == 0 ? 0.0f : ps_acc[u];
+        long long s = ps_acc[u];
 #pragma unroll
         for (int v = 0; v < 16; v++) {
           const uint32_t t = t0 + v;
-          if (t < nq && bytes[v] != 0xff) s = __fadd_rn(s, ps[t * nprobe + bytes[v]]);
+          if (t < nq && bytes[v] != 0xff) s += pfix[t * nprobe + bytes[v]];
         }
         ps_acc[u] = s;
         *reinterpret_cast<uint4 *>(row[u] + t0) = make_uint4(~0u, ~0u, ~0u, ~0u);
@@ -363,7 +370,7 @@ filter_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
 #pragma unroll
     for (int u = 0; u < 2; u++) {
       const uint32_t i = i0 + u * blockDim.x;
-      if (i < n_cand) key[i] = make_key(ps_acc[u], item[u]);
+      if (i < n_cand) key[i] = make_key(from_fixed(ps_acc[u]), item[u]);
     }
   }
   __syncthreads();

@@ -27,7 +27,7 @@ constexpr unsigned kFull = 0xffffffffu;
 constexpr int kTcTile = 128;      // doc tokens per MMA tile (M)
 constexpr int kTcDocs = 32;       // shortlisted docs per CTA
 constexpr int kTcThreads = 256;
-constexpr uint32_t kWaitLimit = 1u << 26;  // bounded mbarrier polls (~1 s)
+constexpr uint64_t kWaitNs = 1000000000ull;  // mbarrier wait bound (1 s)
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -54,20 +54,38 @@ __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count));
 }
 
-// Bounded wait on an mbarrier phase; returns false after kWaitLimit polls.
+// Bounded wait on an mbarrier phase: try_wait suspends the thread until the
+// phase completes (or a hardware time slice passes); gives up after ~1 s of
+// %globaltimer and returns false.
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+  return t;
+}
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
   const uint32_t a = smem_u32(bar);
-  for (uint32_t i = 0; i < kWaitLimit; i++) {
+  uint64_t t0 = 0;
+  for (uint32_t i = 0;; i++) {
     uint32_t done;
     asm volatile(
-        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
         " selp.u32 %0, 1, 0, p;\n}\n"
         : "=r"(done)
         : "r"(a), "r"(parity)
         : "memory");
     if (done) return true;
+    if (i == 0) t0 = global_ns();
+    else if (global_ns() - t0 > kWaitNs) return false;
   }
-  return false;
+}
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(smem)), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
 __device__ __forceinline__ void tc_fence_before() {
@@ -372,35 +390,22 @@ rerank_tc_kernel(DevIndex ix, const __nv_bfloat16 *__restrict__ cen_bf16,
 // Centroid scoring on tensor cores.
 //
 // probe_tc_kernel: CTA = 128 query tokens (operand A, M = 128, BF16
-// swizzled in smem) x a range of 128-centroid tiles (operand B, N = 128).
-// Centroid tiles are stored pre-swizzled in HBM (cen_sw, 32 KB per tile) and
-// streamed with cp.async.bulk into a double buffer, completion tracked by
-// mbarrier transaction counts; one thread issues 8 tcgen05.mma per tile into
-// a double-buffered TMEM accumulator (2 x 128 columns).  Epilogue: thread
-// (token row r, column half h) reads its 64 scores with tcgen05.ld and keeps
-// the best kCand (score desc, id asc) in shared memory.  Candidate ids per
+// swizzled in smem) x a range of 64-centroid tiles (operand B, N = 64).
+// Centroid tiles are stored pre-swizzled in HBM (cen_sw, 16 KB per tile) and
+// streamed by all threads with cp.async into a double buffer; one thread
+// issues 8 tcgen05.mma per tile into a double-buffered TMEM accumulator
+// (2 x 64 columns) whose completion an mbarrier tracks, so the epilogue of
+// tile j-1 overlaps the MMA of tile j.  Epilogue: thread (token row r, column
+// half h) reads its 32 scores with tcgen05.ld, compares their max with the
+// worst of its kCand kept candidates and, rarely, inserts.  Candidate ids per
 // token per split go to `cand`; probe_rescore_kernel recomputes their scores
 // exactly (canonical FP32 fma chain) and selects the top nprobe.
 // ---------------------------------------------------------------------
 constexpr int kPtTok = 128;     // tokens per CTA (M)
-constexpr int kPtCen = 128;     // centroids per tile (N)
+constexpr int kPtCen = 64;      // centroids per tile (N)
 constexpr int kCand = 16;       // candidates kept per (token, column half)
-constexpr size_t kPtSmem = 1024 + 32768 /*A*/ + 2 * 32768 /*B*/ + 2 * kCand * 256 * 4 /*lists*/ +
-                           256 * 33 * 4 /*per-thread staging of 32 scores*/;
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)),
-               "r"(bytes)
-               : "memory");
-}
-
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
-          smem_u32(dst)),
-      "l"(src), "r"(bytes), "r"(smem_u32(bar))
-      : "memory");
-}
+constexpr uint32_t kPtTileBytes = kPtCen * 256;  // one swizzled BF16 centroid tile
+constexpr size_t kPtSmem = 1024 + 32768 /*A*/ + 2 * kPtTileBytes /*B*/ + 2 * kCand * 256 * 4 /*lists*/;
 
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
   asm volatile(
@@ -415,12 +420,16 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 }
 
+struct Worst {
+  float s;
+  uint32_t id;
+};
+
 // Insert (v, c) into thread column `col` of the [kCand][256] candidate lists
 // (sorted best-first); returns the new worst entry.  Out of line on purpose:
 // inserting is rare after the first tiles, and inlining it into the unrolled
 // epilogue blows the kernel past the instruction cache.
-__device__ __noinline__ void cand_insert(float *ls, uint32_t *lid, int col, float v, uint32_t c,
-                                         float *thr_s, uint32_t *thr_id) {
+__device__ __noinline__ Worst cand_insert(float *ls, uint32_t *lid, int col, float v, uint32_t c) {
   int pos = kCand - 1;
   while (pos > 0 && better(v, c, ls[(pos - 1) * 256 + col], lid[(pos - 1) * 256 + col])) {
     ls[pos * 256 + col] = ls[(pos - 1) * 256 + col];
@@ -429,21 +438,20 @@ __device__ __noinline__ void cand_insert(float *ls, uint32_t *lid, int col, floa
   }
   ls[pos * 256 + col] = v;
   lid[pos * 256 + col] = c;
-  *thr_s = ls[(kCand - 1) * 256 + col];
-  *thr_id = lid[(kCand - 1) * 256 + col];
+  return Worst{ls[(kCand - 1) * 256 + col], lid[(kCand - 1) * 256 + col]};
 }
 
-__global__ void __launch_bounds__(256, 1)
+__global__ void __launch_bounds__(256, 2)
 probe_tc_kernel(const float *__restrict__ q, uint32_t n_tok, const uint8_t *__restrict__ cen_sw,
                 uint32_t n_cent, uint32_t tiles_per_split, uint32_t n_tiles,
                 uint32_t *__restrict__ cand, unsigned *__restrict__ err) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint8_t *Aq = smem;                  // [2 K-blocks][128 rows][128 B]
-  uint8_t *Bc = smem + 32768;          // [2 bufs][2 K-blocks][128 rows][128 B]
-  float *ls = reinterpret_cast<float *>(smem + 32768 + 65536);   // [kCand][256]
+  uint8_t *Bc = smem + 32768;          // [2 bufs][2 K-blocks][64 rows][128 B]
+  float *ls = reinterpret_cast<float *>(Bc + 2 * kPtTileBytes);     // [kCand][256]
   uint32_t *lid = reinterpret_cast<uint32_t *>(ls + kCand * 256);  // [kCand][256]
-  __shared__ uint64_t full[2], done[2];
+  __shared__ uint64_t done[2];
   __shared__ uint32_t tmem_base_s;
   __shared__ int s_abort;
 
@@ -457,17 +465,27 @@ probe_tc_kernel(const float *__restrict__ q, uint32_t n_tok, const uint8_t *__re
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
                      smem_u32(&tmem_base_s)),
-                 "r"(256u));
+                 "r"(128u));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
   }
   if (tid == 0) {
-    mbar_init(&full[0], 1);
-    mbar_init(&full[1], 1);
     mbar_init(&done[0], 1);
     mbar_init(&done[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     s_abort = 0;
   }
+  // pre-swizzled centroid tile -> B[buf]: 16 KB = 4 x 16 B per thread
+  auto load_tile = [&](uint32_t tile, int buf) {
+    const uint8_t *src = cen_sw + (size_t)tile * kPtTileBytes;
+    uint8_t *dst = Bc + buf * kPtTileBytes;
+#pragma unroll
+    for (int u = 0; u < (int)(kPtTileBytes / 16 / 256); u++) {
+      const int o = (tid + u * 256) * 16;
+      cp_async16(dst + o, src + o);
+    }
+    cp_async_commit();
+  };
+  load_tile(tile_begin, 0);
   // query tokens -> A (BF16, swizzled; rows >= n_tok zero)
   for (int i = tid; i < kPtTok * 16; i += 256) {
     const int row = i >> 4, ch = i & 15;
@@ -488,86 +506,66 @@ probe_tc_kernel(const float *__restrict__ q, uint32_t n_tok, const uint8_t *__re
     ls[i * 256 + tid] = -INFINITY;
     lid[i * 256 + tid] = 0xffffffffu;
   }
-  fence_async_smem();
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = tmem_base_s;
   const uint32_t a_base = smem_u32(Aq), b_base = smem_u32(Bc);
-  if (tid == 0) {
-    mbar_expect_tx(&full[0], 32768);
-    bulk_g2s(Bc, cen_sw + (size_t)tile_begin * 32768, 32768, &full[0]);
-  }
-  float thr_s = -INFINITY;
-  uint32_t thr_id = 0xffffffffu;
+  Worst w{-INFINITY, 0xffffffffu};
   const uint32_t half = tid >> 7;
 
-  auto epilogue = [&](uint32_t j) {  // tile j = tile_begin + j
-    const int buf = j & 1;
-    const bool ok = __all_sync(kFull, mbar_wait(&done[buf], (j >> 1) & 1));
-    if (!ok) {
-      if (lane == 0) { atomicOr(err, 2u); s_abort = 1; }
-      return;
-    }
+  auto wait_mma = [&](uint32_t j) -> bool {  // MMA of local tile j complete
+    const bool ok = __all_sync(kFull, mbar_wait(&done[j & 1], (j >> 1) & 1));
+    if (!ok && lane == 0) { atomicOr(err, 2u); s_abort = 1; }
+    return ok;
+  };
+  auto epilogue = [&](uint32_t j) {  // MMA j known complete
     tc_fence_after();
-    const uint32_t cbase = (tile_begin + j) * kPtCen + half * 64;
+    uint32_t r[32];
+    tmem_ld32(tmem + ((32u * (warp & 3)) << 16) + (j & 1) * kPtCen + half * 32, r);
+    tc_fence_before();
+    // one compare per chunk in the common case: the chunk's best vs the worst kept
+    float mx = __uint_as_float(r[0]);
 #pragma unroll
-    for (int part = 0; part < 2; part++) {
-      uint32_t r[32];
-      tmem_ld32(tmem + ((32u * (warp & 3)) << 16) + buf * kPtCen + half * 64 + part * 32, r);
-      // candidates better than the current worst kept entry (compare only)
-      uint32_t m = 0;
+    for (int i = 1; i < 32; i++) mx = fmaxf(mx, __uint_as_float(r[i]));
+    if (mx >= w.s) {
+      const uint32_t cbase = (tile_begin + j) * kPtCen + half * 32;
 #pragma unroll
       for (int i = 0; i < 32; i++) {
-        const uint32_t c = cbase + part * 32 + i;
-        m |= (uint32_t)(c < n_cent && better(__uint_as_float(r[i]), c, thr_s, thr_id)) << i;
-      }
-      if (m) {  // rare after the first tiles: spill this chunk and insert
-        float *stage = ls + kCand * 256 * 2 + tid * 33;  // per-thread staging row
-#pragma unroll
-        for (int i = 0; i < 32; i++) stage[i] = __uint_as_float(r[i]);
-        while (m) {
-          const int i = __ffs(m) - 1;
-          m &= m - 1;
-          const uint32_t c = cbase + part * 32 + i;
-          const float v = stage[i];
-          if (better(v, c, thr_s, thr_id)) cand_insert(ls, lid, tid, v, c, &thr_s, &thr_id);
-        }
+        const uint32_t c = cbase + i;
+        const float v = __uint_as_float(r[i]);
+        if (c < n_cent && better(v, c, w.s, w.id)) w = cand_insert(ls, lid, tid, v, c);
       }
     }
-    tc_fence_before();
   };
 
   const uint32_t n_local = tile_end - tile_begin;
   for (uint32_t j = 0; j < n_local; j++) {
     const int buf = j & 1;
-    if (tid == 0) {
-      bool ok = mbar_wait(&full[buf], (j >> 1) & 1);  // tile j landed in B[buf]
-      if (ok) {
-        tc_fence_after();
-        const uint32_t bt = b_base + buf * 32768;
-#pragma unroll
-        for (int kk = 0; kk < 8; kk++) {
-          const uint64_t ad = sw128_desc(a_base + (kk >> 2) * 16384 + (kk & 3) * 32);
-          const uint64_t bd = sw128_desc(bt + (kk >> 2) * 16384 + (kk & 3) * 32);
-          mma_bf16(tmem + buf * kPtCen, ad, bd, idesc, kk > 0 ? 1u : 0u);
-        }
-        mma_commit(&done[buf]);
-        // B[buf ^ 1] is free once MMA j-1 completed; stream tile j+1 into it
-        if (j >= 1) ok = mbar_wait(&done[buf ^ 1], ((j - 1) >> 1) & 1);
-        if (ok && j + 1 < n_local) {
-          mbar_expect_tx(&full[buf ^ 1], 32768);
-          bulk_g2s(Bc + (buf ^ 1) * 32768, cen_sw + (size_t)(tile_begin + j + 1) * 32768, 32768,
-                   &full[buf ^ 1]);
-        }
-      }
-      if (!ok) { atomicOr(err, 2u); s_abort = 1; }
-    }
-    if (j >= 1) epilogue(j - 1);
-    __syncthreads();
+    // MMA j-1 read B[buf^1]: once it completed, stream tile j+1 into it
+    bool ok = true;
+    if (j >= 1) ok = wait_mma(j - 1);
+    if (j + 1 < n_local) load_tile(tile_begin + j + 1, buf ^ 1);
+    else cp_async_commit();
+    cp_async_wait<1>();  // this thread's part of tile j landed
+    fence_async_smem();
+    __syncthreads();     // all of tile j in smem; epilogue(j-2) done with D[buf]
     if (s_abort) break;
+    if (tid == 0) {
+      tc_fence_after();
+      const uint32_t bt = b_base + buf * kPtTileBytes;
+#pragma unroll
+      for (int kk = 0; kk < 8; kk++) {
+        const uint64_t ad = sw128_desc(a_base + (kk >> 2) * 16384 + (kk & 3) * 32);
+        const uint64_t bd = sw128_desc(bt + (kk >> 2) * (kPtTileBytes / 2) + (kk & 3) * 32);
+        mma_bf16(tmem + buf * kPtCen, ad, bd, idesc, kk > 0 ? 1u : 0u);
+      }
+      mma_commit(&done[buf]);
+    }
+    if (j >= 1 && ok) epilogue(j - 1);  // overlaps MMA j
   }
-  if (!s_abort) epilogue(n_local - 1);
+  cp_async_wait<0>();
+  if (!s_abort && wait_mma(n_local - 1)) epilogue(n_local - 1);
   __syncthreads();
   // candidates of this split: [token][split][2 halves][kCand]
   const uint32_t row = 32 * (warp & 3) + lane;
@@ -579,7 +577,7 @@ probe_tc_kernel(const float *__restrict__ q, uint32_t n_tok, const uint8_t *__re
   __syncthreads();
   if (warp == 0) {
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(256u));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(128u));
   }
 }
 
@@ -642,15 +640,16 @@ probe_rescore_kernel(const float *__restrict__ q, uint32_t n_tok, const float *_
   }
 }
 
-// cen_sw[tile][kb][row][128 B] = swizzled BF16 centroid rows (rows >= C zero)
+// cen_sw[tile][kb][row][128 B] = swizzled BF16 centroid rows of 64-centroid
+// tiles (rows >= C zero)
 __global__ void swizzle_centroid_kernel(const float *__restrict__ cen, uint32_t n_cent,
                                         uint32_t n_tiles, uint8_t *__restrict__ out) {
-  const size_t n_chunks = (size_t)n_tiles * 128 * 16;
+  const size_t n_chunks = (size_t)n_tiles * kPtCen * 16;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_chunks;
        i += (size_t)gridDim.x * blockDim.x) {
-    const uint32_t tile = (uint32_t)(i / (128 * 16));
-    const uint32_t row = (uint32_t)((i / 16) % 128), ch = (uint32_t)(i % 16);
-    const uint32_t c = tile * 128 + row;
+    const uint32_t tile = (uint32_t)(i / (kPtCen * 16));
+    const uint32_t row = (uint32_t)((i / 16) % kPtCen), ch = (uint32_t)(i % 16);
+    const uint32_t c = tile * kPtCen + row;
     uint4 v = make_uint4(0, 0, 0, 0);
     if (c < n_cent) {
       const float *src = cen + (size_t)c * kDim + ch * 8;
@@ -661,7 +660,8 @@ __global__ void swizzle_centroid_kernel(const float *__restrict__ cen, uint32_t 
       v.z = *reinterpret_cast<uint32_t *>(&p2);
       v.w = *reinterpret_cast<uint32_t *>(&p3);
     }
-    *reinterpret_cast<uint4 *>(out + (size_t)tile * 32768 + (ch >> 3) * 16384 + sw128_off(row, ch & 7)) = v;
+    *reinterpret_cast<uint4 *>(out + (size_t)tile * kPtTileBytes + (ch >> 3) * (kPtTileBytes / 2) +
+                               sw128_off(row, ch & 7)) = v;
   }
 }
 
@@ -671,9 +671,10 @@ cudaError_t make_centroid_tiles(const float *cen, uint32_t n_cent, uint32_t n_ti
   return cudaGetLastError();
 }
 
-uint32_t probe_tc_cand_per_token(uint32_t n_tok, uint32_t n_tiles, int n_sm, uint32_t *splits) {
+uint32_t probe_tc_cand_per_token(uint32_t n_tok, uint32_t n_cent, int n_sm, uint32_t *splits) {
+  const uint32_t n_tiles = (n_cent + kPtCen - 1) / kPtCen;
   const uint32_t tok_tiles = (n_tok + kPtTok - 1) / kPtTok;
-  uint32_t s = ((uint32_t)n_sm + tok_tiles - 1) / tok_tiles;  // ~1 wave of 1-CTA/SM
+  uint32_t s = (2u * (uint32_t)n_sm + tok_tiles - 1) / tok_tiles;  // ~1 wave of 2 CTAs/SM
   s = std::max(1u, std::min(s, n_tiles));
   const uint32_t per = (n_tiles + s - 1) / s;
   *splits = (n_tiles + per - 1) / per;

@@ -335,6 +335,19 @@ double orc_maxsim_f64(const float *q, uint32_t nq, const float *tok,
 
 typedef struct { float s; uint32_t id; } scored;
 
+/* Fixed-point approximate-score terms: v * 2^32 rounded to nearest-even
+ * (exact for |v| >= 2^-9 since FP32 has a 24-bit significand), clamped to
+ * +-2^30 * 2^32 so that 64 terms cannot overflow; the sum converts back by
+ * one round-to-nearest int64 -> float conversion and an exact 2^-32 scale. */
+int64_t orc_fixed(float v) {
+  double x = (double)v * 4294967296.0;
+  const double lim = 4611686018427387904.0; /* 2^62 */
+  if (x > lim) x = lim;
+  if (x < -lim) x = -lim;
+  return (int64_t)llrint(x);
+}
+float orc_unfixed(int64_t acc) { return (float)acc * (1.0f / 4294967296.0f); }
+
 static int cmp_scored(const void *a, const void *b) {
   const scored *x = (const scored *)a, *y = (const scored *)b;
   if (better(x->s, x->id, y->s, y->id)) return -1;
@@ -406,18 +419,19 @@ static int search_one_ws(const orc_index *ix, orc_ws *w, const float *q,
       }
     }
   qsort(w->cand, n_cand, sizeof(uint32_t), cmp_u32);
-  /* 3. approximate score = sum over q in order (RAFT reduce,
-   * FilterPP.hpp:366-379) */
+  /* 3. approximate score = sum over q of the per-token maxima (RAFT reduce,
+   * FilterPP.hpp:366-379), summed exactly: each term as a 2^-32 fixed-point
+   * integer, the integer sum rounded once to FP32 (order-independent). */
   for (uint32_t i = 0; i < n_cand; i++) {
     const uint32_t it = w->cand[i];
     uint8_t *r = w->rank + (size_t)it * nq;
-    float s = 0.0f;
+    int64_t acc = 0;
     for (uint32_t t = 0; t < nq; t++) {
-      if (r[t] != 0xff) s = s + ps[t * nprobe + r[t]];
+      if (r[t] != 0xff) acc += orc_fixed(ps[t * nprobe + r[t]]);
       r[t] = 0xff;
     }
     w->seen[it] = 0;
-    w->sc[i].s = s;
+    w->sc[i].s = orc_unfixed(acc);
     w->sc[i].id = it;
   }
   if (tr) {

@@ -20,8 +20,9 @@
  *   dot(a,b)   = sequential fmaf over d = 0..D-1 starting from 0.0f
  *   S[q][c]    = dot(q, c) + 1.0f                       (single FP32 add)
  *   probe      = top-nprobe per query token by (S desc, centroid id asc)
- *   approx[c]  = sum over q = 0..nq-1 (in order, FP32) of the score of the
- *                highest-ranked probe of token q whose IVF list holds doc c
+ *   approx[c]  = sum over q of the score of the highest-ranked probe of
+ *                token q whose IVF list holds doc c, summed exactly in 2^-32
+ *                fixed point (int64) and rounded once to FP32
  *   shortlist  = top-probe_topk candidates by (approx desc, doc id asc)
  *   x[t][d]    = centroid[code_t][d] + W[bucket(t,d)]   (single FP32 add)
  *   maxsim     = sum over q (in order, FP32, from 0.0f) of max_t dot(q, x_t)
@@ -88,6 +89,8 @@ uint64_t orc_ivf_build(const uint32_t *code, const uint32_t *item_n_vec,
                        uint32_t *size, uint32_t *ids);
 
 /* ---- search stages -------------------------------------------------- */
+int64_t orc_fixed(float v);
+float orc_unfixed(int64_t acc);
 void orc_centroid_scores(const float *q, uint32_t nq, const float *centroid,
                          uint32_t n_centroid, uint32_t dim, float *S);
 void orc_assign(const float *vec, uint64_t n_vec, const float *centroid,
