@@ -239,6 +239,34 @@ def workload_config(w, path):
             "l2": "flushed (256 MiB write) between timed steps"}
 
 
+def run_profile_case():
+    """A case small enough for ncu (a few GB on the device, one batch per
+    search, inputs larger than L2): the raw tokens are freed before searching,
+    so only the compressed index (~0.5 GB) and the working set are resident."""
+    import torch
+    from mvr import PREC_BF16, build, synth
+    spec = synth.CorpusSpec(200_000, seed=0)
+    tok = synth.tokens(spec, "cuda")
+    ix = build.build_index(tok, spec.item_n_vec, 16384, 2, kmeans_iter=2)
+    del tok
+    g = build.load_built(ix)
+    del ix
+    torch.cuda.empty_cache()
+    n = 64
+    g.set_batch(n)
+    q, _ = synth.queries(spec, n, 32, "cuda", seed=5)
+    out_s = torch.empty((n, 10), dtype=torch.float32, device="cuda")
+    out_i = torch.empty((n, 10), dtype=torch.int32, device="cuda")
+    for fl in (PREC_BF16, 0):
+        st = g.search_device(q.data_ptr(), None, n, 32, 10, 8, 1000, out_s.data_ptr(),
+                             out_i.data_ptr(), 0, semantics=fl)
+        print("flags", fl, "device_ms", round(st.device_ms, 4), "stages_ms",
+              [round(x, 4) for x in st.stage_ms], flush=True)
+    print("max_mem_GB", round(torch.cuda.max_memory_allocated() / 1e9, 2))
+    g.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -249,6 +277,9 @@ def main():
     ap.add_argument("--probe-topk", type=int, default=None)
     ap.add_argument("--rescore", type=int, default=0, help="FP32 re-score width (0: 4*k)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="small profiling target instead of the bench: 200,000 docs, 16,384 "
+                         "centroids, one mixed-precision and one plain search of 64 queries")
     ap.add_argument("--recall-sweep", default="",
                     help="extra nprobe:probe_topk settings whose recall@k is reported, "
                          "e.g. 4:100,8:500")
@@ -258,6 +289,8 @@ def main():
         w["probe_topk"] = args.probe_topk
     if args.impl == "reference":
         return run_reference(args, w)
+    if args.profile_case:
+        return run_profile_case()
 
     import torch
     import torch.distributed as dist

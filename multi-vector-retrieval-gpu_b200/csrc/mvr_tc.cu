@@ -395,17 +395,21 @@ rerank_tc_kernel(DevIndex ix, const __nv_bfloat16 *__restrict__ cen_bf16,
 // streamed by all threads with cp.async into a double buffer; one thread
 // issues 8 tcgen05.mma per tile into a double-buffered TMEM accumulator
 // (2 x 64 columns) whose completion an mbarrier tracks, so the epilogue of
-// tile j-1 overlaps the MMA of tile j.  Epilogue: thread (token row r, column
-// half h) reads its 32 scores with tcgen05.ld, compares their max with the
-// worst of its kCand kept candidates and, rarely, inserts.  Candidate ids per
-// token per split go to `cand`; probe_rescore_kernel recomputes their scores
-// exactly (canonical FP32 fma chain) and selects the top nprobe.
+// tile j-1 overlaps the MMA of tile j.  Epilogue: thread = token row reads its
+// 64 scores with tcgen05.ld; chunks whose max beats the token's running
+// threshold append their qualifying scores (predicated stores, no divergent
+// calls) to a per-token buffer that the warp compacts to the best kCand
+// together when a lane's buffer nears full.  Candidate ids per token per split
+// go to `cand`; probe_rescore_kernel recomputes their scores exactly
+// (canonical FP32 fma chain) and selects the top nprobe.
 // ---------------------------------------------------------------------
-constexpr int kPtTok = 128;     // tokens per CTA (M)
+constexpr int kPtTok = 128;     // tokens per CTA (M) = threads per CTA
 constexpr int kPtCen = 64;      // centroids per tile (N)
-constexpr int kCand = 16;       // candidates kept per (token, column half)
+constexpr int kCand = 16;       // candidates kept per token per split
+constexpr int kCap = 56;        // per-token candidate buffer (kCand kept + a chunk + slack)
 constexpr uint32_t kPtTileBytes = kPtCen * 256;  // one swizzled BF16 centroid tile
-constexpr size_t kPtSmem = 1024 + 32768 /*A*/ + 2 * kPtTileBytes /*B*/ + 2 * kCand * 256 * 4 /*lists*/;
+constexpr uint32_t kPtMaxTilesPerSplit = 1024;   // local centroid offsets fit in 16 bits
+constexpr size_t kPtSmem = 1024 + 32768 /*A*/ + 2 * kPtTileBytes /*B*/ + kCap * kPtTok * 6 /*buffers*/;
 
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
   asm volatile(
@@ -420,28 +424,33 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 }
 
-struct Worst {
-  float s;
-  uint32_t id;
-};
-
-// Insert (v, c) into thread column `col` of the [kCand][256] candidate lists
-// (sorted best-first); returns the new worst entry.  Out of line on purpose:
-// inserting is rare after the first tiles, and inlining it into the unrolled
-// epilogue blows the kernel past the instruction cache.
-__device__ __noinline__ Worst cand_insert(float *ls, uint32_t *lid, int col, float v, uint32_t c) {
-  int pos = kCand - 1;
-  while (pos > 0 && better(v, c, ls[(pos - 1) * 256 + col], lid[(pos - 1) * 256 + col])) {
-    ls[pos * 256 + col] = ls[(pos - 1) * 256 + col];
-    lid[pos * 256 + col] = lid[(pos - 1) * 256 + col];
-    pos--;
+// Keep the best kCand of a token's cnt buffered candidates (score desc, id asc)
+// in slots 0..kCand-1, best first; returns the new count.  bs/bi: [kCap][kPtTok]
+// (bi = centroid offset within the split), column `col`.  Selection sort: it
+// runs only when some lane's buffer cannot take the next 32-score chunk (every
+// ~40 appends of the busiest lane), with all lanes of the warp together.
+__device__ __forceinline__ int cand_compact(float *bs, uint16_t *bi, int col, int cnt) {
+  const int keep = cnt < kCand ? cnt : kCand;
+  for (int k = 0; k < keep; k++) {
+    int b = k;
+    float sb = bs[k * kPtTok + col];
+    uint32_t ib = bi[k * kPtTok + col];
+    for (int i = k + 1; i < cnt; i++) {
+      const float si = bs[i * kPtTok + col];
+      const uint32_t ii = bi[i * kPtTok + col];
+      if (better(si, ii, sb, ib)) { b = i; sb = si; ib = ii; }
+    }
+    if (b != k) {
+      bs[b * kPtTok + col] = bs[k * kPtTok + col];
+      bi[b * kPtTok + col] = bi[k * kPtTok + col];
+      bs[k * kPtTok + col] = sb;
+      bi[k * kPtTok + col] = (uint16_t)ib;
+    }
   }
-  ls[pos * 256 + col] = v;
-  lid[pos * 256 + col] = c;
-  return Worst{ls[(kCand - 1) * 256 + col], lid[(kCand - 1) * 256 + col]};
+  return keep;
 }
 
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(kPtTok, 2)
 probe_tc_kernel(const float *__restrict__ q, uint32_t n_tok, const uint8_t *__restrict__ cen_sw,
                 uint32_t n_cent, uint32_t tiles_per_split, uint32_t n_tiles,
                 uint32_t *__restrict__ cand, unsigned *__restrict__ err) {
@@ -449,8 +458,8 @@ probe_tc_kernel(const float *__restrict__ q, uint32_t n_tok, const uint8_t *__re
   uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint8_t *Aq = smem;                  // [2 K-blocks][128 rows][128 B]
   uint8_t *Bc = smem + 32768;          // [2 bufs][2 K-blocks][64 rows][128 B]
-  float *ls = reinterpret_cast<float *>(Bc + 2 * kPtTileBytes);     // [kCand][256]
-  uint32_t *lid = reinterpret_cast<uint32_t *>(ls + kCand * 256);  // [kCand][256]
+  float *bs = reinterpret_cast<float *>(Bc + 2 * kPtTileBytes);   // [kCap][128]
+  uint16_t *bi = reinterpret_cast<uint16_t *>(bs + kCap * kPtTok);  // [kCap][128]
   __shared__ uint64_t done[2];
   __shared__ uint32_t tmem_base_s;
   __shared__ int s_abort;
@@ -474,20 +483,20 @@ probe_tc_kernel(const float *__restrict__ q, uint32_t n_tok, const uint8_t *__re
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     s_abort = 0;
   }
-  // pre-swizzled centroid tile -> B[buf]: 16 KB = 4 x 16 B per thread
+  // pre-swizzled centroid tile -> B[buf]: 16 KB = 8 x 16 B per thread
   auto load_tile = [&](uint32_t tile, int buf) {
     const uint8_t *src = cen_sw + (size_t)tile * kPtTileBytes;
     uint8_t *dst = Bc + buf * kPtTileBytes;
 #pragma unroll
-    for (int u = 0; u < (int)(kPtTileBytes / 16 / 256); u++) {
-      const int o = (tid + u * 256) * 16;
+    for (int u = 0; u < (int)(kPtTileBytes / 16 / kPtTok); u++) {
+      const int o = (tid + u * kPtTok) * 16;
       cp_async16(dst + o, src + o);
     }
     cp_async_commit();
   };
   load_tile(tile_begin, 0);
   // query tokens -> A (BF16, swizzled; rows >= n_tok zero)
-  for (int i = tid; i < kPtTok * 16; i += 256) {
+  for (int i = tid; i < kPtTok * 16; i += kPtTok) {
     const int row = i >> 4, ch = i & 15;
     uint4 v = make_uint4(0, 0, 0, 0);
     if (t0 + row < n_tok) {
@@ -502,17 +511,13 @@ probe_tc_kernel(const float *__restrict__ q, uint32_t n_tok, const uint8_t *__re
     }
     *reinterpret_cast<uint4 *>(Aq + (ch >> 3) * 16384 + sw128_off(row, ch & 7)) = v;
   }
-  for (int i = 0; i < kCand; i++) {
-    ls[i * 256 + tid] = -INFINITY;
-    lid[i * 256 + tid] = 0xffffffffu;
-  }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = tmem_base_s;
   const uint32_t a_base = smem_u32(Aq), b_base = smem_u32(Bc);
-  Worst w{-INFINITY, 0xffffffffu};
-  const uint32_t half = tid >> 7;
+  int cnt = 0;             // buffered candidates of this thread's token
+  float thr = -INFINITY;   // worst kept score once kCand are kept
 
   auto wait_mma = [&](uint32_t j) -> bool {  // MMA of local tile j complete
     const bool ok = __all_sync(kFull, mbar_wait(&done[j & 1], (j >> 1) & 1));
@@ -521,22 +526,42 @@ probe_tc_kernel(const float *__restrict__ q, uint32_t n_tok, const uint8_t *__re
   };
   auto epilogue = [&](uint32_t j) {  // MMA j known complete
     tc_fence_after();
-    uint32_t r[32];
-    tmem_ld32(tmem + ((32u * (warp & 3)) << 16) + (j & 1) * kPtCen + half * 32, r);
-    tc_fence_before();
-    // one compare per chunk in the common case: the chunk's best vs the worst kept
-    float mx = __uint_as_float(r[0]);
 #pragma unroll
-    for (int i = 1; i < 32; i++) mx = fmaxf(mx, __uint_as_float(r[i]));
-    if (mx >= w.s) {
-      const uint32_t cbase = (tile_begin + j) * kPtCen + half * 32;
+    for (int part = 0; part < 2; part++) {
+      uint32_t r[32];
+      tmem_ld32(tmem + ((32u * warp) << 16) + (j & 1) * kPtCen + part * 32, r);
+      float mx = __uint_as_float(r[0]);
 #pragma unroll
-      for (int i = 0; i < 32; i++) {
-        const uint32_t c = cbase + i;
-        const float v = __uint_as_float(r[i]);
-        if (c < n_cent && better(v, c, w.s, w.id)) w = cand_insert(ls, lid, tid, v, c);
+      for (int i = 1; i < 32; i++) mx = fmaxf(mx, __uint_as_float(r[i]));
+      if (__any_sync(kFull, mx >= thr)) {
+        const uint32_t cbase = (tile_begin + j) * kPtCen + part * 32;
+        const uint32_t valid = cbase >= n_cent        ? 0u
+                               : n_cent - cbase >= 32 ? 0xffffffffu
+                                                      : (1u << (n_cent - cbase)) - 1u;
+        auto qualify = [&]() {
+          uint32_t m = 0;
+#pragma unroll
+          for (int i = 0; i < 32; i++) m |= (__uint_as_float(r[i]) >= thr ? 1u : 0u) << i;
+          return m & valid;
+        };
+        uint32_t m = qualify();
+        if (__any_sync(kFull, cnt + __popc(m) > kCap)) {  // cnt <= kCand after this
+          cnt = cand_compact(bs, bi, tid, cnt);
+          thr = cnt == kCand ? bs[(kCand - 1) * kPtTok + tid] : -INFINITY;
+          m = qualify();
+        }
+        const uint32_t lbase = cbase - tile_begin * kPtCen;
+#pragma unroll
+        for (int i = 0; i < 32; i++) {
+          if ((m >> i) & 1u) {  // predicated append
+            bs[cnt * kPtTok + tid] = __uint_as_float(r[i]);
+            bi[cnt * kPtTok + tid] = (uint16_t)(lbase + i);
+            cnt++;
+          }
+        }
       }
     }
+    tc_fence_before();
   };
 
   const uint32_t n_local = tile_end - tile_begin;
@@ -566,12 +591,13 @@ probe_tc_kernel(const float *__restrict__ q, uint32_t n_tok, const uint8_t *__re
   }
   cp_async_wait<0>();
   if (!s_abort && wait_mma(n_local - 1)) epilogue(n_local - 1);
+  cnt = cand_compact(bs, bi, tid, cnt);
   __syncthreads();
-  // candidates of this split: [token][split][2 halves][kCand]
-  const uint32_t row = 32 * (warp & 3) + lane;
-  if (t0 + row < n_tok && !s_abort) {
-    uint32_t *dst = cand + ((size_t)(t0 + row) * gridDim.x + blockIdx.x) * (2 * kCand) + half * kCand;
-    for (int i = 0; i < kCand; i++) dst[i] = lid[i * 256 + tid];
+  // this split's candidates of this token: [token][split][kCand]
+  if (t0 + tid < n_tok && !s_abort) {
+    uint32_t *dst = cand + ((size_t)(t0 + tid) * gridDim.x + blockIdx.x) * kCand;
+    for (int i = 0; i < kCand; i++)
+      dst[i] = i < cnt ? tile_begin * kPtCen + bi[i * kPtTok + tid] : 0xffffffffu;
   }
   tc_fence_before();
   __syncthreads();
@@ -676,9 +702,10 @@ uint32_t probe_tc_cand_per_token(uint32_t n_tok, uint32_t n_cent, int n_sm, uint
   const uint32_t tok_tiles = (n_tok + kPtTok - 1) / kPtTok;
   uint32_t s = (2u * (uint32_t)n_sm + tok_tiles - 1) / tok_tiles;  // ~1 wave of 2 CTAs/SM
   s = std::max(1u, std::min(s, n_tiles));
-  const uint32_t per = (n_tiles + s - 1) / s;
+  s = std::max(s, (n_tiles + kPtMaxTilesPerSplit - 1) / kPtMaxTilesPerSplit);
+  const uint32_t per = (n_tiles + s - 1) / s;  // <= kPtMaxTilesPerSplit
   *splits = (n_tiles + per - 1) / per;
-  return *splits * 2 * kCand;
+  return *splits * kCand;
 }
 
 cudaError_t launch_probe_tc(const float *q, uint32_t n_tok, const void *cen_sw, const float *cen,
@@ -688,10 +715,10 @@ cudaError_t launch_probe_tc(const float *q, uint32_t n_tok, const void *cen_sw, 
   const uint32_t n_tiles = (n_cent + kPtCen - 1) / kPtCen;
   const uint32_t per = (n_tiles + splits - 1) / splits;
   dim3 grid(splits, (n_tok + kPtTok - 1) / kPtTok);
-  probe_tc_kernel<<<grid, 256, kPtSmem, st>>>(q, n_tok, reinterpret_cast<const uint8_t *>(cen_sw),
-                                              n_cent, per, n_tiles, cand, err);
+  probe_tc_kernel<<<grid, kPtTok, kPtSmem, st>>>(q, n_tok, reinterpret_cast<const uint8_t *>(cen_sw),
+                                                 n_cent, per, n_tiles, cand, err);
   probe_rescore_kernel<<<(n_tok + 7) / 8, 256, 0, st>>>(q, n_tok, cen, n_cent, cand,
-                                                       splits * 2 * kCand, nprobe, out_id, out_s);
+                                                       splits * kCand, nprobe, out_id, out_s);
   *n_launch += 2;
   return cudaGetLastError();
 }

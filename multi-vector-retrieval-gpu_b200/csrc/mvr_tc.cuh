@@ -13,7 +13,7 @@ cudaError_t launch_rerank_tc(const DevIndex &ix, const void *cen_bf16, const voi
                              uint32_t probe_topk, int semantics, uint32_t nq_max, float *approx,
                              unsigned *err, cudaStream_t st, int *n_launch);
 
-// tensor-core centroid scoring: candidates per token = splits * 32; the
+// tensor-core centroid scoring: candidates per token = splits * 16; the
 // centroid tiles hold 64 centroids each (n_tiles = C_pad / 64)
 uint32_t probe_tc_cand_per_token(uint32_t n_tok, uint32_t n_cent, int n_sm, uint32_t *splits);
 cudaError_t make_centroid_tiles(const float *cen, uint32_t n_cent, uint32_t n_tiles, void *out,
