@@ -396,20 +396,19 @@ rerank_tc_kernel(DevIndex ix, const __nv_bfloat16 *__restrict__ cen_bf16,
 // issues 8 tcgen05.mma per tile into a double-buffered TMEM accumulator
 // (2 x 64 columns) whose completion an mbarrier tracks, so the epilogue of
 // tile j-1 overlaps the MMA of tile j.  Epilogue: thread = token row reads its
-// 64 scores with tcgen05.ld; chunks whose max beats the token's running
-// threshold append their qualifying scores (predicated stores, no divergent
-// calls) to a per-token buffer that the warp compacts to the best kCand
-// together when a lane's buffer nears full.  Candidate ids per token per split
-// go to `cand`; probe_rescore_kernel recomputes their scores exactly
-// (canonical FP32 fma chain) and selects the top nprobe.
+// 64 scores with tcgen05.ld (two 32-column chunks) and keeps the token's best
+// kCand of the split sorted in registers.  A chunk whose max beats the list's
+// last score is staged in the thread's shared-memory row and only its
+// qualifying columns are inserted (branch-free 16-slot insertion).  Candidate
+// ids per token per split go to `cand`; probe_rescore_kernel recomputes their
+// scores exactly (canonical FP32 fma chain) and selects the top nprobe.
 // ---------------------------------------------------------------------
 constexpr int kPtTok = 128;     // tokens per CTA (M) = threads per CTA
 constexpr int kPtCen = 64;      // centroids per tile (N)
 constexpr int kCand = 16;       // candidates kept per token per split
-constexpr int kCap = 56;        // per-token candidate buffer (kCand kept + a chunk + slack)
+constexpr int kStage = 36;      // staging row stride in floats (16 B aligned, conflict-free STS.128)
 constexpr uint32_t kPtTileBytes = kPtCen * 256;  // one swizzled BF16 centroid tile
-constexpr uint32_t kPtMaxTilesPerSplit = 1024;   // local centroid offsets fit in 16 bits
-constexpr size_t kPtSmem = 1024 + 32768 /*A*/ + 2 * kPtTileBytes /*B*/ + kCap * kPtTok * 6 /*buffers*/;
+constexpr size_t kPtSmem = 1024 + 32768 /*A*/ + 2 * kPtTileBytes /*B*/ + kPtTok * kStage * 4 /*stage*/;
 
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
   asm volatile(
@@ -424,30 +423,30 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 }
 
-// Keep the best kCand of a token's cnt buffered candidates (score desc, id asc)
-// in slots 0..kCand-1, best first; returns the new count.  bs/bi: [kCap][kPtTok]
-// (bi = centroid offset within the split), column `col`.  Selection sort: it
-// runs only when some lane's buffer cannot take the next 32-score chunk (every
-// ~40 appends of the busiest lane), with all lanes of the warp together.
-__device__ __forceinline__ int cand_compact(float *bs, uint16_t *bi, int col, int cnt) {
-  const int keep = cnt < kCand ? cnt : kCand;
-  for (int k = 0; k < keep; k++) {
-    int b = k;
-    float sb = bs[k * kPtTok + col];
-    uint32_t ib = bi[k * kPtTok + col];
-    for (int i = k + 1; i < cnt; i++) {
-      const float si = bs[i * kPtTok + col];
-      const uint32_t ii = bi[i * kPtTok + col];
-      if (better(si, ii, sb, ib)) { b = i; sb = si; ib = ii; }
-    }
-    if (b != k) {
-      bs[b * kPtTok + col] = bs[k * kPtTok + col];
-      bi[b * kPtTok + col] = bi[k * kPtTok + col];
-      bs[k * kPtTok + col] = sb;
-      bi[k * kPtTok + col] = (uint16_t)ib;
-    }
+// Insert (v, c) into a register list sorted by score descending, given v >
+// s[kCand-1].  Centroids arrive in ascending id order, so an equal score
+// already in the list has the smaller id and stays ahead (strict >).  The 16
+// comparisons are independent and are collected as bits of one integer; each
+// slot then takes its own value, its left neighbour's, or (v, c).  (Holding
+// the comparisons as 16 separate bool values under the caller's v > s[15]
+// guard was compiled into code that never wrote s[15] in some contexts with
+// nvcc 12.9; the bit-mask form is checked by the probe parity tests and a
+// per-token insert count.)
+__device__ __forceinline__ void topk_insert(float (&s)[kCand], uint32_t (&d)[kCand], float v,
+                                            uint32_t c) {
+  uint32_t bm = 0;
+#pragma unroll
+  for (int k = 0; k < kCand; k++) bm |= (v > s[k] ? 1u : 0u) << k;
+#pragma unroll
+  for (int k = kCand - 1; k >= 1; k--) {
+    const bool bk = (bm >> k) & 1u, bp = (bm >> (k - 1)) & 1u;
+    const float sk = bp ? s[k - 1] : v;
+    const uint32_t dk = bp ? d[k - 1] : c;
+    s[k] = bk ? sk : s[k];
+    d[k] = bk ? dk : d[k];
   }
-  return keep;
+  s[0] = (bm & 1u) ? v : s[0];
+  d[0] = (bm & 1u) ? c : d[0];
 }
 
 __global__ void __launch_bounds__(kPtTok, 2)
@@ -458,8 +457,7 @@ probe_tc_kernel(const float *__restrict__ q, uint32_t n_tok, const uint8_t *__re
   uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint8_t *Aq = smem;                  // [2 K-blocks][128 rows][128 B]
   uint8_t *Bc = smem + 32768;          // [2 bufs][2 K-blocks][64 rows][128 B]
-  float *bs = reinterpret_cast<float *>(Bc + 2 * kPtTileBytes);   // [kCap][128]
-  uint16_t *bi = reinterpret_cast<uint16_t *>(bs + kCap * kPtTok);  // [kCap][128]
+  float *stage = reinterpret_cast<float *>(Bc + 2 * kPtTileBytes) + threadIdx.x * kStage;
   __shared__ uint64_t done[2];
   __shared__ uint32_t tmem_base_s;
   __shared__ int s_abort;
@@ -516,8 +514,10 @@ probe_tc_kernel(const float *__restrict__ q, uint32_t n_tok, const uint8_t *__re
   tc_fence_after();
   const uint32_t tmem = tmem_base_s;
   const uint32_t a_base = smem_u32(Aq), b_base = smem_u32(Bc);
-  int cnt = 0;             // buffered candidates of this thread's token
-  float thr = -INFINITY;   // worst kept score once kCand are kept
+  float ts[kCand];     // this thread's token: best kCand scores of the split so far
+  uint32_t td[kCand];  // and their centroid ids
+#pragma unroll
+  for (int k = 0; k < kCand; k++) { ts[k] = -INFINITY; td[k] = 0xffffffffu; }
 
   auto wait_mma = [&](uint32_t j) -> bool {  // MMA of local tile j complete
     const bool ok = __all_sync(kFull, mbar_wait(&done[j & 1], (j >> 1) & 1));
@@ -533,32 +533,29 @@ probe_tc_kernel(const float *__restrict__ q, uint32_t n_tok, const uint8_t *__re
       float mx = __uint_as_float(r[0]);
 #pragma unroll
       for (int i = 1; i < 32; i++) mx = fmaxf(mx, __uint_as_float(r[i]));
-      if (__any_sync(kFull, mx >= thr)) {
+      const float thr = ts[kCand - 1];
+      if (__any_sync(kFull, mx > thr)) {
         const uint32_t cbase = (tile_begin + j) * kPtCen + part * 32;
         const uint32_t valid = cbase >= n_cent        ? 0u
                                : n_cent - cbase >= 32 ? 0xffffffffu
                                                       : (1u << (n_cent - cbase)) - 1u;
-        auto qualify = [&]() {
-          uint32_t m = 0;
+        uint32_t m4[4] = {0, 0, 0, 0};
 #pragma unroll
-          for (int i = 0; i < 32; i++) m |= (__uint_as_float(r[i]) >= thr ? 1u : 0u) << i;
-          return m & valid;
-        };
-        uint32_t m = qualify();
-        if (__any_sync(kFull, cnt + __popc(m) > kCap)) {  // cnt <= kCand after this
-          cnt = cand_compact(bs, bi, tid, cnt);
-          thr = cnt == kCand ? bs[(kCand - 1) * kPtTok + tid] : -INFINITY;
-          m = qualify();
-        }
-        const uint32_t lbase = cbase - tile_begin * kPtCen;
+        for (int i = 0; i < 32; i++) m4[i >> 3] |= (__uint_as_float(r[i]) > thr ? 1u : 0u) << i;
+        uint32_t m = ((m4[0] | m4[1]) | (m4[2] | m4[3])) & valid;
+        if (m) {
 #pragma unroll
-        for (int i = 0; i < 32; i++) {
-          if ((m >> i) & 1u) {  // predicated append
-            bs[cnt * kPtTok + tid] = __uint_as_float(r[i]);
-            bi[cnt * kPtTok + tid] = (uint16_t)(lbase + i);
-            cnt++;
+          for (int i = 0; i < 8; i++)
+            reinterpret_cast<uint4 *>(stage)[i] =
+                make_uint4(r[4 * i], r[4 * i + 1], r[4 * i + 2], r[4 * i + 3]);
+          while (m) {
+            const int i = __ffs(m) - 1;
+            m &= m - 1;
+            const float v = stage[i];
+            if (v > ts[kCand - 1]) topk_insert(ts, td, v, cbase + i);
           }
         }
+        __syncwarp();
       }
     }
     tc_fence_before();
@@ -591,13 +588,13 @@ probe_tc_kernel(const float *__restrict__ q, uint32_t n_tok, const uint8_t *__re
   }
   cp_async_wait<0>();
   if (!s_abort && wait_mma(n_local - 1)) epilogue(n_local - 1);
-  cnt = cand_compact(bs, bi, tid, cnt);
   __syncthreads();
-  // this split's candidates of this token: [token][split][kCand]
+  // this split's candidates of this token: [token][split][kCand], best first
   if (t0 + tid < n_tok && !s_abort) {
-    uint32_t *dst = cand + ((size_t)(t0 + tid) * gridDim.x + blockIdx.x) * kCand;
-    for (int i = 0; i < kCand; i++)
-      dst[i] = i < cnt ? tile_begin * kPtCen + bi[i * kPtTok + tid] : 0xffffffffu;
+    uint4 *dst = reinterpret_cast<uint4 *>(cand + ((size_t)(t0 + tid) * gridDim.x + blockIdx.x) * kCand);
+#pragma unroll
+    for (int i = 0; i < kCand / 4; i++)
+      dst[i] = make_uint4(td[4 * i], td[4 * i + 1], td[4 * i + 2], td[4 * i + 3]);
   }
   tc_fence_before();
   __syncthreads();
@@ -702,8 +699,7 @@ uint32_t probe_tc_cand_per_token(uint32_t n_tok, uint32_t n_cent, int n_sm, uint
   const uint32_t tok_tiles = (n_tok + kPtTok - 1) / kPtTok;
   uint32_t s = (2u * (uint32_t)n_sm + tok_tiles - 1) / tok_tiles;  // ~1 wave of 2 CTAs/SM
   s = std::max(1u, std::min(s, n_tiles));
-  s = std::max(s, (n_tiles + kPtMaxTilesPerSplit - 1) / kPtMaxTilesPerSplit);
-  const uint32_t per = (n_tiles + s - 1) / s;  // <= kPtMaxTilesPerSplit
+  const uint32_t per = (n_tiles + s - 1) / s;
   *splits = (n_tiles + per - 1) / per;
   return *splits * kCand;
 }
