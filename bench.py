@@ -242,7 +242,8 @@ def workload_config(w, path):
 def run_profile_case():
     """A case small enough for ncu (a few GB on the device, one batch per
     search, inputs larger than L2): the raw tokens are freed before searching,
-    so only the compressed index (~0.5 GB) and the working set are resident."""
+    so only the compressed index (~0.5 GB) and the working set are resident.
+    296 queries = 2 filter CTAs per SM."""
     import torch
     from mvr import PREC_BF16, build, synth
     spec = synth.CorpusSpec(200_000, seed=0)
@@ -252,7 +253,7 @@ def run_profile_case():
     g = build.load_built(ix)
     del ix
     torch.cuda.empty_cache()
-    n = 64
+    n = 296
     g.set_batch(n)
     q, _ = synth.queries(spec, n, 32, "cuda", seed=5)
     out_s = torch.empty((n, 10), dtype=torch.float32, device="cuda")
@@ -279,7 +280,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-case", action="store_true",
                     help="small profiling target instead of the bench: 200,000 docs, 16,384 "
-                         "centroids, one mixed-precision and one plain search of 64 queries")
+                         "centroids, one mixed-precision and one plain search of 296 queries")
     ap.add_argument("--recall-sweep", default="",
                     help="extra nprobe:probe_topk settings whose recall@k is reported, "
                          "e.g. 4:100,8:500")
@@ -341,12 +342,14 @@ def main():
 
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
-    def measure(flags, clk=None):
+    def measure(flags, profile=False):
         for _ in range(args.warmup):
             step(flags)
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
+        if profile:  # ncu --profile-from-start off captures exactly the timed steps
+            torch.cuda.profiler.start()
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
               for _ in range(args.steps)]
         acc = dict(stage=np.zeros(6), launches=0, n_cand=0, n_tok=0, n_ent=0)
@@ -361,6 +364,8 @@ def main():
             acc["n_tok"] += st.n_rerank_tok
             acc["n_ent"] += st.n_list_ent
         torch.cuda.synchronize()
+        if profile:
+            torch.cuda.profiler.stop()
         total_ms = mdist.max_over_ranks(sum(a.elapsed_time(b) for a, b in ev), dev)
         if world > 1:
             dist.barrier()
@@ -370,7 +375,7 @@ def main():
 
     plain = measure(PLAIN)
     with ClockSampler(local) as clk:
-        fast = measure(FAST)
+        fast = measure(FAST, profile=True)
     value = fast["qps"]
 
     # end to end: pinned host buffers, copies inside every step
