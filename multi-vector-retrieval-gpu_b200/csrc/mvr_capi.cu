@@ -75,6 +75,14 @@ void dfree(void *p) {
   if (p) cudaFree(p);
 }
 
+// FP32 -> BF16 bits, round to nearest even (finite inputs).
+uint16_t bf16_bits(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  u += 0x7fffu + ((u >> 16) & 1u);
+  return (uint16_t)(u >> 16);
+}
+
 // One decode-table row per byte value: weights of its 8/b values, MSB-first
 // (SQInfoPP ctor, DataStructPP.hpp:150-187).
 std::vector<float> make_lut(uint32_t n_bit, const float *weight) {
@@ -106,6 +114,7 @@ struct Workspace {
   uint32_t *stamp = nullptr;
   uint8_t *rank = nullptr;
   uint64_t *key = nullptr;
+  uint32_t *qcnt = nullptr, *ovf = nullptr;  // [slots] hash-filter counters / overflow flags
   // per batch
   uint32_t batch_slots = 0, tok_cap = 0, np_cap = 0, short_cap = 0, topk_cap = 0;
   size_t part_cap = 0;
@@ -144,6 +153,9 @@ struct mvr_index {
   void *cen_bf16 = nullptr;      // [C][128] BF16 centroid rows
   void *lut_bf16 = nullptr;      // [256][8/b] BF16 decode table
   void *cen_sw = nullptr;        // [C_pad/128][32 KB] swizzled BF16 centroid tiles
+  void *cen_perm = nullptr;      // [C][64] bf16x2 centroid rows, TMEM-rerank K order (b <= 2)
+  uint32_t wlo = 0, whi = 0;     // low / high bytes of the BF16 bucket weights (b <= 2)
+  float x_bound = 0.f;           // bound on the norm of every decoded doc token
   unsigned *d_err = nullptr;     // device error flags of the tensor-core kernels
   Workspace ws;
 
@@ -162,8 +174,8 @@ struct mvr_index {
     if (stream) cudaStreamDestroy(stream);
   }
   void free_scratch() {
-    dfree(ws.stamp); dfree(ws.rank); dfree(ws.key);
-    ws.stamp = nullptr; ws.rank = nullptr; ws.key = nullptr;
+    dfree(ws.stamp); dfree(ws.rank); dfree(ws.key); dfree(ws.qcnt); dfree(ws.ovf);
+    ws.stamp = nullptr; ws.rank = nullptr; ws.key = nullptr; ws.qcnt = nullptr; ws.ovf = nullptr;
     ws.slots = 0;
   }
   void free_batch() {
@@ -206,6 +218,10 @@ int ensure_scratch(mvr_index *h, uint32_t slots, uint32_t rank_stride) {
   MVR_TRY(dalloc(&w.stamp, slots * n));
   MVR_TRY(dalloc(&w.rank, slots * n * rank_stride));
   MVR_TRY(dalloc(&w.key, slots * n));
+  MVR_TRY(dalloc(&w.qcnt, slots));
+  MVR_TRY(dalloc(&w.ovf, slots));
+  CUDA_TRY(cudaMemsetAsync(w.qcnt, 0, slots * sizeof(uint32_t), h->stream));
+  CUDA_TRY(cudaMemsetAsync(w.ovf, 0, slots * sizeof(uint32_t), h->stream));
   CUDA_TRY(cudaMemsetAsync(w.stamp, 0, slots * n * sizeof(uint32_t), h->stream));
   CUDA_TRY(cudaMemsetAsync(w.rank, 0xff, slots * n * rank_stride, h->stream));
   CUDA_TRY(cudaStreamSynchronize(h->stream));
@@ -396,7 +412,7 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
   CUDA_TRY(cudaMemcpyAsync(w.q_off, w.h_off, ((size_t)n_query + n_batch) * sizeof(uint64_t),
                            cudaMemcpyHostToDevice, st));
 
-  FilterScratch scr{w.stamp, w.rank, w.key, h->dix.n_item, w.rank_stride};
+  FilterScratch scr{w.stamp, w.rank, w.key, h->dix.n_item, w.rank_stride, w.qcnt, w.ovf};
   int launches = 0;
   uint64_t h2d = ((size_t)n_query + n_batch) * sizeof(uint64_t), d2h = 0;
   auto ev = [&](uint32_t bt, int k) { return h->events[(size_t)bt * kStages + k]; };
@@ -431,18 +447,23 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
       CUDA_TRY(cudaMemsetAsync(w.stamp, 0, (size_t)w.slots * h->dix.n_item * sizeof(uint32_t), st));
       h->epoch = 1;
     }
-    CUDA_TRY(launch_filter(h->dix, w.probe_id, w.probe_s, nprobe, qo, nb, probe_topk, scr, h->epoch,
-                           w.short_id, w.short_approx, w.n_short, w.qstat + (size_t)s * 3, st,
-                           &launches));
+    CUDA_TRY(launch_filter_hash(h->dix, w.probe_id, w.probe_s, nprobe, qo, nb, probe_topk, scr,
+                                h->epoch, w.short_id, w.short_approx, w.n_short,
+                                w.qstat + (size_t)s * 3, st, &launches));
     CUDA_TRY(cudaEventRecord(ev(bt, 3), st));
     float *os = host_io ? w.out_s : out_s + (size_t)s * topk;
     uint32_t *oi = host_io ? w.out_id : out_id + (size_t)s * topk;
     if (bf16) {
       // BF16 tensor-core MaxSim over the whole shortlist, then the exact FP32
       // kernel re-scores its best R docs
-      CUDA_TRY(launch_rerank_tc(h->dix, h->cen_bf16, h->lut_bf16, qp, qo, nb, w.short_id,
-                                w.n_short, probe_topk, sem, nq_max, w.exact, h->d_err, st,
-                                &launches));
+      if (h->cen_perm)
+        CUDA_TRY(launch_rerank_tmem(h->dix, h->cen_perm, h->wlo, h->whi, qp, qo, nb, w.short_id,
+                                    w.n_short, probe_topk, sem, nq_max, h->x_bound, w.exact,
+                                    h->d_err, st, &launches));
+      else
+        CUDA_TRY(launch_rerank_tc(h->dix, h->cen_bf16, h->lut_bf16, qp, qo, nb, w.short_id,
+                                  w.n_short, probe_topk, sem, nq_max, w.exact, h->d_err, st,
+                                  &launches));
       CUDA_TRY(cudaEventRecord(ev(bt, 4), st));
       CUDA_TRY(launch_topk(w.short_id, w.exact, w.n_short, nb, probe_topk, R, w.r_score, w.r_id,
                            w.n_r, st, &launches));
@@ -540,6 +561,28 @@ int finish_index(mvr_index *h, const uint32_t *item_n_vec_host, const uint32_t *
   MVR_TRY(dalloc(&sw, (size_t)d.n_centroid_pad * 256, &h->bufs));
   CUDA_TRY(make_centroid_tiles(d.centroid, d.n_centroid, d.n_centroid_pad / 64, sw, h->stream));
   h->cen_sw = sw;
+  if (tmem_rerank_supported(d.n_bit)) {
+    uint32_t *cp;
+    MVR_TRY(dalloc(&cp, (size_t)d.n_centroid * 64, &h->bufs));
+    CUDA_TRY(make_centroid_perm(d.centroid, d.n_centroid, d.n_bit, cp, h->stream));
+    h->cen_perm = cp;
+    h->wlo = h->whi = 0;
+    float wmax = 0.f;
+    for (uint32_t k = 0; k < (1u << d.n_bit); k++) wmax = std::max(wmax, std::fabs(weight[k]));
+    float cmax = 0.f;
+    CUDA_TRY(max_centroid_norm(d.centroid, d.n_centroid, h->d_err, &cmax, h->stream));
+    CUDA_TRY(cudaMemsetAsync(h->d_err, 0, sizeof(unsigned), h->stream));  // was scratch
+    h->x_bound = cmax + std::sqrt((float)kDim) * wmax;
+    for (uint32_t k = 0; k < (1u << d.n_bit); k++) {
+      const uint16_t wb = bf16_bits(weight[k]);
+      h->wlo |= (uint32_t)(wb & 0xffu) << (8 * k);
+      h->whi |= (uint32_t)(wb >> 8) << (8 * k);
+    }
+  }
+  uint32_t *ipart;
+  MVR_TRY(dalloc(&ipart, (size_t)d.n_centroid * (kHashParts + 1), &h->bufs));
+  CUDA_TRY(make_ivf_part(d, ipart, h->stream));
+  d.ivf_part = ipart;
   float *ct;
   MVR_TRY(dalloc(&ct, (size_t)kDim * d.n_centroid_pad, &h->bufs));
   CUDA_TRY(launch_transpose_centroid(d.centroid, d.n_centroid, d.n_centroid_pad, ct, h->stream));

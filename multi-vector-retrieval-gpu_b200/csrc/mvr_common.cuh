@@ -12,6 +12,7 @@ constexpr int kMaxQueryTok = 64;   // query tokens per query
 constexpr int kMaxProbe = 32;      // nprobe upper bound
 constexpr int kMaxShort = 8192;    // probe_topk upper bound
 constexpr int kMaxTopk = 1024;
+constexpr int kHashParts = 8;      // doc ranges (CTAs per query) of the hash filter
 
 // Index arrays resident in HBM (one copy per loaded index).
 struct DevIndex {
@@ -28,6 +29,7 @@ struct DevIndex {
   const uint32_t *ivf_size;   // [C]
   const uint32_t *ivf_ids;    // [n_ele_ivf]
   const float *lut;           // [256][8/n_bit] byte -> per-value weight
+  const uint32_t *ivf_part;   // [C][kHashParts + 1] doc-range sub-list starts
 };
 
 // (score desc, id asc) total order used by every top-k on the path.

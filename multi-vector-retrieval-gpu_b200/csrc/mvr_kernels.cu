@@ -227,6 +227,7 @@ probe_merge_kernel(const uint32_t *__restrict__ part_id,
 // probe_topk candidates by the 64-bit key (score desc, id asc).
 // ---------------------------------------------------------------------
 constexpr int kFilterThreads = 1024;
+constexpr int kFilterCluster = 4;  // CTAs (SMs) per query of the rank-table filter
 
 // v * 2^32 rounded to nearest-even, clamped to +-2^62 (exact for |v| >= 2^-9):
 // the approximate score is the exact sum of these terms, rounded once to FP32
@@ -249,28 +250,175 @@ __device__ __forceinline__ uint32_t find_seg(const uint32_t *pref, int n, uint32
   return (uint32_t)lo;
 }
 
+// Cluster form: CL CTAs (one cluster) share one query.  Each CTA takes an
+// interleaved share of every rank's list entries, of the candidates and of
+// the keys; the candidate counter, the shortlist counter and the radix-select
+// histograms are combined through distributed shared memory (CTA 0 holds the
+// counters), and cluster barriers order the phases.  Splitting a query over
+// CL SMs keeps only n_sm / CL queries' rank rows and stamps in flight, a
+// working set that stays in L2.  CL = 1 is the single-CTA kernel.
+template <int CL>
+__device__ __forceinline__ void filter_sync() {
+  if constexpr (CL == 1) {
+    __syncthreads();
+  } else {
+    __threadfence();  // rank bytes / stamps / keys live in global memory
+    asm volatile("barrier.cluster.arrive.release.aligned;\n"
+                 "barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+  }
+}
+
+template <int CL>
+__device__ __forceinline__ uint32_t *cl_ptr(uint32_t *p, uint32_t rank) {
+  if constexpr (CL == 1) {
+    return p;
+  } else {
+    uint32_t *r;
+    asm volatile("mapa.u64 %0, %1, %2;\n" : "=l"(r) : "l"(p), "r"(rank));
+    return r;
+  }
+}
+
+// Shared-memory state of select_emit.
+struct SelectSmem {
+  uint32_t (*hist)[256];  // [2][256]
+  uint32_t *digit, *need, *done;
+};
+
+// Phases C/D of the filter: radix select of the probe_topk largest 64-bit
+// keys among key[0, n_cand) (8-bit digits, high to low, stopping once the
+// boundary digit is unique), then emission of the selected keys as the
+// (unordered) shortlist of query b.  With CL > 1 the CL CTAs of a cluster
+// each take an interleaved share of the keys and add their histograms
+// through distributed shared memory; g_sel / g_stok are CTA 0's counters.
+template <int CL>
+__device__ void select_emit(const DevIndex &ix, const uint64_t *__restrict__ key, uint32_t n_cand,
+                            uint32_t probe_topk, uint32_t b, uint32_t cr, const SelectSmem &sm,
+                            uint32_t *g_sel, uint32_t *g_stok, uint32_t *__restrict__ short_id,
+                            float *__restrict__ short_approx) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t cstride = CL * blockDim.x;
+  const unsigned lt_mask = (1u << lane) - 1u;
+  // ---- phase C: radix select of the probe_topk largest keys ----
+  uint64_t prefix = 0, mask = 0;
+  if (n_cand > probe_topk) {
+    uint32_t need = probe_topk;
+    for (int pass = 0; pass < 8; pass++) {
+      const int shift = 56 - 8 * pass;
+      uint32_t *h = sm.hist[pass & 1];
+      for (int i = tid; i < 256; i += blockDim.x) h[i] = 0;
+      __syncthreads();
+      for (uint32_t i0 = cr * blockDim.x; i0 < n_cand; i0 += cstride) {
+        const uint32_t i = i0 + tid;
+        uint32_t dig = 256;
+        if (i < n_cand) {
+          const uint64_t k = key[i];
+          if ((k & mask) == prefix) dig = (uint32_t)(k >> shift) & 0xffu;
+        }
+        const unsigned grp = __match_any_sync(kFull, dig);
+        if (dig < 256 && lane == __ffs(grp) - 1) atomicAdd(&h[dig], (uint32_t)__popc(grp));
+      }
+      filter_sync<CL>();  // every CTA's histogram of this pass complete
+      if (warp == 0) {
+        // lane l owns bins 255-8l .. 248-8l (high to low), summed over the cluster
+        uint32_t cnt[8], sum = 0;
+#pragma unroll
+        for (int u = 0; u < 8; u++) cnt[u] = 0;
+        for (int r = 0; r < CL; r++) {
+          const uint32_t *hr = cl_ptr<CL>(h, (uint32_t)r);
+#pragma unroll
+          for (int u = 0; u < 8; u++) cnt[u] += hr[255 - 8 * lane - u];
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++) sum += cnt[u];
+        uint32_t incl = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t v = __shfl_up_sync(kFull, incl, o);
+          if (lane >= o) incl += v;
+        }
+        const uint32_t excl = incl - sum;
+        if (excl < need && need <= incl) {
+          uint32_t above = excl;
+#pragma unroll
+          for (int u = 0; u < 8; u++) {
+            if (above < need && need <= above + cnt[u]) {
+              *sm.digit = 255 - 8 * lane - u;
+              *sm.need = need - above;
+              *sm.done = (need - above == cnt[u]) ? 1u : 0u;
+            }
+            above += cnt[u];
+          }
+        }
+      }
+      __syncthreads();
+      prefix |= (uint64_t)*sm.digit << shift;
+      mask |= (uint64_t)0xff << shift;
+      need = *sm.need;
+      if (*sm.done) break;
+    }
+  }
+
+  // ---- phase D: emit the shortlist (unordered) ----
+  for (uint32_t i0 = cr * blockDim.x; i0 < n_cand; i0 += cstride) {
+    const uint32_t i = i0 + tid;
+    uint64_t k = 0;
+    bool sel = false;
+    if (i < n_cand) {
+      k = key[i];
+      sel = (k & mask) >= prefix;
+    }
+    const unsigned m = __ballot_sync(kFull, sel);
+    if (m) {
+      uint32_t base = 0;
+      if (lane == __ffs(m) - 1) base = atomicAdd(g_sel, (uint32_t)__popc(m));
+      base = __shfl_sync(kFull, base, __ffs(m) - 1);
+      const uint32_t pos = base + __popc(m & lt_mask);
+      uint32_t len = 0;
+      if (sel && pos < probe_topk) {
+        short_id[(size_t)b * probe_topk + pos] = key_id(k);
+        short_approx[(size_t)b * probe_topk + pos] = key_score(k);
+        len = ix.item_n_vec[key_id(k)];
+      }
+      const uint32_t tot = __reduce_add_sync(kFull, len);
+      if (lane == 0 && tot) atomicAdd(g_stok, tot);
+    }
+  }
+}
+
+template <int CL>
 __global__ void __launch_bounds__(kFilterThreads, 1)
 filter_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
               const float *__restrict__ probe_s, uint32_t nprobe,
               const uint64_t *__restrict__ q_off, uint32_t probe_topk,
               FilterScratch scr, uint32_t epoch,
               uint32_t *__restrict__ short_id, float *__restrict__ short_approx,
-              uint32_t *__restrict__ n_short_out, uint32_t *__restrict__ qstat) {
+              uint32_t *__restrict__ n_short_out, uint32_t *__restrict__ qstat,
+              uint32_t *__restrict__ only_if) {
   __shared__ long long pfix[kMaxQueryTok * kMaxProbe];
   __shared__ uint32_t pref[kMaxQueryTok + 1];
   __shared__ uint32_t lsz[kMaxQueryTok * kMaxProbe];
   __shared__ uint64_t lof[kMaxQueryTok * kMaxProbe];
-  __shared__ uint32_t hist[256];
-  __shared__ uint32_t s_ncand, s_sel, s_digit, s_need, s_done, s_entries, s_stok;
+  __shared__ uint32_t hist[2][256];
+  __shared__ uint32_t s_ncand, s_sel, s_stok;     // CTA 0's copies are the cluster's
+  __shared__ uint32_t s_digit, s_need, s_done, s_entries;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int n_warp = blockDim.x >> 5;
-  const uint32_t b = blockIdx.x;
+  uint32_t cr = 0;
+  if constexpr (CL > 1) asm volatile("mov.u32 %0, %%cluster_ctarank;\n" : "=r"(cr));
+  const uint32_t b = blockIdx.x / CL;
+  // fallback use: only the queries whose hash-table filter overflowed (the
+  // flag is the same for every CTA of the cluster, read before any barrier)
+  if (only_if && only_if[b] == 0) return;
   const uint64_t tok0 = q_off[b];
   const uint32_t nq = (uint32_t)(q_off[b + 1] - tok0);
   uint32_t *stamp = scr.stamp + (size_t)b * scr.n_item;
   uint8_t *rank = scr.rank + (size_t)b * scr.n_item * scr.rank_stride;
   uint64_t *key = scr.key + (size_t)b * scr.n_item;
+  uint32_t *g_ncand = cl_ptr<CL>(&s_ncand, 0), *g_sel = cl_ptr<CL>(&s_sel, 0),
+           *g_stok = cl_ptr<CL>(&s_stok, 0);
+  const unsigned lt_mask = (1u << lane) - 1u;
 
   // probe scores (fixed point) and list sizes / offsets of every probe
   // (probe id 0xffffffff = no finite score)
@@ -280,10 +428,11 @@ filter_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
     lsz[i] = c < ix.n_centroid ? ix.ivf_size[c] : 0u;
     lof[i] = c < ix.n_centroid ? ix.ivf_off[c] : 0ull;
   }
-  if (tid == 0) { s_ncand = 0; s_entries = 0; s_stok = 0; }
-  __syncthreads();
+  if (tid == 0) { s_ncand = 0; s_sel = 0; s_stok = 0; s_entries = 0; }
+  filter_sync<CL>();  // counters of CTA 0 initialised before any remote update
 
   // ---- phase A: scatter probed lists rank by rank ----
+  const uint32_t gwarp = cr * n_warp + warp, gstride = CL * n_warp * 128;
   for (uint32_t j = 0; j < nprobe; j++) {
     if (warp == 0) {  // exclusive prefix of the nq list sizes of rank j
       const uint32_t s0 = (uint32_t)lane < nq ? lsz[lane * nprobe + j] : 0u;
@@ -306,7 +455,7 @@ filter_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
     __syncthreads();
     const uint32_t total = pref[nq];
     // 4 entries per lane in flight: independent list-id and rank-byte loads
-    for (uint32_t e0 = warp * 128; e0 < total; e0 += n_warp * 128) {
+    for (uint32_t e0 = gwarp * 128; e0 < total; e0 += gstride) {
       uint32_t item[4], tt[4];
       uint8_t rv[4];
 #pragma unroll
@@ -324,27 +473,34 @@ filter_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
         if (tt[u] != 0xffffffffu) rv[u] = rank[(size_t)item[u] * scr.rank_stride + tt[u]];
 #pragma unroll
       for (int u = 0; u < 4; u++) {
+        bool fresh = false;
         if (tt[u] != 0xffffffffu && rv[u] == 0xff) {
           rank[(size_t)item[u] * scr.rank_stride + tt[u]] = (uint8_t)j;
-          if (atomicExch(stamp + item[u], epoch) != epoch) {
-            const uint32_t pos = atomicAdd(&s_ncand, 1u);
-            key[pos] = item[u];
-          }
+          fresh = atomicExch(stamp + item[u], epoch) != epoch;
+        }
+        // warp-aggregated append to the cluster's candidate list
+        const unsigned m = __ballot_sync(kFull, fresh);
+        if (m) {
+          uint32_t base = 0;
+          if (lane == __ffs(m) - 1) base = atomicAdd(g_ncand, (uint32_t)__popc(m));
+          base = __shfl_sync(kFull, base, __ffs(m) - 1);
+          if (fresh) key[base + __popc(m & lt_mask)] = item[u];
         }
       }
     }
-    __syncthreads();
+    filter_sync<CL>();
   }
-  const uint32_t n_cand = s_ncand;
+  const uint32_t n_cand = *g_ncand;
 
   // ---- phase B: approximate score, restore rank rows (2 candidates in flight) ----
-  for (uint32_t i0 = tid; i0 < n_cand; i0 += 2 * blockDim.x) {
+  const uint32_t cstride = CL * blockDim.x;
+  for (uint32_t i0 = cr * blockDim.x + tid; i0 < n_cand; i0 += 2 * cstride) {
     long long ps_acc[2] = {0, 0};
     uint32_t item[2];
     uint8_t *row[2];
 #pragma unroll
     for (int u = 0; u < 2; u++) {
-      const uint32_t i = i0 + u * blockDim.x;
+      const uint32_t i = i0 + u * cstride;
       item[u] = i < n_cand ? (uint32_t)key[i] : 0u;
       row[u] = rank + (size_t)item[u] * scr.rank_stride;
     }
@@ -352,10 +508,10 @@ filter_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
       uint4 w[2];
 #pragma unroll
       for (int u = 0; u < 2; u++)
-        if (i0 + u * blockDim.x < n_cand) w[u] = *reinterpret_cast<uint4 *>(row[u] + t0);
+        if (i0 + u * cstride < n_cand) w[u] = *reinterpret_cast<uint4 *>(row[u] + t0);
 #pragma unroll
       for (int u = 0; u < 2; u++) {
-        if (i0 + u * blockDim.x >= n_cand) continue;
+        if (i0 + u * cstride >= n_cand) continue;
         const uint8_t *bytes = reinterpret_cast<const uint8_t *>(&w[u]);
         long long s = ps_acc[u];
 #pragma unroll
@@ -369,86 +525,203 @@ filter_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
     }
 #pragma unroll
     for (int u = 0; u < 2; u++) {
-      const uint32_t i = i0 + u * blockDim.x;
+      const uint32_t i = i0 + u * cstride;
       if (i < n_cand) key[i] = make_key(from_fixed(ps_acc[u]), item[u]);
     }
   }
-  __syncthreads();
+  filter_sync<CL>();
 
-  // ---- phase C: radix select of the probe_topk largest keys ----
-  uint64_t prefix = 0, mask = 0;
-  if (n_cand > probe_topk) {
-    if (tid == 0) { s_need = probe_topk; s_done = 0; }
-    for (int pass = 0; pass < 8; pass++) {
-      const int shift = 56 - 8 * pass;
-      for (int i = tid; i < 256; i += blockDim.x) hist[i] = 0;
-      __syncthreads();
-      for (uint32_t i0 = 0; i0 < n_cand; i0 += blockDim.x) {
-        const uint32_t i = i0 + tid;
-        uint32_t dig = 256;
-        if (i < n_cand) {
-          const uint64_t k = key[i];
-          if ((k & mask) == prefix) dig = (uint32_t)(k >> shift) & 0xffu;
-        }
-        const unsigned grp = __match_any_sync(kFull, dig);
-        if (dig < 256 && lane == __ffs(grp) - 1) atomicAdd(&hist[dig], (uint32_t)__popc(grp));
-      }
-      __syncthreads();
-      if (warp == 0) {
-        // lane l owns bins 255-8l .. 248-8l (high to low)
-        uint32_t cnt[8], sum = 0;
-#pragma unroll
-        for (int u = 0; u < 8; u++) { cnt[u] = hist[255 - 8 * lane - u]; sum += cnt[u]; }
-        uint32_t incl = sum;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const uint32_t v = __shfl_up_sync(kFull, incl, o);
-          if (lane >= o) incl += v;
-        }
-        const uint32_t excl = incl - sum;
-        const uint32_t need = s_need;
-        if (excl < need && need <= incl) {
-          uint32_t above = excl;
-#pragma unroll
-          for (int u = 0; u < 8; u++) {
-            if (above < need && need <= above + cnt[u]) {
-              s_digit = 255 - 8 * lane - u;
-              s_need = need - above;
-              s_done = (need - above == cnt[u]) ? 1u : 0u;
-            }
-            above += cnt[u];
-          }
-        }
-      }
-      __syncthreads();
-      prefix |= (uint64_t)s_digit << shift;
-      mask |= (uint64_t)0xff << shift;
-      const uint32_t done = s_done;
-      __syncthreads();
-      if (done) break;
-    }
-  }
-
-  // ---- phase D: emit the shortlist (unordered) ----
-  if (tid == 0) s_sel = 0;
-  __syncthreads();
-  for (uint32_t i = tid; i < n_cand; i += blockDim.x) {
-    const uint64_t k = key[i];
-    if ((k & mask) >= prefix) {
-      const uint32_t pos = atomicAdd(&s_sel, 1u);
-      if (pos < probe_topk) {
-        short_id[(size_t)b * probe_topk + pos] = key_id(k);
-        short_approx[(size_t)b * probe_topk + pos] = key_score(k);
-        atomicAdd(&s_stok, ix.item_n_vec[key_id(k)]);
-      }
-    }
-  }
-  __syncthreads();
-  if (tid == 0) {
+  // ---- phases C/D: radix select + emit ----
+  SelectSmem sm{hist, &s_digit, &s_need, &s_done};
+  select_emit<CL>(ix, key, n_cand, probe_topk, b, cr, sm, g_sel, g_stok, short_id, short_approx);
+  filter_sync<CL>();
+  if (cr == 0 && tid == 0) {
     n_short_out[b] = min(s_sel, probe_topk);
     qstat[b * 3 + 0] = n_cand;
     qstat[b * 3 + 1] = s_entries;
     qstat[b * 3 + 2] = s_stok;
+    if (only_if) only_if[b] = 0;
+  }
+}
+
+// ---------------------------------------------------------------------
+// Hash-table filter (main search path).  kHashParts CTAs share a query; CTA
+// p owns the docs [p * n_item / P, (p + 1) * n_item / P) and keeps one
+// shared-memory hash-table slot per candidate doc of its range: doc id, the
+// mask of query tokens that have visited it and the exact fixed-point sum of
+// the first-visit probe scores.  The IVF lists are sorted by doc id, so the
+// CTA's part of each probed list is the contiguous sub-list given by the
+// index's partition table (ivf_part).  Warp w walks token w's sub-lists in
+// probe-rank order (probes are sorted best-first), so the token's first
+// visit of a doc carries the max over its probes; different tokens only meet
+// in the order-free atomics (OR of the mask, integer add of the score).
+// score = sum over tokens of those maxima, the same value the rank-table
+// filter computes.  Each candidate's 64-bit (score, id) key goes to the
+// query's key array, from which filter_select_kernel takes the shortlist.  A
+// CTA whose range holds more than kHashFill candidates marks the query in
+// scr.ovf and the rank-table filter redoes that query.
+// ---------------------------------------------------------------------
+constexpr uint32_t kHashLog = 13, kHashCap = 1u << kHashLog;  // slots per CTA
+constexpr uint32_t kHashFill = 7168;                          // inserts allowed per CTA
+constexpr uint32_t kEmpty = 0xffffffffu;
+
+__host__ __device__ constexpr size_t hash_smem_bytes(int mw) {
+  return (size_t)kHashCap * (4 + 4 * mw + 8);
+}
+
+template <int MW>
+__global__ void __launch_bounds__(kFilterThreads, 1)
+filter_hash_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
+                   const float *__restrict__ probe_s, uint32_t nprobe,
+                   const uint64_t *__restrict__ q_off, FilterScratch scr,
+                   uint32_t *__restrict__ qstat) {
+  extern __shared__ __align__(16) uint8_t hsm[];
+  uint32_t *tkey = reinterpret_cast<uint32_t *>(hsm);                      // [cap]
+  uint32_t *tmask = tkey + kHashCap;                                       // [cap][MW]
+  unsigned long long *tacc = reinterpret_cast<unsigned long long *>(tmask + kHashCap * MW);
+  __shared__ long long pfix[kMaxQueryTok * kMaxProbe];
+  __shared__ uint32_t lsz[kMaxQueryTok * kMaxProbe];   // this CTA's sub-list sizes
+  __shared__ uint64_t lof[kMaxQueryTok * kMaxProbe];   // and offsets in ivf_ids
+  __shared__ uint32_t s_fill, s_ovf, s_entries;
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int n_warp = blockDim.x >> 5;
+  const uint32_t b = blockIdx.x / kHashParts, part = blockIdx.x % kHashParts;
+  const uint64_t tok0 = q_off[b];
+  const uint32_t nq = (uint32_t)(q_off[b + 1] - tok0);
+  const unsigned lt_mask = (1u << lane) - 1u;
+
+  for (uint32_t i = tid; i < kHashCap; i += blockDim.x) {
+    tkey[i] = kEmpty;
+    tacc[i] = 0ull;
+#pragma unroll
+    for (int w = 0; w < MW; w++) tmask[i * MW + w] = 0u;
+  }
+  if (tid == 0) { s_fill = 0; s_ovf = 0; s_entries = 0; }
+  __syncthreads();
+  uint32_t ent = 0;
+  for (uint32_t i = tid; i < nq * nprobe; i += blockDim.x) {
+    const uint32_t c = probe_id[tok0 * nprobe + i];
+    pfix[i] = to_fixed(probe_s[tok0 * nprobe + i]);
+    uint32_t p0 = 0, p1 = 0;
+    uint64_t o = 0;
+    if (c < ix.n_centroid) {
+      const uint32_t *pt = ix.ivf_part + (size_t)c * (kHashParts + 1) + part;
+      p0 = pt[0];
+      p1 = pt[1];
+      o = ix.ivf_off[c];
+      ent += ix.ivf_size[c];
+    }
+    lsz[i] = p1 - p0;
+    lof[i] = o + p0;
+  }
+  if (part == 0) {
+    ent = __reduce_add_sync(kFull, ent);
+    if (lane == 0 && ent) atomicAdd(&s_entries, ent);
+  }
+  __syncthreads();
+
+  for (uint32_t t = warp; t < nq; t += n_warp) {
+    const uint32_t bit = 1u << (t & 31), word = t >> 5;
+    for (uint32_t j = 0; j < nprobe; j++) {
+      const uint32_t sz = lsz[t * nprobe + j];
+      const uint32_t *ids = ix.ivf_ids + lof[t * nprobe + j];
+      const unsigned long long add = (unsigned long long)pfix[t * nprobe + j];
+      for (uint32_t p = lane; p < sz; p += 32) {
+        const uint32_t it = __ldg(ids + p);
+        // find or insert `it` (linear probing; the fill limit keeps >= 1024
+        // slots empty, so the walk ends)
+        uint32_t h = (it * 2654435769u) >> (32 - kHashLog);
+        uint32_t slot = kEmpty;
+        for (uint32_t step = 0; step < kHashCap; step++) {
+          const uint32_t k = *reinterpret_cast<volatile uint32_t *>(&tkey[h]);
+          if (k == it) { slot = h; break; }
+          if (k == kEmpty) {
+            if (atomicAdd(&s_fill, 1u) >= kHashFill) { s_ovf = 1; break; }
+            const uint32_t old = atomicCAS(&tkey[h], kEmpty, it);
+            if (old == kEmpty) { slot = h; break; }
+            atomicSub(&s_fill, 1u);  // lost the slot to another insert
+            if (old == it) { slot = h; break; }
+          }
+          h = (h + 1) & (kHashCap - 1);
+        }
+        if (slot == kEmpty) continue;
+        const uint32_t old = atomicOr(&tmask[slot * MW + word], bit);
+        if (!(old & bit)) atomicAdd(&tacc[slot], add);
+      }
+      __syncwarp();  // rank j of token t before rank j + 1
+    }
+  }
+  __syncthreads();
+
+  // emit this CTA's candidates as (score, id) keys
+  uint64_t *key = scr.key + (size_t)b * scr.n_item;
+  for (uint32_t s0 = 0; s0 < kHashCap; s0 += blockDim.x) {
+    const uint32_t sl = s0 + tid;
+    const uint32_t k = sl < kHashCap ? tkey[sl] : kEmpty;
+    const bool has = k != kEmpty;
+    const unsigned m = __ballot_sync(kFull, has);
+    if (m) {
+      uint32_t base = 0;
+      if (lane == __ffs(m) - 1) base = atomicAdd(scr.qcnt + b, (uint32_t)__popc(m));
+      base = __shfl_sync(kFull, base, __ffs(m) - 1);
+      if (has) key[base + __popc(m & lt_mask)] = make_key(from_fixed((long long)tacc[sl]), k);
+    }
+  }
+  if (tid == 0) {
+    if (s_ovf) atomicOr(scr.ovf + b, 1u);
+    if (part == 0) qstat[b * 3 + 1] = s_entries;
+  }
+}
+
+// ivf_part[c][p] = first position of list c whose doc id is >= p * n_item / P
+// (p = 0..P): the doc-range sub-lists of the hash filter.
+__global__ void ivf_part_kernel(const uint64_t *__restrict__ ivf_off,
+                                const uint32_t *__restrict__ ivf_size,
+                                const uint32_t *__restrict__ ivf_ids, uint32_t n_cent,
+                                uint32_t n_item, uint32_t *__restrict__ out) {
+  const size_t n = (size_t)n_cent * (kHashParts + 1);
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t c = (uint32_t)(i / (kHashParts + 1)), p = (uint32_t)(i % (kHashParts + 1));
+    const uint32_t bound = (uint32_t)((uint64_t)p * n_item / kHashParts);
+    const uint32_t *l = ivf_ids + ivf_off[c];
+    uint32_t lo = 0, hi = ivf_size[c];
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (l[mid] < bound) lo = mid + 1; else hi = mid;
+    }
+    out[i] = lo;
+  }
+}
+
+cudaError_t make_ivf_part(const DevIndex &ix, uint32_t *out, cudaStream_t st) {
+  ivf_part_kernel<<<592, 256, 0, st>>>(ix.ivf_off, ix.ivf_size, ix.ivf_ids, ix.n_centroid,
+                                       ix.n_item, out);
+  return cudaGetLastError();
+}
+
+// Shortlist of every query from the keys filter_hash_kernel emitted; resets
+// the query's key counter for the next batch.
+__global__ void __launch_bounds__(kFilterThreads, 1)
+filter_select_kernel(DevIndex ix, uint32_t probe_topk, FilterScratch scr,
+                     uint32_t *__restrict__ short_id, float *__restrict__ short_approx,
+                     uint32_t *__restrict__ n_short_out, uint32_t *__restrict__ qstat) {
+  __shared__ uint32_t hist[2][256];
+  __shared__ uint32_t s_sel, s_stok, s_digit, s_need, s_done;
+  const uint32_t b = blockIdx.x;
+  const uint32_t n_cand = scr.qcnt[b];
+  if (threadIdx.x == 0) { s_sel = 0; s_stok = 0; }
+  __syncthreads();
+  SelectSmem sm{hist, &s_digit, &s_need, &s_done};
+  select_emit<1>(ix, scr.key + (size_t)b * scr.n_item, n_cand, probe_topk, b, 0, sm, &s_sel,
+                 &s_stok, short_id, short_approx);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    n_short_out[b] = min(s_sel, probe_topk);
+    qstat[b * 3 + 0] = n_cand;
+    qstat[b * 3 + 2] = s_stok;
+    scr.qcnt[b] = 0;
   }
 }
 
@@ -658,6 +931,12 @@ cudaError_t configure_kernels() {
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(rerank_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rerank_smem_bytes(8));
   if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(filter_hash_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)hash_smem_bytes(1));
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(filter_hash_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)hash_smem_bytes(2));
+  if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)(kMaxShort * sizeof(uint64_t)));
 }
@@ -700,10 +979,62 @@ cudaError_t launch_filter(const DevIndex &ix, const uint32_t *probe_id,
                           uint32_t epoch, uint32_t *short_id,
                           float *short_approx, uint32_t *n_short,
                           uint32_t *qstat, cudaStream_t st, int *n_launch) {
-  filter_kernel<<<n_query, kFilterThreads, 0, st>>>(ix, probe_id, probe_s, nprobe, q_off, probe_topk,
-                                                    scr, epoch, short_id, short_approx, n_short, qstat);
+  filter_kernel<1><<<n_query, kFilterThreads, 0, st>>>(ix, probe_id, probe_s, nprobe, q_off,
+                                                       probe_topk, scr, epoch, short_id,
+                                                       short_approx, n_short, qstat, nullptr);
   *n_launch += 1;
   return cudaGetLastError();
+}
+
+cudaError_t launch_filter_cluster(const DevIndex &ix, const uint32_t *probe_id,
+                                  const float *probe_s, uint32_t nprobe,
+                                  const uint64_t *q_off, uint32_t n_query,
+                                  uint32_t probe_topk, const FilterScratch &scr,
+                                  uint32_t epoch, uint32_t *short_id,
+                                  float *short_approx, uint32_t *n_short,
+                                  uint32_t *qstat, cudaStream_t st, int *n_launch,
+                                  uint32_t *only_if) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(n_query * kFilterCluster, 1, 1);
+  cfg.blockDim = dim3(kFilterThreads, 1, 1);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = kFilterCluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaError_t e = cudaLaunchKernelEx(&cfg, filter_kernel<kFilterCluster>, ix, probe_id, probe_s,
+                                     nprobe, q_off, probe_topk, scr, epoch, short_id,
+                                     short_approx, n_short, qstat, only_if);
+  *n_launch += 1;
+  return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+cudaError_t launch_filter_hash(const DevIndex &ix, const uint32_t *probe_id,
+                               const float *probe_s, uint32_t nprobe,
+                               const uint64_t *q_off, uint32_t n_query,
+                               uint32_t probe_topk, const FilterScratch &scr,
+                               uint32_t epoch, uint32_t *short_id,
+                               float *short_approx, uint32_t *n_short,
+                               uint32_t *qstat, cudaStream_t st, int *n_launch) {
+  if (scr.rank_stride <= 32)
+    filter_hash_kernel<1><<<n_query * kHashParts, kFilterThreads, hash_smem_bytes(1), st>>>(
+        ix, probe_id, probe_s, nprobe, q_off, scr, qstat);
+  else
+    filter_hash_kernel<2><<<n_query * kHashParts, kFilterThreads, hash_smem_bytes(2), st>>>(
+        ix, probe_id, probe_s, nprobe, q_off, scr, qstat);
+  filter_select_kernel<<<n_query, kFilterThreads, 0, st>>>(ix, probe_topk, scr, short_id,
+                                                          short_approx, n_short, qstat);
+  *n_launch += 2;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  // queries whose candidates overflowed a hash table: rank-table filter
+  return launch_filter_cluster(ix, probe_id, probe_s, nprobe, q_off, n_query, probe_topk, scr,
+                               epoch, short_id, short_approx, n_short, qstat, st, n_launch,
+                               scr.ovf);
 }
 
 cudaError_t launch_rerank(const DevIndex &ix, const float *q, const uint64_t *q_off,

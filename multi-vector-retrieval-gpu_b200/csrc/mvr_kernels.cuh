@@ -13,9 +13,13 @@ struct FilterScratch {
   uint64_t *key;         // [slots][n_item] candidate (score, id) keys
   uint32_t n_item;
   uint32_t rank_stride;  // 32 or 64 (>= query tokens, multiple of 16)
+  uint32_t *qcnt;        // [slots] candidate keys emitted by the hash filter (0 between batches)
+  uint32_t *ovf;         // [slots] 1: the hash filter overflowed (0 between batches)
 };
 
 cudaError_t configure_kernels();
+// ivf_part table of an index ([C][kHashParts + 1] u32)
+cudaError_t make_ivf_part(const DevIndex &ix, uint32_t *out, cudaStream_t st);
 int probe_splits(uint32_t n_tok, uint32_t n_cent_pad, int n_sm);
 cudaError_t launch_probe(const DevIndex &ix, const float *q, uint32_t n_tok,
                          uint32_t nprobe, int n_split, uint32_t *part_id,
@@ -30,6 +34,25 @@ cudaError_t launch_filter(const DevIndex &ix, const uint32_t *probe_id,
                           uint32_t *qstat /*[n_query][3]: n_cand, list entries
                                             visited, shortlist tokens*/,
                           cudaStream_t st, int *n_launch);
+// The same filter with each query split over a cluster of 4 CTAs; with
+// only_if set, only the queries whose flag is set run (and clear it).
+cudaError_t launch_filter_cluster(const DevIndex &ix, const uint32_t *probe_id,
+                                  const float *probe_s, uint32_t nprobe,
+                                  const uint64_t *q_off, uint32_t n_query,
+                                  uint32_t probe_topk, const FilterScratch &scr,
+                                  uint32_t epoch, uint32_t *short_id,
+                                  float *short_approx, uint32_t *n_short,
+                                  uint32_t *qstat, cudaStream_t st, int *n_launch,
+                                  uint32_t *only_if);
+// Main-path filter: shared-memory hash tables over doc ranges (8 CTAs per
+// query), a select kernel, and the rank-table filter for overflowed queries.
+cudaError_t launch_filter_hash(const DevIndex &ix, const uint32_t *probe_id,
+                               const float *probe_s, uint32_t nprobe,
+                               const uint64_t *q_off, uint32_t n_query,
+                               uint32_t probe_topk, const FilterScratch &scr,
+                               uint32_t epoch, uint32_t *short_id,
+                               float *short_approx, uint32_t *n_short,
+                               uint32_t *qstat, cudaStream_t st, int *n_launch);
 cudaError_t launch_rerank(const DevIndex &ix, const float *q, const uint64_t *q_off,
                           uint32_t n_query, const uint32_t *short_id,
                           const uint32_t *n_short, uint32_t probe_topk,

@@ -18,6 +18,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <cstring>
 
 namespace mvr {
 
@@ -387,6 +388,379 @@ rerank_tc_kernel(DevIndex ix, const __nv_bfloat16 *__restrict__ cen_bf16,
 }
 
 // ---------------------------------------------------------------------
+// rerank_tmem_kernel: BF16 MaxSim for 1- and 2-bit residual codes with the
+// doc-token operand in tensor memory.
+//
+// Per 128-token tile every thread decodes one half row (64 dims) in
+// registers and writes it to TMEM with tcgen05.st; tcgen05.mma then reads A
+// (M = 128 doc tokens, K = 128) from TMEM and B (the query tokens, N = 32 or
+// 64) from a swizzled shared-memory tile, so the decoded tile never passes
+// through shared memory.  Decode of one 32-bit residual word (4*VPB dims)
+// needs no table lookups: the codes j of the four bytes are isolated with one
+// shift and mask, turned into PRMT byte selectors with one IMAD
+// (k -> k | (k+4) << 4 per byte), and two PRMTs pick the low / high bytes of
+// the BF16 bucket weights held in two registers, giving bf16x2 words that a
+// HADD2 adds to the centroid's.  That fixes the order of K inside each word's
+// block of 4*VPB dims: position 4j + 2h + e holds dim VPB*(2h + e) + j.  The
+// centroid rows (cen_perm) and the query tile are stored in the same order,
+// so the contraction is unchanged.  Two A stages and three D stages in TMEM:
+// iteration i issues tile i's loads, runs the epilogue of tile i-2 (its MMA
+// was issued a whole iteration earlier, so the completion wait is short;
+// tcgen05.ld, per-doc max with warp REDUX, shared-memory atomicMax), decodes
+// tile i into A[i%2] and issues its MMA into D[i%3].  Every D stage starts
+// at OFF, a power of two above |q.x| for every pair of the CTA (Cauchy-
+// Schwarz with the query norms and the index's bound on |x|), so D holds
+// positive floats whose bit patterns order like integers: the epilogue takes
+// full-warp REDUX.MAX of the raw bits per doc group and re-arms the stage
+// with OFF after reading it.
+// ---------------------------------------------------------------------
+constexpr int kTmTile = 128;
+constexpr int kTmDocs = 64;       // shortlisted docs per CTA
+constexpr int kTmThreads = 256;   // warp w: TMEM lane quadrant w & 3, half row w >> 2
+// TMEM columns: A[2] x 64 + D[3] x N  (N = 32: 224 -> 256, 2 CTAs per SM;
+// N = 64: 320 -> 512, one CTA per SM, enforced through the smem size)
+__host__ __device__ constexpr uint32_t tm_cols(uint32_t n_max) { return n_max <= 32 ? 256u : 512u; }
+
+template <int NBIT>
+__host__ __device__ constexpr uint32_t tm_dim_of(uint32_t kappa) {
+  constexpr uint32_t VPB = 8 / NBIT, WD = 4 * VPB;
+  const uint32_t m = kappa / WD, r = kappa % WD;
+  return m * WD + VPB * (r % 4) + r / 4;
+}
+
+__host__ __device__ constexpr size_t tm_smem_bytes(uint32_t n_max) {
+  return n_max <= 32 ? 1024 + (size_t)n_max * 256 : 120 * 1024;  // dynamic part: B tile
+}
+
+__device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
+  uint32_t d;
+  asm("prmt.b32 %0, %1, %2, %3;\n" : "=r"(d) : "r"(a), "r"(b), "r"(sel));
+  return d;
+}
+
+__device__ __forceinline__ uint32_t hadd2_u32(uint32_t a, uint32_t b) {
+  __nv_bfloat162 r = __hadd2(*reinterpret_cast<__nv_bfloat162 *>(&a),
+                             *reinterpret_cast<__nv_bfloat162 *>(&b));
+  return *reinterpret_cast<uint32_t *>(&r);
+}
+
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+      "%14,%15,%16};\n" ::"r"(taddr),
+      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]),
+      "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]),
+      "r"(r[15])
+      : "memory");
+}
+
+// the same word into 16 consecutive TMEM columns of the warp's 32 lanes
+__device__ __forceinline__ void tmem_fill16(uint32_t taddr, uint32_t x) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,"
+      "%1,%1};\n" ::"r"(taddr), "r"(x)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_bf16_ta(uint32_t tmem_d, uint32_t tmem_a, uint64_t b,
+                                            uint32_t idesc, uint32_t accum) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n}\n" ::"r"(tmem_d),
+      "r"(tmem_a), "l"(b), "r"(idesc), "r"(accum)
+      : "memory");
+}
+
+// 16 output columns (bf16x2) of one half row from WPS residual words
+// (WPS = 16 / (2 * VPB): 2 words for 2-bit, 1 for 1-bit) and 4 uint4 of the
+// permuted centroid row.
+template <int NBIT>
+__device__ __forceinline__ void tm_decode16(const uint32_t *res, const uint4 *cen, uint32_t wlo,
+                                            uint32_t whi, uint32_t (&out)[16]) {
+  constexpr int VPB = 8 / NBIT;
+  constexpr uint32_t MASK = NBIT == 2 ? 0x03030303u : 0x01010101u;
+  constexpr int WPS = 16 / (2 * VPB);
+#pragma unroll
+  for (int wi = 0; wi < WPS; wi++) {
+    const uint32_t w = res[wi];
+#pragma unroll
+    for (int j = 0; j < VPB; j++) {
+      const uint32_t x = (w >> (8 - NBIT * (j + 1))) & MASK;
+      const uint32_t t = x * 0x11u + 0x40404040u;
+      out[wi * 2 * VPB + 2 * j] = prmt(wlo, whi, t);
+      out[wi * 2 * VPB + 2 * j + 1] = prmt(wlo, whi, t >> 16);
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    out[4 * c + 0] = hadd2_u32(cen[c].x, out[4 * c + 0]);
+    out[4 * c + 1] = hadd2_u32(cen[c].y, out[4 * c + 1]);
+    out[4 * c + 2] = hadd2_u32(cen[c].z, out[4 * c + 2]);
+    out[4 * c + 3] = hadd2_u32(cen[c].w, out[4 * c + 3]);
+  }
+}
+
+template <int NBIT>
+__global__ void __launch_bounds__(kTmThreads, 2)
+rerank_tmem_kernel(DevIndex ix, const uint32_t *__restrict__ cen_perm, uint32_t wlo, uint32_t whi,
+                   const float *__restrict__ q, const uint64_t *__restrict__ q_off,
+                   const uint32_t *__restrict__ short_id, const uint32_t *__restrict__ n_short,
+                   uint32_t probe_topk, int semantics, uint32_t n_max, float x_bound,
+                   float *__restrict__ approx, unsigned *__restrict__ err) {
+  constexpr int VPB = 8 / NBIT;
+  constexpr int HW = 64 / (4 * VPB);  // residual words of a 64-dim half row (4 or 2)
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint8_t *Bq = smem;                                      // [2 K-blocks][n_max rows][128 B]
+  __shared__ uint32_t best[kTmDocs * kMaxQueryTok];        // [doc][query token], bits of OFF + max
+  __shared__ uint32_t s_qss;                               // max squared query-token norm
+  __shared__ __align__(16) uint32_t stage[kTmThreads / 32][16];  // per-warp epilogue staging
+  __shared__ uint64_t bar[2];
+  __shared__ uint32_t tmem_base_s;
+  __shared__ uint32_t d_len[kTmDocs], d_pref[kTmDocs + 1];
+  __shared__ uint64_t d_off[kTmDocs];
+  __shared__ int tok_doc[3][kTmTile];
+  __shared__ int s_abort;
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t b = blockIdx.y;
+  const uint32_t ns = n_short[b];
+  const uint32_t d0 = blockIdx.x * kTmDocs;
+  if (d0 >= ns) return;  // uniform: before any TMEM / barrier use
+  const uint32_t nd = min((uint32_t)kTmDocs, ns - d0);
+  const uint64_t tok0 = q_off[b];
+  const uint32_t nq = (uint32_t)(q_off[b + 1] - tok0);
+  const uint32_t N = nq <= 32 ? 32u : 64u;  // <= n_max (host sizes smem by the batch)
+  const uint32_t idesc = idesc_bf16(kTmTile, (int)N);
+  const uint32_t n_cols = tm_cols(n_max);
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     smem_u32(&tmem_base_s)),
+                 "r"(n_cols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    s_abort = 0;
+    s_qss = 0;
+  }
+  if (tid < (int)nd) {
+    const uint32_t it = short_id[(size_t)b * probe_topk + d0 + tid];
+    d_len[tid] = ix.item_n_vec[it];
+    d_off[tid] = ix.item_off[it];
+  }
+  for (int i = tid; i < kMaxQueryTok * kTmDocs; i += kTmThreads) best[i] = 0u;
+  __syncthreads();  // s_qss
+  // query tokens -> B operand (BF16, permuted K order, swizzled, rows >= nq
+  // zero); the 16 lanes of a row also sum its squares (fixed shuffle order)
+  for (int i = tid; i < (int)N * 16; i += kTmThreads) {  // N * 16 is a multiple of 256
+    const int row = i >> 4, ch = i & 15;  // 16 chunks of 8 positions
+    uint32_t v[4] = {0, 0, 0, 0};
+    float ss = 0.0f;
+    if ((uint32_t)row < nq) {
+      const float *src = q + (tok0 + row) * kDim;
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const float lo = __ldg(src + tm_dim_of<NBIT>(8 * ch + 2 * u));
+        const float hi = __ldg(src + tm_dim_of<NBIT>(8 * ch + 2 * u + 1));
+        ss = fmaf(lo, lo, fmaf(hi, hi, ss));
+        __nv_bfloat162 p = __floats2bfloat162_rn(lo, hi);
+        v[u] = *reinterpret_cast<uint32_t *>(&p);
+      }
+    }
+    *reinterpret_cast<uint4 *>(Bq + (ch >> 3) * (N * 128) + sw128_off(row, ch & 7)) =
+        make_uint4(v[0], v[1], v[2], v[3]);
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) ss += __shfl_xor_sync(kFull, ss, o);
+    if ((lane & 15) == 0) atomicMax(&s_qss, __float_as_uint(ss));
+  }
+  __syncthreads();
+  if (tid == 0) {
+    uint32_t acc = 0;
+    for (uint32_t i = 0; i < nd; i++) { d_pref[i] = acc; acc += d_len[i]; }
+    d_pref[nd] = acc;
+  }
+  fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_s;
+  const uint32_t n_tok = d_pref[nd];
+  // OFF: smallest power of two >= 1 above max |q| * |x| (margin for BF16 rounding)
+  const float off = fmaxf(1.0f, exp2f(ceilf(log2f(sqrtf(__uint_as_float(s_qss)) * x_bound * 1.02f + 1e-30f))));
+  const uint32_t off_bits = __float_as_uint(off);
+  const uint32_t n_tiles = (n_tok + kTmTile - 1) / kTmTile;
+  const uint32_t b_base = smem_u32(Bq);
+  const uint32_t qd = warp & 3, hf = warp >> 2;
+  const uint32_t row = 32 * qd + lane;
+  const uint32_t lane_off = (32u * qd) << 16;
+
+  // per-thread row cursor: (doc, vector id) of this thread's row of a tile
+  uint32_t di = 0;
+  auto locate = [&](uint32_t tile, int &doc, uint64_t &v) {
+    const uint32_t s = tile * kTmTile + row;
+    doc = -1;
+    v = 0;
+    if (tile < n_tiles && s < n_tok) {
+      while (d_pref[di + 1] <= s) di++;
+      doc = (int)di;
+      v = d_off[di] + (s - d_pref[di]);
+    }
+  };
+  auto load_res = [&](uint64_t v, uint32_t (&r)[HW]) {
+    const uint8_t *p = ix.residual + v * ix.bytes_per_vec + hf * (HW * 4);
+    if constexpr (HW == 4) {
+      const uint4 t = __ldg(reinterpret_cast<const uint4 *>(p));
+      r[0] = t.x; r[1] = t.y; r[2] = t.z; r[3] = t.w;
+    } else {
+      const uint2 t = __ldg(reinterpret_cast<const uint2 *>(p));
+      r[0] = t.x; r[1] = t.y;
+    }
+  };
+
+  // every D stage starts at OFF (this warp's quadrant and column half)
+  for (uint32_t st = 0; st < 3; st++)
+    for (uint32_t c0 = hf * (N / 2); c0 < (hf + 1) * (N / 2); c0 += 16)
+      tmem_fill16(tmem + lane_off + 128u + N * st + c0, off_bits);
+
+  auto epilogue = [&](uint32_t tile) {
+    const bool ok = __all_sync(kFull, mbar_wait(&bar[tile & 1], (tile >> 1) & 1));
+    if (!ok) {  // warp-uniform: record, skip, stop after the next barrier
+      if (lane == 0) { atomicOr(err, 4u); s_abort = 1; }
+      return;
+    }
+    tc_fence_after();
+    const int doc = tok_doc[tile % 3][row];
+    const uint32_t dcol = tmem + lane_off + 128u + N * (tile % 3);
+    for (uint32_t c0 = hf * (N / 2); c0 < (hf + 1) * (N / 2); c0 += 16) {
+      uint32_t v[16];
+      tmem_ld16(dcol + c0, v);
+      tmem_fill16(dcol + c0, off_bits);  // re-arm the stage for tile + 3
+      // doc groups of this warp's 32 rows, one uniform pass each: 16 full-warp
+      // REDUX, the maxima staged in shared memory, one atomicMax by 16 lanes
+      unsigned rem = __ballot_sync(kFull, doc >= 0);
+      while (rem) {
+        const int g = __shfl_sync(kFull, doc, __ffs(rem) - 1);
+        const bool in = doc == g;
+        rem &= ~__ballot_sync(kFull, in);
+        uint32_t m[16];
+#pragma unroll
+        for (int j = 0; j < 16; j++) m[j] = __reduce_max_sync(kFull, in ? v[j] : 0u);
+        if (lane == 0) {
+          uint4 *dst = reinterpret_cast<uint4 *>(stage[warp]);
+#pragma unroll
+          for (int u = 0; u < 4; u++) dst[u] = make_uint4(m[4 * u], m[4 * u + 1], m[4 * u + 2], m[4 * u + 3]);
+        }
+        __syncwarp();
+        if (lane < 16 && c0 + lane < nq) atomicMax(&best[g * kMaxQueryTok + c0 + lane], stage[warp][lane]);
+        __syncwarp();
+      }
+    }
+    tc_fence_before();
+  };
+
+  int doc_c;
+  uint64_t v_c;
+  uint32_t code_c = 0, res_c[HW];
+  locate(0, doc_c, v_c);
+  if (doc_c >= 0) {
+    code_c = __ldg(ix.vq_code + v_c);
+    load_res(v_c, res_c);
+  }
+  for (uint32_t tile = 0; tile < n_tiles; tile++) {
+    const int st = tile & 1;
+    // centroid half row of this tile (permuted BF16, 8 x 16 B)
+    uint4 cen[8];
+    if (doc_c >= 0) {
+      const uint4 *cp = reinterpret_cast<const uint4 *>(cen_perm + (size_t)code_c * 64 + hf * 32);
+#pragma unroll
+      for (int u = 0; u < 8; u++) cen[u] = __ldg(cp + u);
+    }
+    // next tile's code and residual words
+    int doc_n;
+    uint64_t v_n;
+    uint32_t code_n = 0, res_n[HW];
+    locate(tile + 1, doc_n, v_n);
+    if (doc_n >= 0) {
+      code_n = __ldg(ix.vq_code + v_n);
+      load_res(v_n, res_n);
+    }
+    if (tile > 1) epilogue(tile - 2);  // its MMA completed during the previous iteration
+    if (hf == 0) tok_doc[tile % 3][row] = doc_c;
+    const uint32_t acol = tmem + lane_off + 64u * st + 32u * hf;
+#pragma unroll
+    for (int part = 0; part < 2; part++) {
+      uint32_t out[16];
+      if (doc_c >= 0) {
+        tm_decode16<NBIT>(res_c + part * (HW / 2), cen + part * 4, wlo, whi, out);
+      } else {
+#pragma unroll
+        for (int u = 0; u < 16; u++) out[u] = 0u;
+      }
+      tmem_st16(acol + 16u * part, out);
+    }
+    asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    if (s_abort) break;
+    if (tid == 0) {
+      tc_fence_after();
+      const uint32_t dcol = tmem + 128u + N * (tile % 3);
+#pragma unroll
+      for (int kk = 0; kk < 8; kk++) {
+        const uint64_t bd = sw128_desc(b_base + (kk >> 2) * (N * 128) + (kk & 3) * 32);
+        mma_bf16_ta(dcol, tmem + 64u * st + 8u * kk, bd, idesc, 1u);  // D starts at OFF
+      }
+      mma_commit(&bar[st]);
+    }
+    doc_c = doc_n;
+    v_c = v_n;
+    code_c = code_n;
+#pragma unroll
+    for (int u = 0; u < HW; u++) res_c[u] = res_n[u];
+  }
+  if (!s_abort && n_tiles > 1) epilogue(n_tiles - 2);
+  if (!s_abort && n_tiles > 0) epilogue(n_tiles - 1);
+  __syncthreads();
+
+  if (tid < (int)nd && !s_abort) {
+    const bool clamp = semantics == 1 && d_len[tid] < ix.max_item_n_vec;
+    float s = 0.0f;
+    for (uint32_t t = 0; t < nq; t++) {
+      float m = __uint_as_float(best[tid * kMaxQueryTok + t]) - off;
+      if (clamp) m = fmaxf(m, 0.0f);
+      s += m;
+    }
+    approx[(size_t)b * probe_topk + d0 + tid] = s;
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(n_cols));
+  }
+}
+
+// cen_perm[c][w] = bf16x2 of centroid c at K positions 2w, 2w+1 of the
+// rerank_tmem_kernel order.
+template <int NBIT>
+__global__ void perm_centroid_kernel(const float *__restrict__ cen, uint32_t n_cent,
+                                     uint32_t *__restrict__ out) {
+  const size_t n = (size_t)n_cent * 64;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const size_t c = i / 64;
+    const uint32_t w = (uint32_t)(i % 64);
+    const float *row = cen + c * kDim;
+    __nv_bfloat162 p = __floats2bfloat162_rn(row[tm_dim_of<NBIT>(2 * w)], row[tm_dim_of<NBIT>(2 * w + 1)]);
+    out[i] = *reinterpret_cast<uint32_t *>(&p);
+  }
+}
+
+// ---------------------------------------------------------------------
 // Centroid scoring on tensor cores.
 //
 // probe_tc_kernel: CTA = 128 query tokens (operand A, M = 128, BF16
@@ -740,6 +1114,10 @@ cudaError_t configure_tc_kernels() {
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(probe_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPtSmem);
   if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(rerank_tmem_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tm_smem_bytes(64));
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(rerank_tmem_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tm_smem_bytes(64));
+  if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(rerank_tc_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem_bytes(8, 64));
 }
 
@@ -758,6 +1136,63 @@ cudaError_t launch_rerank_tc(const DevIndex &ix, const void *cen_bf16, const voi
     case 2: rerank_tc_kernel<2><<<grid, kTcThreads, sm, st>>>(ix, c, l, q, q_off, short_id, n_short, probe_topk, semantics, n_max, approx, err); break;
     case 4: rerank_tc_kernel<4><<<grid, kTcThreads, sm, st>>>(ix, c, l, q, q_off, short_id, n_short, probe_topk, semantics, n_max, approx, err); break;
     case 8: rerank_tc_kernel<8><<<grid, kTcThreads, sm, st>>>(ix, c, l, q, q_off, short_id, n_short, probe_topk, semantics, n_max, approx, err); break;
+    default: return cudaErrorInvalidValue;
+  }
+  *n_launch += 1;
+  return cudaGetLastError();
+}
+
+bool tmem_rerank_supported(uint32_t n_bit) { return n_bit == 1 || n_bit == 2; }
+
+__global__ void centroid_norm_max_kernel(const float *__restrict__ cen, uint32_t n_cent,
+                                         unsigned *__restrict__ out) {
+  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < n_cent; c += gridDim.x * blockDim.x) {
+    const float4 *row = reinterpret_cast<const float4 *>(cen + (size_t)c * kDim);
+    float ss = 0.0f;
+    for (int i = 0; i < kDim / 4; i++) {
+      const float4 v = row[i];
+      ss = fmaf(v.x, v.x, fmaf(v.y, v.y, fmaf(v.z, v.z, fmaf(v.w, v.w, ss))));
+    }
+    atomicMax(out, __float_as_uint(sqrtf(ss)));
+  }
+}
+
+cudaError_t max_centroid_norm(const float *cen, uint32_t n_cent, unsigned *d_tmp, float *out,
+                              cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(d_tmp, 0, sizeof(unsigned), st);
+  if (e != cudaSuccess) return e;
+  centroid_norm_max_kernel<<<296, 256, 0, st>>>(cen, n_cent, d_tmp);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  unsigned bits = 0;
+  e = cudaMemcpyAsync(&bits, d_tmp, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+  if (e != cudaSuccess) return e;
+  e = cudaStreamSynchronize(st);
+  std::memcpy(out, &bits, 4);
+  return e;
+}
+
+cudaError_t make_centroid_perm(const float *cen, uint32_t n_cent, uint32_t n_bit, void *out,
+                               cudaStream_t st) {
+  uint32_t *o = reinterpret_cast<uint32_t *>(out);
+  if (n_bit == 2) perm_centroid_kernel<2><<<592, 256, 0, st>>>(cen, n_cent, o);
+  else if (n_bit == 1) perm_centroid_kernel<1><<<592, 256, 0, st>>>(cen, n_cent, o);
+  else return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rerank_tmem(const DevIndex &ix, const void *cen_perm, uint32_t wlo, uint32_t whi,
+                               const float *q, const uint64_t *q_off, uint32_t n_query,
+                               const uint32_t *short_id, const uint32_t *n_short,
+                               uint32_t probe_topk, int semantics, uint32_t nq_max, float x_bound,
+                               float *approx, unsigned *err, cudaStream_t st, int *n_launch) {
+  dim3 grid((probe_topk + kTmDocs - 1) / kTmDocs, n_query);
+  const uint32_t n_max = nq_max <= 32 ? 32u : 64u;
+  const size_t sm = tm_smem_bytes(n_max);
+  const uint32_t *c = reinterpret_cast<const uint32_t *>(cen_perm);
+  switch (ix.n_bit) {
+    case 1: rerank_tmem_kernel<1><<<grid, kTmThreads, sm, st>>>(ix, c, wlo, whi, q, q_off, short_id, n_short, probe_topk, semantics, n_max, x_bound, approx, err); break;
+    case 2: rerank_tmem_kernel<2><<<grid, kTmThreads, sm, st>>>(ix, c, wlo, whi, q, q_off, short_id, n_short, probe_topk, semantics, n_max, x_bound, approx, err); break;
     default: return cudaErrorInvalidValue;
   }
   *n_launch += 1;

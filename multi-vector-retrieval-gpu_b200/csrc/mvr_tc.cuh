@@ -13,6 +13,22 @@ cudaError_t launch_rerank_tc(const DevIndex &ix, const void *cen_bf16, const voi
                              uint32_t probe_topk, int semantics, uint32_t nq_max, float *approx,
                              unsigned *err, cudaStream_t st, int *n_launch);
 
+// BF16 MaxSim with the decoded doc tokens in tensor memory (1- and 2-bit
+// codes); cen_perm: [C][64] bf16x2 centroid rows in the kernel's K order
+// (make_centroid_perm); wlo / whi: low / high bytes of the BF16 bucket weights;
+// x_bound: upper bound on the norm of every decoded doc token
+bool tmem_rerank_supported(uint32_t n_bit);
+// largest L2 norm of the centroid rows (d_tmp: one device word of scratch)
+cudaError_t max_centroid_norm(const float *cen, uint32_t n_cent, unsigned *d_tmp, float *out,
+                              cudaStream_t st);
+cudaError_t make_centroid_perm(const float *cen, uint32_t n_cent, uint32_t n_bit, void *out,
+                               cudaStream_t st);
+cudaError_t launch_rerank_tmem(const DevIndex &ix, const void *cen_perm, uint32_t wlo, uint32_t whi,
+                               const float *q, const uint64_t *q_off, uint32_t n_query,
+                               const uint32_t *short_id, const uint32_t *n_short,
+                               uint32_t probe_topk, int semantics, uint32_t nq_max, float x_bound,
+                               float *approx, unsigned *err, cudaStream_t st, int *n_launch);
+
 // tensor-core centroid scoring: candidates per token = splits * 16; the
 // centroid tiles hold 64 centroids each (n_tiles = C_pad / 64)
 uint32_t probe_tc_cand_per_token(uint32_t n_tok, uint32_t n_cent, int n_sm, uint32_t *splits);

@@ -218,3 +218,28 @@ def test_config1_scale_gpu_built_index_bit_exact():
     g.close()
     del tok
     torch.cuda.empty_cache()
+
+
+def test_hash_filter_overflow_falls_back_bit_exact():
+    """The main filter keeps each query's candidates in per-CTA shared-memory
+    hash tables over 8 doc ranges (at most 7,168 candidates per range).  With
+    80,000 short docs and half the centroids probed, every range overflows and
+    the rank-table filter redoes the query; with one probe nothing overflows.
+    Both must match the oracle bit for bit, and queries of the two kinds mixed
+    in one batch must not disturb each other."""
+    lens = np.random.default_rng(11).integers(6, 12, 80_000)
+    ix = tiny_index(n_doc=80_000, n_centroid=32, n_bit=2, seed=12, lengths=lens, n_latent=64)
+    g, o = gpu_index(ix), oracle_of(ix)
+    q, off = make_queries(ix, 4, 32, seed=13)
+    for nprobe in (16, 1):
+        qi = q[off[0]:off[1]]
+        t = g.trace(qi, 10, nprobe, 1000)
+        compare_trace(t, o.search_one(qi, 10, nprobe, 1000))
+        if nprobe == 16:
+            assert len(t["cand_id"]) > 8 * 7168
+    # mixed batch: the same queries at nprobe 16 in one call
+    s, i = g.search(q, 10, 16, 1000, tok_off=off)
+    rs, ri = o.search(q, off, 10, 16, 1000)
+    np.testing.assert_array_equal(i, ri)
+    np.testing.assert_array_equal(s, rs)
+    g.close()
