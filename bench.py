@@ -40,11 +40,14 @@ CACHE_VERSION = "mvr-index-v1"
 
 WORKLOADS = {
     # 1M docs, 65,536 centroids, nbits 2, 10,000 queries
+    # probe_topk: the shortlist tuner's pick for recall@10 >= 0.99 against
+    # exhaustive MaxSim over the index's decoded vectors (300 tuning queries)
     "medium": dict(n_doc=1_000_000, n_centroid=65536, n_bit=2, n_query=10_000, n_tok=32,
-                   nprobe=8, topk=10, probe_topk=1000, kmeans_iter=4, seed=0, n_gt=100),
+                   nprobe=8, topk=10, probe_topk=1500, kmeans_iter=4, seed=0, n_gt=100,
+                   n_tune=300),
     # 10k docs, 8,192 centroids, nbits 2, 1,000 queries
     "small": dict(n_doc=10_000, n_centroid=8192, n_bit=2, n_query=1000, n_tok=32, nprobe=4,
-                  topk=10, probe_topk=200, kmeans_iter=8, seed=0, n_gt=200),
+                  topk=10, probe_topk=200, kmeans_iter=8, seed=0, n_gt=200, n_tune=300),
 }
 
 
@@ -158,7 +161,7 @@ def load_gpu_index(host, device_idx):
                              host["n_bit"], host["residual"], device=device_idx)
 
 
-def cpu_port_qps(host, q_np, off, w, n_threads, budget_s=15.0):
+def cpu_port_qps(host, q_np, off, w, n_threads, probe_topk, budget_s=15.0):
     """The oracle's CPU port of the path (test infrastructure) on a bounded
     query sample; returns (qps, sample size, seconds)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -168,12 +171,12 @@ def cpu_port_qps(host, q_np, off, w, n_threads, budget_s=15.0):
                         host["n_bit"])
     probe_n = min(len(off) - 1, max(2 * n_threads, 8))
     t = time.perf_counter()
-    o.search(q_np[: off[probe_n]], off[: probe_n + 1], w["topk"], w["nprobe"], w["probe_topk"],
+    o.search(q_np[: off[probe_n]], off[: probe_n + 1], w["topk"], w["nprobe"], probe_topk,
              n_threads=n_threads)
     per_q = (time.perf_counter() - t) / probe_n
     n = int(min(len(off) - 1, max(probe_n, budget_s / max(per_q, 1e-6))))
     t = time.perf_counter()
-    o.search(q_np[: off[n]], off[: n + 1], w["topk"], w["nprobe"], w["probe_topk"],
+    o.search(q_np[: off[n]], off[: n + 1], w["topk"], w["nprobe"], probe_topk,
              n_threads=n_threads)
     dt = time.perf_counter() - t
     return n / dt, n, dt, o
@@ -219,7 +222,7 @@ def run_reference(args, w):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": workload_config(w, "CPU port of the reference path (oracle)"),
+        "config": workload_config(w, "CPU port of the reference path (oracle)", w["probe_topk"]),
         "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": n_threads, "kind": "port",
                          "sample": f"{n} queries per step of the {w['n_query']}-query workload"},
         "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0,
@@ -228,14 +231,14 @@ def run_reference(args, w):
     print(json.dumps(line))
 
 
-def workload_config(w, path):
+def workload_config(w, path, probe_topk):
     return {"workload": (f"{path}: {w['n_doc']:,} synthetic docs (lognormal 70/35, clipped 8..180), "
                          f"{w['n_centroid']:,} centroids, nbits {w['n_bit']}, "
                          f"{w['n_query']:,} queries x {w['n_tok']} tok, nprobe {w['nprobe']}, "
-                         f"k {w['topk']}, probe_topk {w['probe_topk']}"),
+                         f"k {w['topk']}, probe_topk {probe_topk}"),
             "n_doc": w["n_doc"], "n_centroid": w["n_centroid"], "n_bit": w["n_bit"],
             "queries_per_step": w["n_query"], "query_tokens": w["n_tok"], "nprobe": w["nprobe"],
-            "topk": w["topk"], "probe_topk": w["probe_topk"], "kmeans_iter": w["kmeans_iter"],
+            "topk": w["topk"], "probe_topk": probe_topk, "kmeans_iter": w["kmeans_iter"],
             "l2": "flushed (256 MiB write) between timed steps"}
 
 
@@ -281,13 +284,17 @@ def main():
     ap.add_argument("--profile-case", action="store_true",
                     help="small profiling target instead of the bench: 200,000 docs, 16,384 "
                          "centroids, one mixed-precision and one plain search of 296 queries")
-    ap.add_argument("--recall-sweep", default="",
-                    help="extra nprobe:probe_topk settings whose recall@k is reported, "
-                         "e.g. 4:100,8:500")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="skip the shortlist tuner (it only reports unless --use-tuned)")
+    ap.add_argument("--use-tuned", action="store_true",
+                    help="time this run's tuned shortlist sizes instead of the workload's")
+    ap.add_argument("--target", type=float, default=0.99,
+                    help="recall@k target of the shortlist tuner (vs exhaustive MaxSim over "
+                         "the index's decoded vectors)")
     args = ap.parse_args()
     w = dict(WORKLOADS[args.workload])
     if args.probe_topk:
-        w["probe_topk"] = args.probe_topk
+        w["probe_topk"] = w["probe_topk_fast"] = args.probe_topk
     if args.impl == "reference":
         return run_reference(args, w)
     if args.profile_case:
@@ -295,7 +302,7 @@ def main():
 
     import torch
     import torch.distributed as dist
-    from mvr import PREC_BF16, exhaustive, formats, synth
+    from mvr import PREC_BF16, exhaustive, formats, synth, tune
     from mvr import dist as mdist
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -311,34 +318,63 @@ def main():
     g.set_rescore(args.rescore)
     q, off = synth.queries(spec, w["n_query"], w["n_tok"], dev, seed=100 + rank)
     n_query, T = w["n_query"], q.shape[0]
-    k, nprobe, ptk = w["topk"], w["nprobe"], w["probe_topk"]
+    k, nprobe = w["topk"], w["nprobe"]
     stream = torch.cuda.current_stream()
     out_s = torch.empty((n_query, k), dtype=torch.float32, device=dev)
     out_i = torch.empty((n_query, k), dtype=torch.int32, device=dev)
     FAST, PLAIN = PREC_BF16, 0
+    # shortlist sizes: the workload's fixed values (the tuner's picks for this
+    # corpus at the default target, so the reference arm times the same
+    # configuration); --use-tuned times this run's own picks instead
+    ptk = {FAST: w.get("probe_topk_fast", w["probe_topk"]), PLAIN: w["probe_topk"]}
 
     def step(flags):
-        return g.search_device(q.data_ptr(), None, n_query, w["n_tok"], k, nprobe, ptk,
+        return g.search_device(q.data_ptr(), None, n_query, w["n_tok"], k, nprobe, ptk[flags],
                                out_s.data_ptr(), out_i.data_ptr(), stream.cuda_stream,
                                semantics=flags)
 
-    # recall@k against exhaustive FP64 MaxSim over the raw tokens (rank 0)
-    recall, sweep = {}, {}
+    # ground truths (rank 0): exhaustive FP64 MaxSim over the raw tokens, and
+    # over the index's own decoded tokens (what candidate generation can
+    # reach); the shortlist sizes are tuned on a separate query sample against
+    # the latter, then recall is measured on the first n_gt workload queries
+    recall, tuning = {}, {}
     if rank == 0:
-        n_gt = w["n_gt"]
+        n_gt, n_tune = w["n_gt"], w["n_tune"]
         qg = q[: n_gt * w["n_tok"]]
-        gs, gi = exhaustive.exhaustive_topk(qg, off[: n_gt + 1], tok, spec.item_n_vec, k)
+        qt, offt = synth.queries(spec, n_tune, w["n_tok"], dev, seed=900)
+        _, gi_raw = exhaustive.exhaustive_topk(qg, off[: n_gt + 1], tok, spec.item_n_vec, k)
+        del tok
+        torch.cuda.empty_cache()
+        dec = exhaustive.decode_tokens(torch.from_numpy(host["centroid"]).to(dev),
+                                       torch.from_numpy(host["vq_code"].view(np.int32)).to(dev),
+                                       torch.from_numpy(host["residual"]).to(dev).view(-1, 128 * host["n_bit"] // 8),
+                                       torch.from_numpy(host["weight"]), host["n_bit"])
+        both = torch.cat([qg, qt])
+        both_off = np.concatenate([off[: n_gt + 1], off[n_gt] + offt[1:]]).astype(np.uint64)
+        _, gi_idx = exhaustive.exhaustive_topk(both, both_off, dec, spec.item_n_vec, k)
+        del dec
+        torch.cuda.empty_cache()
+        gi_eval, gi_tune = gi_idx[:n_gt], gi_idx[n_gt:]
+        qt_np = qt.cpu().numpy().reshape(n_tune, w["n_tok"], 128)
+        if not args.no_tune:
+            for name, fl in (("bf16", FAST), ("plain", PLAIN)):
+                t = tune.tune(g, qt_np, gi_tune, k, nprobe, args.target, fl)
+                tuning[name] = dict(probe_topk=t["probe_topk"], recall_tune=t["recall"],
+                                    reached=t["reached"], fixed=ptk[fl],
+                                    table=[(x["probe_topk"], round(x["recall"], 4),
+                                            round(x["ms"], 3)) for x in t["table"]])
+                if args.use_tuned:
+                    ptk[fl] = t["probe_topk"]
         for name, fl in (("bf16", FAST), ("plain", PLAIN)):
             step(fl)
             est = out_i[:n_gt].cpu().numpy().view(np.uint32)
-            recall[name] = float(formats.recall_at_k(gi, est, k).mean())
-        qg_np = qg.cpu().numpy()
-        for item in filter(None, args.recall_sweep.split(",")):
-            npb, ptk_s = (int(x) for x in item.split(":"))
-            _, si = g.search(qg_np.reshape(n_gt, w["n_tok"], 128), k, npb, ptk_s)
-            sweep[item] = float(formats.recall_at_k(gi, si, k).mean())
-        del tok
+            recall[name] = float(formats.recall_at_k(gi_eval, est, k).mean())
+            recall[name + "_raw"] = float(formats.recall_at_k(gi_raw, est, k).mean())
         torch.cuda.empty_cache()
+    if world > 1:  # every rank serves at rank 0's tuned shortlist sizes
+        pt = torch.tensor([ptk[FAST], ptk[PLAIN]], dtype=torch.int64, device=dev)
+        dist.broadcast(pt, 0)
+        ptk[FAST], ptk[PLAIN] = int(pt[0]), int(pt[1])
 
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
@@ -387,7 +423,7 @@ def main():
     for s in range(args.warmup + args.steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        st_e = g.search_host_ptr(hq.data_ptr(), None, n_query, w["n_tok"], k, nprobe, ptk,
+        st_e = g.search_host_ptr(hq.data_ptr(), None, n_query, w["n_tok"], k, nprobe, ptk[FAST],
                                  hs.data_ptr(), hi.data_ptr(), semantics=FAST, qtime=qtime)
         if s >= args.warmup:
             e2e_dt.append(time.perf_counter() - t0)
@@ -429,7 +465,7 @@ def main():
 
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
-        qps_cpu, n_s, dt_s, _ = cpu_port_qps(host, hq.numpy(), off, w, os.cpu_count())
+        qps_cpu, n_s, dt_s, _ = cpu_port_qps(host, hq.numpy(), off, w, os.cpu_count(), ptk[PLAIN])
         cpu = {"value": qps_cpu, "unit": "queries/s", "cores": os.cpu_count(), "kind": "port",
                "sample": f"first {n_s} of the {n_query} queries ({dt_s:.1f} s)"}
 
@@ -438,10 +474,15 @@ def main():
         "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": S,
         "warmup": args.warmup, "ms_per_step": fast["total_ms"] / S, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "bf16", "data": "synthetic",
-        "config": dict(workload_config(w, "BF16 tensor-core MaxSim + FP32 re-score"),
-                       **{"rescore": R, "recall@10": recall.get("bf16"),
-                          "recall@10_plain": recall.get("plain"), "recall_queries": w["n_gt"],
-                          "recall_sweep_plain": sweep, "plain_fp32_qps": plain["qps"],
+        "config": dict(workload_config(w, "BF16 tensor-core MaxSim + FP32 re-score", ptk[FAST]),
+                       **{"rescore": R, "probe_topk": ptk[FAST], "probe_topk_plain": ptk[PLAIN],
+                          "recall@10": recall.get("bf16"), "recall@10_plain": recall.get("plain"),
+                          "recall@10_vs_raw": recall.get("bf16_raw"),
+                          "recall@10_plain_vs_raw": recall.get("plain_raw"),
+                          "recall_ground_truth": "exhaustive FP64 MaxSim over the index's decoded "
+                          "vectors (recall@10); over the raw synthetic tokens (..._vs_raw)",
+                          "recall_queries": w["n_gt"], "tuning": tuning,
+                          "plain_fp32_qps": plain["qps"],
                           "speedup_vs_plain": value / plain["qps"],
                           "plain_stage_ms_per_step": [float(x / S) for x in plain["stage"]],
                           "p50_ms": p50, "p99_ms": p99, "latency": "per query = its batch's "

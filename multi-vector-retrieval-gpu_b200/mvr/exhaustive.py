@@ -42,3 +42,25 @@ def exhaustive_topk(q, tok_off, doc_tokens, item_n_vec, k, dtype=torch.float64,
     # (score desc, id asc): stable sort of ids by descending score
     order = torch.sort(scores, dim=1, descending=True, stable=True)
     return order.values[:, :k].cpu().numpy(), order.indices[:, :k].cpu().numpy()
+
+
+def decode_tokens(centroid, vq_code, residual, weight, n_bit, chunk=1 << 22):
+    """Every token of an index decoded the way the FP32 search path decodes
+    it: x = centroid[code] + weight[bucket] (one FP32 add per value), buckets
+    unpacked MSB-first, dim j = byte * (8 / n_bit) + i (RerankPP.hpp:100-111).
+    Inputs are torch tensors on the GPU (residual uint8 [n_vec, 128*n_bit/8]);
+    returns float32 [n_vec, 128] on the same device."""
+    dev = centroid.device
+    n = vq_code.shape[0]
+    vpb = 8 // n_bit
+    shifts = torch.tensor([8 - n_bit * (i + 1) for i in range(vpb)], device=dev,
+                          dtype=torch.int32)
+    w = weight.to(dev, torch.float32)
+    code = vq_code.to(torch.int64)
+    out = torch.empty((n, 128), dtype=torch.float32, device=dev)
+    for a in range(0, n, chunk):
+        b = min(n, a + chunk)
+        r = residual[a:b].to(torch.int32).unsqueeze(-1)            # [m, bytes, 1]
+        bucket = ((r >> shifts) & ((1 << n_bit) - 1)).reshape(b - a, 128)
+        out[a:b] = centroid[code[a:b]] + w[bucket.to(torch.int64)]
+    return out

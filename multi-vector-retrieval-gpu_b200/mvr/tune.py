@@ -1,0 +1,46 @@
+"""Shortlist-size autotuner.
+
+The search path's cost grows with the shortlist (probe_topk docs are
+decompressed and scored per query) and, on the mixed-precision path, with the
+FP32 re-score width R.  `tune` measures, on a sample of queries with a known
+ground truth, the recall@k and the device time of every candidate setting and
+returns the cheapest one whose recall reaches the target: the smallest
+shortlist (then the smallest re-score width), a deterministic choice since
+the work per query grows with both.  The ground truth is
+whatever the caller wants the search to reproduce: the exhaustive MaxSim over
+the index's own decoded vectors measures the loss of candidate generation
+alone (the quantity a shortlist size can change), the exhaustive MaxSim over
+raw embeddings adds the loss of the residual codes.
+"""
+import numpy as np
+
+from .formats import recall_at_k
+
+
+def tune(index, queries, gnd_ids, k, nprobe, target, semantics,
+         probe_topks=(100, 150, 200, 300, 400, 600, 800, 1000, 1500, 2000),
+         rescores=(0,), repeats=3):
+    """queries: float32 [n_query, n_tok, 128] (host); gnd_ids: [n_query, >= k].
+    Returns dict(probe_topk, rescore, recall, ms, table, reached) for the
+    smallest setting with mean recall@k >= target (the most accurate one if
+    none reaches it); `table` lists every setting measured."""
+    table = []
+    for ptk in probe_topks:
+        if ptk < k:
+            continue
+        for r in rescores:
+            if r and (r < k or r > ptk):
+                continue
+            index.set_rescore(r)
+            best_ms = None
+            for _ in range(repeats):
+                s, i, st = index.search(queries, k, nprobe, ptk, semantics=semantics,
+                                        with_stats=True)
+                best_ms = st["device_ms"] if best_ms is None else min(best_ms, st["device_ms"])
+            rec = float(recall_at_k(gnd_ids, i, k).mean())
+            table.append(dict(probe_topk=ptk, rescore=r, recall=rec, ms=best_ms))
+    index.set_rescore(0)
+    ok = [t for t in table if t["recall"] >= target]
+    pick = (min(ok, key=lambda t: (t["probe_topk"], t["rescore"])) if ok
+            else max(table, key=lambda t: (t["recall"], -t["probe_topk"])))
+    return dict(pick, table=table, reached=bool(ok))
