@@ -242,13 +242,13 @@ def workload_config(w, path, probe_topk):
             "l2": "flushed (256 MiB write) between timed steps"}
 
 
-def run_profile_case():
+def run_profile_case(fast_flag):
     """A case small enough for ncu (a few GB on the device, one batch per
     search, inputs larger than L2): the raw tokens are freed before searching,
     so only the compressed index (~0.5 GB) and the working set are resident.
     296 queries = 2 filter CTAs per SM."""
     import torch
-    from mvr import PREC_BF16, build, synth
+    from mvr import build, synth
     spec = synth.CorpusSpec(200_000, seed=0)
     tok = synth.tokens(spec, "cuda")
     ix = build.build_index(tok, spec.item_n_vec, 16384, 2, kmeans_iter=2)
@@ -261,7 +261,7 @@ def run_profile_case():
     q, _ = synth.queries(spec, n, 32, "cuda", seed=5)
     out_s = torch.empty((n, 10), dtype=torch.float32, device="cuda")
     out_i = torch.empty((n, 10), dtype=torch.int32, device="cuda")
-    for fl in (PREC_BF16, 0):
+    for fl in (fast_flag, 0):
         st = g.search_device(q.data_ptr(), None, n, 32, 10, 8, 1000, out_s.data_ptr(),
                              out_i.data_ptr(), 0, semantics=fl)
         print("flags", fl, "device_ms", round(st.device_ms, 4), "stages_ms",
@@ -280,6 +280,8 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="medium")
     ap.add_argument("--probe-topk", type=int, default=None)
     ap.add_argument("--rescore", type=int, default=0, help="FP32 re-score width (0: 4*k)")
+    ap.add_argument("--precision", choices=["bf16", "fp8"], default="bf16",
+                    help="tensor-core MaxSim precision of the headline path")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-case", action="store_true",
                     help="small profiling target instead of the bench: 200,000 docs, 16,384 "
@@ -298,11 +300,12 @@ def main():
     if args.impl == "reference":
         return run_reference(args, w)
     if args.profile_case:
-        return run_profile_case()
+        from mvr import PREC_BF16, PREC_FP8
+        return run_profile_case(PREC_FP8 if args.precision == "fp8" else PREC_BF16)
 
     import torch
     import torch.distributed as dist
-    from mvr import PREC_BF16, exhaustive, formats, synth, tune
+    from mvr import PREC_BF16, PREC_FP8, exhaustive, formats, synth, tune
     from mvr import dist as mdist
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -322,7 +325,7 @@ def main():
     stream = torch.cuda.current_stream()
     out_s = torch.empty((n_query, k), dtype=torch.float32, device=dev)
     out_i = torch.empty((n_query, k), dtype=torch.int32, device=dev)
-    FAST, PLAIN = PREC_BF16, 0
+    FAST, PLAIN = (PREC_FP8 if args.precision == "fp8" else PREC_BF16), 0
     # shortlist sizes: the workload's fixed values (the tuner's picks for this
     # corpus at the default target, so the reference arm times the same
     # configuration); --use-tuned times this run's own picks instead
@@ -473,8 +476,9 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": S,
         "warmup": args.warmup, "ms_per_step": fast["total_ms"] / S, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "bf16", "data": "synthetic",
-        "config": dict(workload_config(w, "BF16 tensor-core MaxSim + FP32 re-score", ptk[FAST]),
+        "scaling": "weak", "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
+        "config": dict(workload_config(w, f"{args.precision.upper()} tensor-core MaxSim + FP32 "
+                                          "re-score", ptk[FAST]),
                        **{"rescore": R, "probe_topk": ptk[FAST], "probe_topk_plain": ptk[PLAIN],
                           "recall@10": recall.get("bf16"), "recall@10_plain": recall.get("plain"),
                           "recall@10_vs_raw": recall.get("bf16_raw"),

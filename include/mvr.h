@@ -43,6 +43,13 @@ typedef enum {
                             accumulation, and its best R docs are re-scored by
                             the exact FP32 kernel (R: mvr_index_set_rescore).
                             Returned scores are always exact FP32 MaxSim. */
+#define MVR_PREC_FP8 4u  /* as MVR_PREC_BF16 with the shortlist scored in FP8
+                            (E4M3) on the tensor cores: query tokens with
+                            per-token power-of-two scales, centroid rows and
+                            bucket weights as E4M3, FP32 accumulation; the
+                            best R docs are re-scored exactly in FP32.
+                            2-bit indexes; other code widths run the BF16
+                            kernel.  May be combined with MVR_SEM_BASIC. */
 
 typedef struct mvr_index mvr_index;
 

@@ -3,6 +3,8 @@
 // pipeline and the index-build entry points.
 #include "mvr.h"
 
+#include <cuda_fp8.h>
+
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -156,6 +158,8 @@ struct mvr_index {
   void *cen_perm = nullptr;      // [C][64] bf16x2 centroid rows, TMEM-rerank K order (b <= 2)
   uint32_t wlo = 0, whi = 0;     // low / high bytes of the BF16 bucket weights (b <= 2)
   float x_bound = 0.f;           // bound on the norm of every decoded doc token
+  void *cen8 = nullptr;          // [C][128] E4M3 centroid rows, FP8-rerank K order (b = 2)
+  uint32_t wtab8 = 0;            // E4M3 bucket weights in bytes 0..3 (b = 2)
   unsigned *d_err = nullptr;     // device error flags of the tensor-core kernels
   Workspace ws;
 
@@ -370,10 +374,11 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
     return MVR_OK;
   }
   if (!query || !out_s || !out_id) return set_err(MVR_ERR_INVALID_ARG, "null query/result buffer");
-  if (flags & ~(MVR_SEM_BASIC | MVR_PREC_BF16))
+  if (flags & ~(MVR_SEM_BASIC | MVR_PREC_BF16 | MVR_PREC_FP8))
     return set_err(MVR_ERR_INVALID_ARG, "unknown flags %u", flags);
   const int sem = (flags & MVR_SEM_BASIC) ? 1 : 0;
-  const bool bf16 = (flags & MVR_PREC_BF16) != 0;
+  const bool fp8 = (flags & MVR_PREC_FP8) != 0 && h->cen8 != nullptr;
+  const bool bf16 = (flags & (MVR_PREC_BF16 | MVR_PREC_FP8)) != 0;  // mixed-precision path
   uint32_t R = h->rescore ? h->rescore : 4 * topk;
   R = std::min(std::max(R, topk), probe_topk);
   std::vector<uint64_t> off;
@@ -456,10 +461,14 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
     if (bf16) {
       // BF16 tensor-core MaxSim over the whole shortlist, then the exact FP32
       // kernel re-scores its best R docs
-      if (h->cen_perm)
+      if (fp8)
+        CUDA_TRY(launch_rerank_tmem(h->dix, h->cen8, h->wtab8, 0u, qp, qo, nb, w.short_id,
+                                    w.n_short, probe_topk, sem, nq_max, h->x_bound, w.exact,
+                                    h->d_err, st, &launches, true));
+      else if (h->cen_perm)
         CUDA_TRY(launch_rerank_tmem(h->dix, h->cen_perm, h->wlo, h->whi, qp, qo, nb, w.short_id,
                                     w.n_short, probe_topk, sem, nq_max, h->x_bound, w.exact,
-                                    h->d_err, st, &launches));
+                                    h->d_err, st, &launches, false));
       else
         CUDA_TRY(launch_rerank_tc(h->dix, h->cen_bf16, h->lut_bf16, qp, qo, nb, w.short_id,
                                   w.n_short, probe_topk, sem, nq_max, w.exact, h->d_err, st,
@@ -573,6 +582,15 @@ int finish_index(mvr_index *h, const uint32_t *item_n_vec_host, const uint32_t *
     CUDA_TRY(max_centroid_norm(d.centroid, d.n_centroid, h->d_err, &cmax, h->stream));
     CUDA_TRY(cudaMemsetAsync(h->d_err, 0, sizeof(unsigned), h->stream));  // was scratch
     h->x_bound = cmax + std::sqrt((float)kDim) * wmax;
+    if (fp8_rerank_supported(d.n_bit)) {
+      uint8_t *c8;
+      MVR_TRY(dalloc(&c8, (size_t)d.n_centroid * kDim, &h->bufs));
+      CUDA_TRY(make_centroid_fp8(d.centroid, d.n_centroid, c8, h->stream));
+      h->cen8 = c8;
+      h->wtab8 = 0;
+      for (uint32_t k = 0; k < 4; k++)
+        h->wtab8 |= (uint32_t)__nv_cvt_float_to_fp8(weight[k], __NV_SATFINITE, __NV_E4M3) << (8 * k);
+    }
     for (uint32_t k = 0; k < (1u << d.n_bit); k++) {
       const uint16_t wb = bf16_bits(weight[k]);
       h->wlo |= (uint32_t)(wb & 0xffu) << (8 * k);

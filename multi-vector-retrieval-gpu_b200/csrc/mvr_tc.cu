@@ -16,6 +16,7 @@
 #include "mvr_tc.cuh"
 
 #include <cuda_bf16.h>
+#include <cuda_fp8.h>
 
 #include <algorithm>
 #include <cstring>
@@ -500,20 +501,65 @@ __device__ __forceinline__ void tm_decode16(const uint32_t *res, const uint4 *ce
   }
 }
 
-template <int NBIT>
+// FP8 (e4m3) variant for 2-bit codes.  The 16 dims of one residual word
+// expand with one PRMT per 4 dims: y1 = w & 0x33333333 puts the codes of dims
+// 4i+3 and 4i+1 of byte i in nibbles 2i and 2i+1, y0 = (w >> 2) & 0x33333333
+// those of dims 4i+2 and 4i; each nibble, used as a PRMT selector on the four
+// FP8 bucket weights, yields the dim's weight.  K position 4p + e of the
+// word's block (output word p = PRMT of y1, y1 >> 16, y0, y0 >> 16) holds
+// dim kFp8Dim[4p + e].  The centroid part and the residual part are two A
+// operands in TMEM accumulated into the same D (c + W[b] is never formed), so
+// the centroid row goes from its loads to TMEM unchanged.  Query tokens are
+// quantized with per-token power-of-two scales (their largest entry maps into
+// [112, 224]), removed from the per-doc maxima at the end.
+__host__ __device__ constexpr uint32_t fp8_dim_of(uint32_t kappa) {
+  constexpr uint8_t kFp8Dim[16] = {3, 1, 7, 5, 11, 9, 15, 13, 2, 0, 6, 4, 10, 8, 14, 12};
+  return (kappa & ~15u) + kFp8Dim[kappa & 15u];
+}
+
+// kind::f8f6f4 instruction descriptor: E4M3 A/B, FP32 D, both K-major.
+__host__ __device__ constexpr uint32_t idesc_e4m3(int m, int n) {
+  return (1u << 4) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_e4m3_ta(uint32_t tmem_d, uint32_t tmem_a, uint64_t b,
+                                            uint32_t idesc) {
+  asm volatile("tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], [%1], %2, %3, 1;\n" ::"r"(tmem_d),
+               "r"(tmem_a), "l"(b), "r"(idesc)
+               : "memory");
+}
+
+// 16 A_r columns (4 FP8 weights each) of one 64-dim half row from its 4
+// residual words; wtab: the 4 FP8 bucket weights in bytes 0..3.
+__device__ __forceinline__ void fp8_decode16(const uint32_t *res, uint32_t wtab,
+                                             uint32_t (&out)[16]) {
+#pragma unroll
+  for (int wi = 0; wi < 4; wi++) {
+    const uint32_t y1 = res[wi] & 0x33333333u, y0 = (res[wi] >> 2) & 0x33333333u;
+    out[4 * wi + 0] = prmt(wtab, 0u, y1);
+    out[4 * wi + 1] = prmt(wtab, 0u, y1 >> 16);
+    out[4 * wi + 2] = prmt(wtab, 0u, y0);
+    out[4 * wi + 3] = prmt(wtab, 0u, y0 >> 16);
+  }
+}
+
+template <int NBIT, bool FP8>
 __global__ void __launch_bounds__(kTmThreads, 2)
 rerank_tmem_kernel(DevIndex ix, const uint32_t *__restrict__ cen_perm, uint32_t wlo, uint32_t whi,
                    const float *__restrict__ q, const uint64_t *__restrict__ q_off,
                    const uint32_t *__restrict__ short_id, const uint32_t *__restrict__ n_short,
                    uint32_t probe_topk, int semantics, uint32_t n_max, float x_bound,
                    float *__restrict__ approx, unsigned *__restrict__ err) {
+  static_assert(!FP8 || NBIT == 2, "the FP8 rerank decodes 2-bit codes");
   constexpr int VPB = 8 / NBIT;
   constexpr int HW = 64 / (4 * VPB);  // residual words of a 64-dim half row (4 or 2)
+  constexpr int CW = FP8 ? 16 : 32;   // centroid words (TMEM columns) of a half row
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  uint8_t *Bq = smem;                                      // [2 K-blocks][n_max rows][128 B]
+  uint8_t *Bq = smem;  // BF16: [2 K-blocks][n_max rows][128 B]; FP8: [n_max rows][128 B]
   __shared__ uint32_t best[kTmDocs * kMaxQueryTok];        // [doc][query token], bits of OFF + max
-  __shared__ uint32_t s_qss;                               // max squared query-token norm
+  __shared__ uint32_t s_qss;                               // max squared (scaled) token norm
+  __shared__ float s_qinv[kMaxQueryTok];                   // FP8: 1 / query-token scale
   __shared__ __align__(16) uint32_t stage[kTmThreads / 32][16];  // per-warp epilogue staging
   __shared__ uint64_t bar[2];
   __shared__ uint32_t tmem_base_s;
@@ -531,7 +577,7 @@ rerank_tmem_kernel(DevIndex ix, const uint32_t *__restrict__ cen_perm, uint32_t 
   const uint64_t tok0 = q_off[b];
   const uint32_t nq = (uint32_t)(q_off[b + 1] - tok0);
   const uint32_t N = nq <= 32 ? 32u : 64u;  // <= n_max (host sizes smem by the batch)
-  const uint32_t idesc = idesc_bf16(kTmTile, (int)N);
+  const uint32_t idesc = FP8 ? idesc_e4m3(kTmTile, (int)N) : idesc_bf16(kTmTile, (int)N);
   const uint32_t n_cols = tm_cols(n_max);
 
   if (warp == 0) {
@@ -554,6 +600,42 @@ rerank_tmem_kernel(DevIndex ix, const uint32_t *__restrict__ cen_perm, uint32_t 
   }
   for (int i = tid; i < kMaxQueryTok * kTmDocs; i += kTmThreads) best[i] = 0u;
   __syncthreads();  // s_qss
+  if constexpr (FP8) {
+    // query tokens -> B operand (E4M3, scaled per token, permuted K order,
+    // swizzled, rows >= nq zero); 8 lanes per row, 16 positions each
+    for (int i = tid; i < (int)N * 8; i += kTmThreads) {  // N * 8 is a multiple of 256
+      const int row = i >> 3, ch = i & 7;
+      float x[16];
+      float amax = 0.0f, ss = 0.0f;
+#pragma unroll
+      for (int u = 0; u < 16; u++) {
+        x[u] = (uint32_t)row < nq ? __ldg(q + (tok0 + row) * kDim + fp8_dim_of(16 * ch + u)) : 0.0f;
+        amax = fmaxf(amax, fabsf(x[u]));
+        ss = fmaf(x[u], x[u], ss);
+      }
+#pragma unroll
+      for (int o = 4; o > 0; o >>= 1) {
+        amax = fmaxf(amax, __shfl_xor_sync(kFull, amax, o));
+        ss += __shfl_xor_sync(kFull, ss, o);
+      }
+      // power-of-two scale: largest entry into [112, 224] (1 for an all-zero row)
+      const float sc = amax > 0.0f ? exp2f(floorf(log2f(224.0f / amax))) : 1.0f;
+      uint32_t v[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const __nv_fp8x2_storage_t lo = __nv_cvt_float2_to_fp8x2(
+            make_float2(x[4 * u] * sc, x[4 * u + 1] * sc), __NV_SATFINITE, __NV_E4M3);
+        const __nv_fp8x2_storage_t hi = __nv_cvt_float2_to_fp8x2(
+            make_float2(x[4 * u + 2] * sc, x[4 * u + 3] * sc), __NV_SATFINITE, __NV_E4M3);
+        v[u] = (uint32_t)lo | ((uint32_t)hi << 16);
+      }
+      *reinterpret_cast<uint4 *>(Bq + sw128_off(row, ch)) = make_uint4(v[0], v[1], v[2], v[3]);
+      if ((lane & 7) == 0) {
+        atomicMax(&s_qss, __float_as_uint(ss * sc * sc));
+        if (row < kMaxQueryTok) s_qinv[row] = 1.0f / sc;
+      }
+    }
+  } else
   // query tokens -> B operand (BF16, permuted K order, swizzled, rows >= nq
   // zero); the 16 lanes of a row also sum its squares (fixed shuffle order)
   for (int i = tid; i < (int)N * 16; i += kTmThreads) {  // N * 16 is a multiple of 256
@@ -589,8 +671,10 @@ rerank_tmem_kernel(DevIndex ix, const uint32_t *__restrict__ cen_perm, uint32_t 
   tc_fence_after();
   const uint32_t tmem = tmem_base_s;
   const uint32_t n_tok = d_pref[nd];
-  // OFF: smallest power of two >= 1 above max |q| * |x| (margin for BF16 rounding)
-  const float off = fmaxf(1.0f, exp2f(ceilf(log2f(sqrtf(__uint_as_float(s_qss)) * x_bound * 1.02f + 1e-30f))));
+  // OFF: smallest power of two >= 1 above max |q| * |x| (margin for BF16 /
+  // FP8 rounding; FP8: scaled query tokens)
+  const float off = fmaxf(1.0f, exp2f(ceilf(log2f(sqrtf(__uint_as_float(s_qss)) * x_bound *
+                                                  (FP8 ? 1.15f : 1.02f) + 1e-30f))));
   const uint32_t off_bits = __float_as_uint(off);
   const uint32_t n_tiles = (n_tok + kTmTile - 1) / kTmTile;
   const uint32_t b_base = smem_u32(Bq);
@@ -672,12 +756,12 @@ rerank_tmem_kernel(DevIndex ix, const uint32_t *__restrict__ cen_perm, uint32_t 
   }
   for (uint32_t tile = 0; tile < n_tiles; tile++) {
     const int st = tile & 1;
-    // centroid half row of this tile (permuted BF16, 8 x 16 B)
-    uint4 cen[8];
+    // centroid half row of this tile (permuted BF16: 8 x 16 B; FP8: 4 x 16 B)
+    uint4 cen[CW / 4];
     if (doc_c >= 0) {
-      const uint4 *cp = reinterpret_cast<const uint4 *>(cen_perm + (size_t)code_c * 64 + hf * 32);
+      const uint4 *cp = reinterpret_cast<const uint4 *>(cen_perm + (size_t)code_c * (2 * CW) + hf * CW);
 #pragma unroll
-      for (int u = 0; u < 8; u++) cen[u] = __ldg(cp + u);
+      for (int u = 0; u < CW / 4; u++) cen[u] = __ldg(cp + u);
     }
     // next tile's code and residual words
     int doc_n;
@@ -690,17 +774,38 @@ rerank_tmem_kernel(DevIndex ix, const uint32_t *__restrict__ cen_perm, uint32_t 
     }
     if (tile > 1) epilogue(tile - 2);  // its MMA completed during the previous iteration
     if (hf == 0) tok_doc[tile % 3][row] = doc_c;
-    const uint32_t acol = tmem + lane_off + 64u * st + 32u * hf;
-#pragma unroll
-    for (int part = 0; part < 2; part++) {
+    if constexpr (FP8) {
+      // A_c: columns 64 st + 16 hf (centroid, as loaded); A_r: + 32 (weights)
+      const uint32_t acol = tmem + lane_off + 64u * st + 16u * hf;
       uint32_t out[16];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        out[4 * u] = doc_c >= 0 ? cen[u].x : 0u;
+        out[4 * u + 1] = doc_c >= 0 ? cen[u].y : 0u;
+        out[4 * u + 2] = doc_c >= 0 ? cen[u].z : 0u;
+        out[4 * u + 3] = doc_c >= 0 ? cen[u].w : 0u;
+      }
+      tmem_st16(acol, out);
       if (doc_c >= 0) {
-        tm_decode16<NBIT>(res_c + part * (HW / 2), cen + part * 4, wlo, whi, out);
+        fp8_decode16(res_c, wlo, out);
       } else {
 #pragma unroll
         for (int u = 0; u < 16; u++) out[u] = 0u;
       }
-      tmem_st16(acol + 16u * part, out);
+      tmem_st16(acol + 32u, out);
+    } else {
+      const uint32_t acol = tmem + lane_off + 64u * st + 32u * hf;
+#pragma unroll
+      for (int part = 0; part < 2; part++) {
+        uint32_t out[16];
+        if (doc_c >= 0) {
+          tm_decode16<NBIT>(res_c + part * (HW / 2), cen + part * 4, wlo, whi, out);
+        } else {
+#pragma unroll
+          for (int u = 0; u < 16; u++) out[u] = 0u;
+        }
+        tmem_st16(acol + 16u * part, out);
+      }
     }
     asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory");
     tc_fence_before();
@@ -709,10 +814,19 @@ rerank_tmem_kernel(DevIndex ix, const uint32_t *__restrict__ cen_perm, uint32_t 
     if (tid == 0) {
       tc_fence_after();
       const uint32_t dcol = tmem + 128u + N * (tile % 3);
+      if constexpr (FP8) {
 #pragma unroll
-      for (int kk = 0; kk < 8; kk++) {
-        const uint64_t bd = sw128_desc(b_base + (kk >> 2) * (N * 128) + (kk & 3) * 32);
-        mma_bf16_ta(dcol, tmem + 64u * st + 8u * kk, bd, idesc, 1u);  // D starts at OFF
+        for (int kk = 0; kk < 4; kk++) {  // K = 32 per MMA; centroid part, then residual part
+          const uint64_t bd = sw128_desc(b_base + kk * 32);
+          mma_e4m3_ta(dcol, tmem + 64u * st + 8u * kk, bd, idesc);        // D starts at OFF
+          mma_e4m3_ta(dcol, tmem + 64u * st + 32u + 8u * kk, bd, idesc);
+        }
+      } else {
+#pragma unroll
+        for (int kk = 0; kk < 8; kk++) {
+          const uint64_t bd = sw128_desc(b_base + (kk >> 2) * (N * 128) + (kk & 3) * 32);
+          mma_bf16_ta(dcol, tmem + 64u * st + 8u * kk, bd, idesc, 1u);  // D starts at OFF
+        }
       }
       mma_commit(&bar[st]);
     }
@@ -731,6 +845,7 @@ rerank_tmem_kernel(DevIndex ix, const uint32_t *__restrict__ cen_perm, uint32_t 
     float s = 0.0f;
     for (uint32_t t = 0; t < nq; t++) {
       float m = __uint_as_float(best[tid * kMaxQueryTok + t]) - off;
+      if constexpr (FP8) m *= s_qinv[t];
       if (clamp) m = fmaxf(m, 0.0f);
       s += m;
     }
@@ -1114,9 +1229,11 @@ cudaError_t configure_tc_kernels() {
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(probe_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPtSmem);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(rerank_tmem_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tm_smem_bytes(64));
+  e = cudaFuncSetAttribute(rerank_tmem_kernel<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tm_smem_bytes(64));
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(rerank_tmem_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tm_smem_bytes(64));
+  e = cudaFuncSetAttribute(rerank_tmem_kernel<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tm_smem_bytes(64));
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(rerank_tmem_kernel<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tm_smem_bytes(64));
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(rerank_tc_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem_bytes(8, 64));
 }
@@ -1143,6 +1260,24 @@ cudaError_t launch_rerank_tc(const DevIndex &ix, const void *cen_bf16, const voi
 }
 
 bool tmem_rerank_supported(uint32_t n_bit) { return n_bit == 1 || n_bit == 2; }
+bool fp8_rerank_supported(uint32_t n_bit) { return n_bit == 2; }
+
+// cen8[c][k] = E4M3 of centroid c at K position k of the FP8 rerank order
+__global__ void perm_centroid_fp8_kernel(const float *__restrict__ cen, uint32_t n_cent,
+                                         uint8_t *__restrict__ out) {
+  const size_t n = (size_t)n_cent * kDim;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const size_t c = i / kDim;
+    out[i] = __nv_cvt_float_to_fp8(cen[c * kDim + fp8_dim_of((uint32_t)(i % kDim))], __NV_SATFINITE,
+                                   __NV_E4M3);
+  }
+}
+
+cudaError_t make_centroid_fp8(const float *cen, uint32_t n_cent, void *out, cudaStream_t st) {
+  perm_centroid_fp8_kernel<<<592, 256, 0, st>>>(cen, n_cent, reinterpret_cast<uint8_t *>(out));
+  return cudaGetLastError();
+}
 
 __global__ void centroid_norm_max_kernel(const float *__restrict__ cen, uint32_t n_cent,
                                          unsigned *__restrict__ out) {
@@ -1185,14 +1320,21 @@ cudaError_t launch_rerank_tmem(const DevIndex &ix, const void *cen_perm, uint32_
                                const float *q, const uint64_t *q_off, uint32_t n_query,
                                const uint32_t *short_id, const uint32_t *n_short,
                                uint32_t probe_topk, int semantics, uint32_t nq_max, float x_bound,
-                               float *approx, unsigned *err, cudaStream_t st, int *n_launch) {
+                               float *approx, unsigned *err, cudaStream_t st, int *n_launch,
+                               bool fp8) {
+  if (fp8 && ix.n_bit != 2) return cudaErrorInvalidValue;
   dim3 grid((probe_topk + kTmDocs - 1) / kTmDocs, n_query);
   const uint32_t n_max = nq_max <= 32 ? 32u : 64u;
   const size_t sm = tm_smem_bytes(n_max);
   const uint32_t *c = reinterpret_cast<const uint32_t *>(cen_perm);
   switch (ix.n_bit) {
-    case 1: rerank_tmem_kernel<1><<<grid, kTmThreads, sm, st>>>(ix, c, wlo, whi, q, q_off, short_id, n_short, probe_topk, semantics, n_max, x_bound, approx, err); break;
-    case 2: rerank_tmem_kernel<2><<<grid, kTmThreads, sm, st>>>(ix, c, wlo, whi, q, q_off, short_id, n_short, probe_topk, semantics, n_max, x_bound, approx, err); break;
+    case 1: rerank_tmem_kernel<1, false><<<grid, kTmThreads, sm, st>>>(ix, c, wlo, whi, q, q_off, short_id, n_short, probe_topk, semantics, n_max, x_bound, approx, err); break;
+    case 2:
+      if (fp8)
+        rerank_tmem_kernel<2, true><<<grid, kTmThreads, sm, st>>>(ix, c, wlo, whi, q, q_off, short_id, n_short, probe_topk, semantics, n_max, x_bound, approx, err);
+      else
+        rerank_tmem_kernel<2, false><<<grid, kTmThreads, sm, st>>>(ix, c, wlo, whi, q, q_off, short_id, n_short, probe_topk, semantics, n_max, x_bound, approx, err);
+      break;
     default: return cudaErrorInvalidValue;
   }
   *n_launch += 1;

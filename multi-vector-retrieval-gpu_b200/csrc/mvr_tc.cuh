@@ -27,7 +27,13 @@ cudaError_t launch_rerank_tmem(const DevIndex &ix, const void *cen_perm, uint32_
                                const float *q, const uint64_t *q_off, uint32_t n_query,
                                const uint32_t *short_id, const uint32_t *n_short,
                                uint32_t probe_topk, int semantics, uint32_t nq_max, float x_bound,
-                               float *approx, unsigned *err, cudaStream_t st, int *n_launch);
+                               float *approx, unsigned *err, cudaStream_t st, int *n_launch,
+                               bool fp8);
+// FP8 (E4M3) MaxSim for 2-bit codes: cen8 [C][128] E4M3 centroid rows in
+// the FP8 kernel's K order (make_centroid_fp8); pass it as cen_perm and the 4
+// E4M3 bucket weights in the bytes of wlo, with fp8 = true
+bool fp8_rerank_supported(uint32_t n_bit);
+cudaError_t make_centroid_fp8(const float *cen, uint32_t n_cent, void *out, cudaStream_t st);
 
 // tensor-core centroid scoring: candidates per token = splits * 16; the
 // centroid tiles hold 64 centroids each (n_tiles = C_pad / 64)

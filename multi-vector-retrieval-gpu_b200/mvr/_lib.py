@@ -19,6 +19,7 @@ MVR_ERR_UNSUPPORTED = 5
 MVR_SEM_PP = 0
 MVR_SEM_BASIC = 1
 MVR_PREC_BF16 = 2
+MVR_PREC_FP8 = 4
 
 # every symbol include/mvr.h declares
 EXPORTS = (

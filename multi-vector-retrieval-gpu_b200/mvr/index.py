@@ -15,6 +15,7 @@ from ._lib import check, lib
 SEM_PP = _lib.MVR_SEM_PP
 SEM_BASIC = _lib.MVR_SEM_BASIC
 PREC_BF16 = _lib.MVR_PREC_BF16
+PREC_FP8 = _lib.MVR_PREC_FP8
 
 
 def _ptr(a):

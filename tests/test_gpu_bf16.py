@@ -1,15 +1,16 @@
-"""Mixed-precision path (MVR_PREC_BF16): the BF16 tensor-core (tcgen05)
-MaxSim over the shortlist followed by the exact FP32 re-score of its best R
-docs.  Checked against the oracle: the BF16 scores lie within BF16 rounding
-of the exact FP32 MaxSim, every returned score is bit-identical to the
-oracle's FP32 MaxSim of that doc, and the top-k equals the plain path's
-wherever the plain path's exact ranking survives the BF16 pre-selection."""
+"""Mixed-precision paths (MVR_PREC_BF16, MVR_PREC_FP8): the BF16 or FP8
+(E4M3) tensor-core (tcgen05) MaxSim over the shortlist followed by the exact
+FP32 re-score of its best R docs.  Checked against the oracle: the
+approximate scores lie within BF16 (FP8) rounding of the exact FP32 MaxSim,
+every returned score is bit-identical to the oracle's FP32 MaxSim of that
+doc, and the top-k equals the plain path's wherever the plain path's exact
+ranking survives the approximate pre-selection."""
 import numpy as np
 import pytest
 
 import pyoracle
 from helpers import make_queries, oracle_of, tiny_index
-from mvr import PREC_BF16, SEM_BASIC, SEM_PP, Index
+from mvr import PREC_BF16, PREC_FP8, SEM_BASIC, SEM_PP, Index
 
 pytestmark = pytest.mark.gpu
 
@@ -115,3 +116,69 @@ def test_tensor_core_probe_matches_exact(n_centroid):
     s2, i2 = g.search(q, 10, 8, 100, tok_off=off)
     assert (i == i2).all(axis=1).sum() >= 5
     g.close()
+
+
+@pytest.fixture(scope="module")
+def pair2():
+    ix = tiny_index(n_doc=600, n_centroid=96, n_bit=2, seed=77)
+    g = gpu_index(ix)
+    yield ix, g, oracle_of(ix)
+    g.close()
+
+
+@pytest.mark.parametrize("sem", [SEM_PP, SEM_BASIC], ids=["pp", "basic"])
+def test_fp8_scores_close_to_exact(pair2, sem):
+    """E4M3 operands (3 mantissa bits) with FP32 accumulation: per-doc MaxSim
+    within 6e-2 relative of the exact FP32 value, 1.5e-2 on average."""
+    ix, g, o = pair2
+    q, off = make_queries(ix, 4, (8, 64), seed=51)
+    rel = []
+    for i in range(4):
+        qi = q[off[i]:off[i + 1]]
+        t = g.trace(qi, 10, 6, 200, sem | PREC_FP8)
+        r = o.search_one(qi, 10, 6, 200, sem)
+        np.testing.assert_array_equal(t["short_id"], np.sort(r["short_id"]))
+        exact = np.array([o.maxsim_item(qi, d, sem) for d in t["short_id"]])
+        err = np.abs(t["short_exact"] - exact) / np.maximum(np.abs(exact), 1e-3)
+        rel.append(err)
+        assert err.max() < 6e-2, err.max()
+    assert np.concatenate(rel).mean() < 1.5e-2
+
+
+@pytest.mark.parametrize("sem", [SEM_PP, SEM_BASIC], ids=["pp", "basic"])
+def test_fp8_topk_scores_are_exact_fp32(pair2, sem):
+    ix, g, o = pair2
+    q, off = make_queries(ix, 24, 32, seed=53)
+    s8, i8 = g.search(q.reshape(24, 32, 128), 10, 6, 200, semantics=sem | PREC_FP8)
+    s_pl, i_pl = g.search(q.reshape(24, 32, 128), 10, 6, 200, semantics=sem)
+    same = 0
+    for k in range(24):
+        qk = q[off[k]:off[k + 1]]
+        for d, s in zip(i8[k], s8[k]):
+            if d != 0xFFFFFFFF:
+                assert s == o.maxsim_item(qk, d, sem)  # bit-exact FP32 re-score
+        same += np.array_equal(i8[k], i_pl[k])
+    assert same >= 20, same
+
+
+def test_fp8_rescore_all_equals_plain_and_other_widths_run(pair2):
+    ix, g, o = pair2
+    q, off = make_queries(ix, 30, (1, 64), seed=55)
+    ref_s, ref_i = g.search(q, 10, 4, 150, tok_off=off)
+    g.set_rescore(150)
+    g.set_batch(7)
+    s, i = g.search(q, 10, 4, 150, tok_off=off, semantics=PREC_FP8)
+    g.set_rescore(0)
+    g.set_batch(0)
+    np.testing.assert_array_equal(i, ref_i)
+    np.testing.assert_array_equal(s, ref_s)
+    # a 4-bit index takes the BF16 kernel under MVR_PREC_FP8
+    ix4 = tiny_index(n_doc=200, n_centroid=40, n_bit=4, seed=78)
+    g4, o4 = gpu_index(ix4), oracle_of(ix4)
+    q4, off4 = make_queries(ix4, 3, 32, seed=56)
+    s4, i4 = g4.search(q4.reshape(3, 32, 128), 10, 4, 60, semantics=PREC_FP8)
+    for k in range(3):
+        for d, sc in zip(i4[k], s4[k]):
+            if d != 0xFFFFFFFF:
+                assert sc == o4.maxsim_item(q4[off4[k]:off4[k + 1]], d, SEM_PP)
+    g4.close()
