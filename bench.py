@@ -37,6 +37,7 @@ sys.path.insert(0, os.path.join(ROOT, "multi-vector-retrieval-gpu_b200"))
 METRIC = ("QPS & p99 ms at recall@10>=0.99 vs exact MaxSim: learned+BF16/FP8 vs plain, "
           "1 B200")
 CACHE_VERSION = "mvr-index-v1"
+RERANK_DRAM_BYTES_PER_TOKEN = 33.2  # ncu: dram__bytes_read+write of rerank_tmem_kernel (FP8) / token
 
 WORKLOADS = {
     # 1M docs, 65,536 centroids, nbits 2, 10,000 queries
@@ -280,7 +281,10 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="medium")
     ap.add_argument("--probe-topk", type=int, default=None)
     ap.add_argument("--rescore", type=int, default=0, help="FP32 re-score width (0: 4*k)")
-    ap.add_argument("--precision", choices=["bf16", "fp8"], default="bf16",
+    ap.add_argument("--impute", action="store_true",
+                    help="headline path: approximate scores impute unmatched query tokens "
+                         "(MVR_CAND_IMPUTE); the plain path keeps the reference's scores")
+    ap.add_argument("--precision", choices=["bf16", "fp8"], default="fp8",
                     help="tensor-core MaxSim precision of the headline path")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-case", action="store_true",
@@ -305,7 +309,7 @@ def main():
 
     import torch
     import torch.distributed as dist
-    from mvr import PREC_BF16, PREC_FP8, exhaustive, formats, synth, tune
+    from mvr import CAND_IMPUTE, PREC_BF16, PREC_FP8, exhaustive, formats, synth, tune
     from mvr import dist as mdist
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -326,6 +330,8 @@ def main():
     out_s = torch.empty((n_query, k), dtype=torch.float32, device=dev)
     out_i = torch.empty((n_query, k), dtype=torch.int32, device=dev)
     FAST, PLAIN = (PREC_FP8 if args.precision == "fp8" else PREC_BF16), 0
+    if args.impute:
+        FAST |= CAND_IMPUTE
     # shortlist sizes: the workload's fixed values (the tuner's picks for this
     # corpus at the default target, so the reference arm times the same
     # configuration); --use-tuned times this run's own picks instead
@@ -360,7 +366,7 @@ def main():
         gi_eval, gi_tune = gi_idx[:n_gt], gi_idx[n_gt:]
         qt_np = qt.cpu().numpy().reshape(n_tune, w["n_tok"], 128)
         if not args.no_tune:
-            for name, fl in (("bf16", FAST), ("plain", PLAIN)):
+            for name, fl in (("fast", FAST), ("plain", PLAIN)):
                 t = tune.tune(g, qt_np, gi_tune, k, nprobe, args.target, fl)
                 tuning[name] = dict(probe_topk=t["probe_topk"], recall_tune=t["recall"],
                                     reached=t["reached"], fixed=ptk[fl],
@@ -368,7 +374,7 @@ def main():
                                             round(x["ms"], 3)) for x in t["table"]])
                 if args.use_tuned:
                     ptk[fl] = t["probe_topk"]
-        for name, fl in (("bf16", FAST), ("plain", PLAIN)):
+        for name, fl in (("fast", FAST), ("plain", PLAIN)):
             step(fl)
             est = out_i[:n_gt].cpu().numpy().view(np.uint32)
             recall[name] = float(formats.recall_at_k(gi_eval, est, k).mean())
@@ -391,7 +397,7 @@ def main():
             torch.cuda.profiler.start()
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
               for _ in range(args.steps)]
-        acc = dict(stage=np.zeros(6), launches=0, n_cand=0, n_tok=0, n_ent=0)
+        acc = dict(stage=np.zeros(6), launches=0, n_cand=0, n_tok=0, n_ent=0, n_batch=0)
         for s in range(args.steps):
             flush.fill_(s & 0xFF)
             ev[s][0].record(stream)
@@ -402,6 +408,7 @@ def main():
             acc["n_cand"] += st.n_cand_total
             acc["n_tok"] += st.n_rerank_tok
             acc["n_ent"] += st.n_list_ent
+            acc["n_batch"] += st.n_batch
         torch.cuda.synchronize()
         if profile:
             torch.cuda.profiler.stop()
@@ -413,6 +420,10 @@ def main():
         return acc
 
     plain = measure(PLAIN)
+    other = (FAST ^ PREC_FP8 ^ PREC_BF16) if FAST & (PREC_FP8 | PREC_BF16) else PREC_BF16
+    # (the other tensor-core precision, same candidate scoring)
+    ptk[other] = ptk[FAST]
+    alt = measure(other)
     with ClockSampler(local) as clk:
         fast = measure(FAST, profile=True)
     value = fast["qps"]
@@ -445,25 +456,35 @@ def main():
     C, D = w["n_centroid"], 128
     bpv = D * w["n_bit"] // 8
     stage = fast["stage"]
+    n_launch = max(1, fast["n_batch"])  # batches = launches of each stage's kernel, all steps
+    tok_launch = fast["n_tok"] / n_launch
     probe_flop = 2.0 * T * C * D * S
-    rerank_flop = 2.0 * w["n_tok"] * D * fast["n_tok"]
-    rerank_bytes = (4.0 + bpv) * fast["n_tok"]
-    filter_bytes = 4.0 * fast["n_ent"] + (4 + 32 + 8) * fast["n_cand"]
-    kern = {1: ("probe_topk_kernel", "tensor", probe_flop / 1e12, pk["tc_sus"], "TFLOP/s"),
-            2: ("filter_kernel", "hbm", filter_bytes / 1e9, pk["hbm"], "GB/s"),
-            3: ("rerank_tc_kernel", "tensor", rerank_flop / 1e12, pk["tc_sus"], "TFLOP/s")}
+    rerank_bytes = (4.0 + bpv) * fast["n_tok"]           # vq code + residual bytes per token
+    filter_bytes = 4.0 * fast["n_ent"] + 16.0 * fast["n_cand"]  # list entries; keys out + in
+    rk = "rerank_tmem_kernel (FP8)" if FAST & PREC_FP8 else "rerank_tmem_kernel (BF16)"
+    kern = {1: ("probe_tc_kernel + probe_rescore_kernel", "tensor", probe_flop / 1e12,
+                pk["tc_sus"], "TFLOP/s"),
+            2: ("filter_hash_kernel + filter_select_kernel", "hbm", filter_bytes / 1e9, pk["hbm"],
+                "GB/s"),
+            3: (rk, "hbm", rerank_bytes / 1e9, pk["hbm"], "GB/s")}
     dom = max((1, 2, 3), key=lambda i: stage[i])
     name, bound, work, peak, unit = kern[dom]
     achieved = work / (stage[dom] / 1e3)
     names = ("query_copy", "probe", "filter", "rerank", "rescore_topk", "result_copy")
+    # DRAM bytes per reranked token of the FP8 rerank kernel, measured by ncu
+    # on the 200,000-doc profiling case (profiles/ncu_profile_case_fp8.md),
+    # scaled to a launch of this workload by its reranked tokens
+    traffic = RERANK_DRAM_BYTES_PER_TOKEN * tok_launch if (dom == 3 and FAST & PREC_FP8) else None
     roof = {"kernel": name, "bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
-            "frac": achieved / peak, "traffic": None,
+            "frac": achieved / peak, "traffic": traffic,
+            "algorithmic_bytes_per_launch": rerank_bytes / n_launch if dom == 3 else None,
             "peak_source": f"{pk['src']} ({'bf16 sustained' if bound == 'tensor' else 'HBM copy'})",
             "stage_share": {n: float(stage[i] / stage.sum()) for i, n in enumerate(names)},
-            "per_stage": {kern[i][0]: {"ms_per_step": float(stage[i] / S),
+            "per_stage": {kern[i][0]: {"ms_per_step": float(stage[i] / S), "bound": kern[i][1],
                                        "achieved": kern[i][2] / (stage[i] / 1e3),
+                                       "frac": kern[i][2] / (stage[i] / 1e3) / kern[i][3],
                                        "unit": kern[i][4]} for i in (1, 2, 3)},
-            "rerank_tc_hbm_gbs": rerank_bytes / 1e9 / (stage[3] / 1e3),
+            "rerank_tflops": 2.0 * w["n_tok"] * D * fast["n_tok"] / 1e12 / (stage[3] / 1e3),
             "rescore_topk_ms_per_step": float(stage[4] / S)}
 
     cpu = None
@@ -480,13 +501,16 @@ def main():
         "config": dict(workload_config(w, f"{args.precision.upper()} tensor-core MaxSim + FP32 "
                                           "re-score", ptk[FAST]),
                        **{"rescore": R, "probe_topk": ptk[FAST], "probe_topk_plain": ptk[PLAIN],
-                          "recall@10": recall.get("bf16"), "recall@10_plain": recall.get("plain"),
-                          "recall@10_vs_raw": recall.get("bf16_raw"),
+                          "recall@10": recall.get("fast"), "recall@10_plain": recall.get("plain"),
+                          "recall@10_vs_raw": recall.get("fast_raw"),
                           "recall@10_plain_vs_raw": recall.get("plain_raw"),
                           "recall_ground_truth": "exhaustive FP64 MaxSim over the index's decoded "
                           "vectors (recall@10); over the raw synthetic tokens (..._vs_raw)",
                           "recall_queries": w["n_gt"], "tuning": tuning,
                           "plain_fp32_qps": plain["qps"],
+                          ("bf16_qps" if other & PREC_BF16 else "fp8_qps"): alt["qps"],
+                          "candidate_scores": "imputed (MVR_CAND_IMPUTE)" if args.impute
+                          else "reference (0 for unmatched tokens)",
                           "speedup_vs_plain": value / plain["qps"],
                           "plain_stage_ms_per_step": [float(x / S) for x in plain["stage"]],
                           "p50_ms": p50, "p99_ms": p99, "latency": "per query = its batch's "

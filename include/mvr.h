@@ -51,6 +51,14 @@ typedef enum {
                             2-bit indexes; other code widths run the BF16
                             kernel.  May be combined with MVR_SEM_BASIC. */
 
+#define MVR_CAND_IMPUTE 8u /* candidate filter: a query token that visits no
+                            probed list holding the doc adds its lowest probed
+                            centroid score to the doc's approximate score
+                            (the reference adds 0).  Ranks the shortlist
+                            closer to the exact MaxSim; not a reference
+                            option, so candidate scores then differ from the
+                            reference's. */
+
 typedef struct mvr_index mvr_index;
 
 typedef struct {

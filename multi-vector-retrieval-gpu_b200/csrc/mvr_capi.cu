@@ -374,7 +374,7 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
     return MVR_OK;
   }
   if (!query || !out_s || !out_id) return set_err(MVR_ERR_INVALID_ARG, "null query/result buffer");
-  if (flags & ~(MVR_SEM_BASIC | MVR_PREC_BF16 | MVR_PREC_FP8))
+  if (flags & ~(MVR_SEM_BASIC | MVR_PREC_BF16 | MVR_PREC_FP8 | MVR_CAND_IMPUTE))
     return set_err(MVR_ERR_INVALID_ARG, "unknown flags %u", flags);
   const int sem = (flags & MVR_SEM_BASIC) ? 1 : 0;
   const bool fp8 = (flags & MVR_PREC_FP8) != 0 && h->cen8 != nullptr;
@@ -454,7 +454,8 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
     }
     CUDA_TRY(launch_filter_hash(h->dix, w.probe_id, w.probe_s, nprobe, qo, nb, probe_topk, scr,
                                 h->epoch, w.short_id, w.short_approx, w.n_short,
-                                w.qstat + (size_t)s * 3, st, &launches));
+                                w.qstat + (size_t)s * 3, st, &launches,
+                                (flags & MVR_CAND_IMPUTE) ? 1 : 0));
     CUDA_TRY(cudaEventRecord(ev(bt, 3), st));
     float *os = host_io ? w.out_s : out_s + (size_t)s * topk;
     uint32_t *oi = host_io ? w.out_id : out_id + (size_t)s * topk;

@@ -394,8 +394,9 @@ filter_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
               FilterScratch scr, uint32_t epoch,
               uint32_t *__restrict__ short_id, float *__restrict__ short_approx,
               uint32_t *__restrict__ n_short_out, uint32_t *__restrict__ qstat,
-              uint32_t *__restrict__ only_if) {
+              uint32_t *__restrict__ only_if, int impute) {
   __shared__ long long pfix[kMaxQueryTok * kMaxProbe];
+  __shared__ long long impf[kMaxQueryTok];  // imputed score of an unmatched token (0: off)
   __shared__ uint32_t pref[kMaxQueryTok + 1];
   __shared__ uint32_t lsz[kMaxQueryTok * kMaxProbe];
   __shared__ uint64_t lof[kMaxQueryTok * kMaxProbe];
@@ -428,6 +429,8 @@ filter_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
     lsz[i] = c < ix.n_centroid ? ix.ivf_size[c] : 0u;
     lof[i] = c < ix.n_centroid ? ix.ivf_off[c] : 0ull;
   }
+  for (uint32_t t = tid; t < nq; t += blockDim.x)
+    impf[t] = impute ? to_fixed(probe_s[(tok0 + t) * nprobe + nprobe - 1]) : 0ll;
   if (tid == 0) { s_ncand = 0; s_sel = 0; s_stok = 0; s_entries = 0; }
   filter_sync<CL>();  // counters of CTA 0 initialised before any remote update
 
@@ -517,7 +520,7 @@ filter_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
 #pragma unroll
         for (int v = 0; v < 16; v++) {
           const uint32_t t = t0 + v;
-          if (t < nq && bytes[v] != 0xff) s += pfix[t * nprobe + bytes[v]];
+          if (t < nq) s += bytes[v] != 0xff ? pfix[t * nprobe + bytes[v]] : impf[t];
         }
         ps_acc[u] = s;
         *reinterpret_cast<uint4 *>(row[u] + t0) = make_uint4(~0u, ~0u, ~0u, ~0u);
@@ -574,7 +577,7 @@ __global__ void __launch_bounds__(kFilterThreads, 1)
 filter_hash_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
                    const float *__restrict__ probe_s, uint32_t nprobe,
                    const uint64_t *__restrict__ q_off, FilterScratch scr,
-                   uint32_t *__restrict__ qstat) {
+                   uint32_t *__restrict__ qstat, int impute) {
   extern __shared__ __align__(16) uint8_t hsm[];
   uint32_t *tkey = reinterpret_cast<uint32_t *>(hsm);                      // [cap]
   uint32_t *tmask = tkey + kHashCap;                                       // [cap][MW]
@@ -582,6 +585,8 @@ filter_hash_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
   __shared__ long long pfix[kMaxQueryTok * kMaxProbe];
   __shared__ uint32_t lsz[kMaxQueryTok * kMaxProbe];   // this CTA's sub-list sizes
   __shared__ uint64_t lof[kMaxQueryTok * kMaxProbe];   // and offsets in ivf_ids
+  __shared__ long long impf[kMaxQueryTok];  // imputed score of an unmatched token (0: off)
+  __shared__ long long s_imp;               // sum of impf over the query's tokens
   __shared__ uint32_t s_fill, s_ovf, s_entries;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -598,7 +603,14 @@ filter_hash_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
     for (int w = 0; w < MW; w++) tmask[i * MW + w] = 0u;
   }
   if (tid == 0) { s_fill = 0; s_ovf = 0; s_entries = 0; }
+  for (uint32_t t = tid; t < nq; t += blockDim.x)
+    impf[t] = impute ? to_fixed(probe_s[(tok0 + t) * nprobe + nprobe - 1]) : 0ll;
   __syncthreads();
+  if (tid == 0) {  // fixed order: the same integer in every CTA
+    long long a = 0;
+    for (uint32_t t = 0; t < nq; t++) a += impf[t];
+    s_imp = a;
+  }
   uint32_t ent = 0;
   for (uint32_t i = tid; i < nq * nprobe; i += blockDim.x) {
     const uint32_t c = probe_id[tok0 * nprobe + i];
@@ -626,7 +638,8 @@ filter_hash_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
     for (uint32_t j = 0; j < nprobe; j++) {
       const uint32_t sz = lsz[t * nprobe + j];
       const uint32_t *ids = ix.ivf_ids + lof[t * nprobe + j];
-      const unsigned long long add = (unsigned long long)pfix[t * nprobe + j];
+      // first visit: the probe score replaces the token's imputed score
+      const unsigned long long add = (unsigned long long)(pfix[t * nprobe + j] - impf[t]);
       for (uint32_t p = lane; p < sz; p += 32) {
         const uint32_t it = __ldg(ids + p);
         // find or insert `it` (linear probing; the fill limit keeps >= 1024
@@ -665,7 +678,8 @@ filter_hash_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
       uint32_t base = 0;
       if (lane == __ffs(m) - 1) base = atomicAdd(scr.qcnt + b, (uint32_t)__popc(m));
       base = __shfl_sync(kFull, base, __ffs(m) - 1);
-      if (has) key[base + __popc(m & lt_mask)] = make_key(from_fixed((long long)tacc[sl]), k);
+      if (has)
+        key[base + __popc(m & lt_mask)] = make_key(from_fixed((long long)tacc[sl] + s_imp), k);
     }
   }
   if (tid == 0) {
@@ -981,7 +995,7 @@ cudaError_t launch_filter(const DevIndex &ix, const uint32_t *probe_id,
                           uint32_t *qstat, cudaStream_t st, int *n_launch) {
   filter_kernel<1><<<n_query, kFilterThreads, 0, st>>>(ix, probe_id, probe_s, nprobe, q_off,
                                                        probe_topk, scr, epoch, short_id,
-                                                       short_approx, n_short, qstat, nullptr);
+                                                       short_approx, n_short, qstat, nullptr, 0);
   *n_launch += 1;
   return cudaGetLastError();
 }
@@ -993,7 +1007,7 @@ cudaError_t launch_filter_cluster(const DevIndex &ix, const uint32_t *probe_id,
                                   uint32_t epoch, uint32_t *short_id,
                                   float *short_approx, uint32_t *n_short,
                                   uint32_t *qstat, cudaStream_t st, int *n_launch,
-                                  uint32_t *only_if) {
+                                  uint32_t *only_if, int impute) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(n_query * kFilterCluster, 1, 1);
   cfg.blockDim = dim3(kFilterThreads, 1, 1);
@@ -1008,7 +1022,7 @@ cudaError_t launch_filter_cluster(const DevIndex &ix, const uint32_t *probe_id,
   cfg.numAttrs = 1;
   cudaError_t e = cudaLaunchKernelEx(&cfg, filter_kernel<kFilterCluster>, ix, probe_id, probe_s,
                                      nprobe, q_off, probe_topk, scr, epoch, short_id,
-                                     short_approx, n_short, qstat, only_if);
+                                     short_approx, n_short, qstat, only_if, impute);
   *n_launch += 1;
   return e != cudaSuccess ? e : cudaGetLastError();
 }
@@ -1019,13 +1033,13 @@ cudaError_t launch_filter_hash(const DevIndex &ix, const uint32_t *probe_id,
                                uint32_t probe_topk, const FilterScratch &scr,
                                uint32_t epoch, uint32_t *short_id,
                                float *short_approx, uint32_t *n_short,
-                               uint32_t *qstat, cudaStream_t st, int *n_launch) {
+                               uint32_t *qstat, cudaStream_t st, int *n_launch, int impute) {
   if (scr.rank_stride <= 32)
     filter_hash_kernel<1><<<n_query * kHashParts, kFilterThreads, hash_smem_bytes(1), st>>>(
-        ix, probe_id, probe_s, nprobe, q_off, scr, qstat);
+        ix, probe_id, probe_s, nprobe, q_off, scr, qstat, impute);
   else
     filter_hash_kernel<2><<<n_query * kHashParts, kFilterThreads, hash_smem_bytes(2), st>>>(
-        ix, probe_id, probe_s, nprobe, q_off, scr, qstat);
+        ix, probe_id, probe_s, nprobe, q_off, scr, qstat, impute);
   filter_select_kernel<<<n_query, kFilterThreads, 0, st>>>(ix, probe_topk, scr, short_id,
                                                           short_approx, n_short, qstat);
   *n_launch += 2;
@@ -1034,7 +1048,7 @@ cudaError_t launch_filter_hash(const DevIndex &ix, const uint32_t *probe_id,
   // queries whose candidates overflowed a hash table: rank-table filter
   return launch_filter_cluster(ix, probe_id, probe_s, nprobe, q_off, n_query, probe_topk, scr,
                                epoch, short_id, short_approx, n_short, qstat, st, n_launch,
-                               scr.ovf);
+                               scr.ovf, impute);
 }
 
 cudaError_t launch_rerank(const DevIndex &ix, const float *q, const uint64_t *q_off,

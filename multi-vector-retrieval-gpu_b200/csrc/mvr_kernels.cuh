@@ -43,16 +43,18 @@ cudaError_t launch_filter_cluster(const DevIndex &ix, const uint32_t *probe_id,
                                   uint32_t epoch, uint32_t *short_id,
                                   float *short_approx, uint32_t *n_short,
                                   uint32_t *qstat, cudaStream_t st, int *n_launch,
-                                  uint32_t *only_if);
+                                  uint32_t *only_if, int impute);
 // Main-path filter: shared-memory hash tables over doc ranges (8 CTAs per
 // query), a select kernel, and the rank-table filter for overflowed queries.
+// impute: an unmatched query token adds its lowest probed score to a
+// candidate's approximate score (MVR_CAND_IMPUTE) instead of 0.
 cudaError_t launch_filter_hash(const DevIndex &ix, const uint32_t *probe_id,
                                const float *probe_s, uint32_t nprobe,
                                const uint64_t *q_off, uint32_t n_query,
                                uint32_t probe_topk, const FilterScratch &scr,
                                uint32_t epoch, uint32_t *short_id,
                                float *short_approx, uint32_t *n_short,
-                               uint32_t *qstat, cudaStream_t st, int *n_launch);
+                               uint32_t *qstat, cudaStream_t st, int *n_launch, int impute);
 cudaError_t launch_rerank(const DevIndex &ix, const float *q, const uint64_t *q_off,
                           uint32_t n_query, const uint32_t *short_id,
                           const uint32_t *n_short, uint32_t probe_topk,

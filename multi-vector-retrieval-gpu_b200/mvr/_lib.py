@@ -20,6 +20,7 @@ MVR_SEM_PP = 0
 MVR_SEM_BASIC = 1
 MVR_PREC_BF16 = 2
 MVR_PREC_FP8 = 4
+MVR_CAND_IMPUTE = 8
 
 # every symbol include/mvr.h declares
 EXPORTS = (

@@ -16,6 +16,7 @@ SEM_PP = _lib.MVR_SEM_PP
 SEM_BASIC = _lib.MVR_SEM_BASIC
 PREC_BF16 = _lib.MVR_PREC_BF16
 PREC_FP8 = _lib.MVR_PREC_FP8
+CAND_IMPUTE = _lib.MVR_CAND_IMPUTE
 
 
 def _ptr(a):

@@ -395,6 +395,8 @@ static int search_one_ws(const orc_index *ix, orc_ws *w, const float *q,
                          float *out_score, uint32_t *out_id) {
   uint32_t pid[64 * 64];
   float ps[64 * 64];
+  const int impute = (semantics & ORC_CAND_IMPUTE) != 0;
+  semantics &= ~ORC_CAND_IMPUTE;
   /* 1. centroid scores + probe */
   orc_centroid_scores(q, nq, ix->centroid, ix->n_centroid, ix->dim, w->S);
   orc_probe(w->S, nq, ix->n_centroid, nprobe, pid, ps);
@@ -421,13 +423,17 @@ static int search_one_ws(const orc_index *ix, orc_ws *w, const float *q,
   qsort(w->cand, n_cand, sizeof(uint32_t), cmp_u32);
   /* 3. approximate score = sum over q of the per-token maxima (RAFT reduce,
    * FilterPP.hpp:366-379), summed exactly: each term as a 2^-32 fixed-point
-   * integer, the integer sum rounded once to FP32 (order-independent). */
+   * integer, the integer sum rounded once to FP32 (order-independent).
+   * With ORC_CAND_IMPUTE (not a reference option) a token that visits no
+   * list holding the doc contributes its lowest probed centroid score
+   * instead of 0. */
   for (uint32_t i = 0; i < n_cand; i++) {
     const uint32_t it = w->cand[i];
     uint8_t *r = w->rank + (size_t)it * nq;
     int64_t acc = 0;
     for (uint32_t t = 0; t < nq; t++) {
       if (r[t] != 0xff) acc += orc_fixed(ps[t * nprobe + r[t]]);
+      else if (impute) acc += orc_fixed(ps[t * nprobe + nprobe - 1]);
       r[t] = 0xff;
     }
     w->seen[it] = 0;

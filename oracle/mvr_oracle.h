@@ -41,6 +41,9 @@ extern "C" {
  * BASIC pads every doc to max_item_n_vec with zero rows (Rerank.hpp:166-179,
  * 293-306), i.e. max(0, .) for docs shorter than the longest doc. */
 enum { ORC_SEM_PP = 0, ORC_SEM_BASIC = 1 };
+/* search flag (OR-ed into semantics; not a reference option): approximate
+ * scores impute an unmatched query token with its lowest probed score */
+enum { ORC_CAND_IMPUTE = 8 };
 
 typedef struct {
   uint32_t n_item, n_centroid, dim, n_bit;

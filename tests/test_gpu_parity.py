@@ -242,4 +242,25 @@ def test_hash_filter_overflow_falls_back_bit_exact():
     rs, ri = o.search(q, off, 10, 16, 1000)
     np.testing.assert_array_equal(i, ri)
     np.testing.assert_array_equal(s, rs)
+    # imputed candidate scores through the fallback
+    from mvr import CAND_IMPUTE
+    qi = q[off[1]:off[2]]
+    compare_trace(g.trace(qi, 10, 16, 1000, CAND_IMPUTE),
+                  o.search_one(qi, 10, 16, 1000, CAND_IMPUTE))
     g.close()
+
+
+@pytest.mark.parametrize("sem", [SEM_PP, SEM_BASIC], ids=["pp", "basic"])
+def test_imputed_candidate_scores_bit_exact(pair, sem):
+    """MVR_CAND_IMPUTE: an unmatched query token contributes its lowest probed
+    score to the approximate score; candidates, scores, shortlist and top-k
+    match the oracle's (the same option) bit for bit, through the hash filter
+    and through the rank-table fallback (80,000-doc case below)."""
+    from mvr import CAND_IMPUTE
+    ix, g, o = pair
+    q, off = make_queries(ix, 3, 32, seed=23)
+    for i in range(3):
+        qi = q[off[i]:off[i + 1]]
+        for nprobe, ptk, k in ((4, 100, 10), (8, 300, 100)):
+            compare_trace(g.trace(qi, k, nprobe, ptk, sem | CAND_IMPUTE),
+                          o.search_one(qi, k, nprobe, ptk, sem | CAND_IMPUTE))
