@@ -281,6 +281,8 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="medium")
     ap.add_argument("--probe-topk", type=int, default=None)
     ap.add_argument("--rescore", type=int, default=0, help="FP32 re-score width (0: 4*k)")
+    ap.add_argument("--batch", type=int, default=0,
+                    help="queries per device batch (0: the library's default)")
     ap.add_argument("--impute", action="store_true",
                     help="headline path: approximate scores impute unmatched query tokens "
                          "(MVR_CAND_IMPUTE); the plain path keeps the reference's scores")
@@ -323,6 +325,8 @@ def main():
     spec, host, tok, built_s = get_index(w, dev, rank, want_tokens=(rank == 0))
     g = load_gpu_index(host, local)
     g.set_rescore(args.rescore)
+    if args.batch:
+        g.set_batch(args.batch)
     q, off = synth.queries(spec, w["n_query"], w["n_tok"], dev, seed=100 + rank)
     n_query, T = w["n_query"], q.shape[0]
     k, nprobe = w["topk"], w["nprobe"]

@@ -112,10 +112,11 @@ __global__ void validate_kernel(const uint32_t *code, uint64_t n_vec, uint32_t n
 // handle
 // ----------------------------------------------------------------------
 struct Workspace {
-  uint32_t slots = 0, rank_stride = 0;
-  uint32_t *stamp = nullptr;
-  uint8_t *rank = nullptr;
-  uint64_t *key = nullptr;
+  uint32_t slots = 0, fb_slots = 0, rank_stride = 0;
+  uint32_t *stamp = nullptr;    // rank-table fallback: [fb_slots][n_item]
+  uint8_t *rank = nullptr;      //   [fb_slots][n_item][rank_stride]
+  uint64_t *key = nullptr;      //   [fb_slots][n_item]
+  uint64_t *hkey = nullptr;     // hash filter: [slots][kHashKeys] candidate keys
   uint32_t *qcnt = nullptr, *ovf = nullptr;  // [slots] hash-filter counters / overflow flags
   // per batch
   uint32_t batch_slots = 0, tok_cap = 0, np_cap = 0, short_cap = 0, topk_cap = 0;
@@ -178,8 +179,9 @@ struct mvr_index {
     if (stream) cudaStreamDestroy(stream);
   }
   void free_scratch() {
-    dfree(ws.stamp); dfree(ws.rank); dfree(ws.key); dfree(ws.qcnt); dfree(ws.ovf);
-    ws.stamp = nullptr; ws.rank = nullptr; ws.key = nullptr; ws.qcnt = nullptr; ws.ovf = nullptr;
+    dfree(ws.stamp); dfree(ws.rank); dfree(ws.key); dfree(ws.hkey); dfree(ws.qcnt); dfree(ws.ovf);
+    ws.stamp = nullptr; ws.rank = nullptr; ws.key = nullptr; ws.hkey = nullptr;
+    ws.qcnt = nullptr; ws.ovf = nullptr;
     ws.slots = 0;
   }
   void free_batch() {
@@ -204,14 +206,19 @@ struct mvr_index {
 
 namespace {
 
-uint32_t default_batch(const mvr_index *h) {
-  // Per-slot filter scratch is n_item * (4 + 32 + 8) bytes; keep all slots
-  // within ~16 GB and aim for two waves of 1024-thread filter CTAs.
-  const double per_slot = (double)h->dix.n_item * 44.0;
-  uint32_t b = 2u * (uint32_t)h->n_sm;
-  const double budget = 16.0 * (1ull << 30);
-  while (b > 1 && per_slot * b > budget) b--;
-  return std::max(1u, b);
+// Queries per device batch: 8 per SM (1,184 on B200) -- large batches fill
+// the tensor-core probe's token tiles and the re-score's CTAs; the hash
+// filter's key space is kHashKeys * 8 B = 459 KB per query.
+uint32_t default_batch(const mvr_index *h) { return 8u * (uint32_t)h->n_sm; }
+
+// Slots of the rank-table fallback (n_item * (4 + 32|64 + 8) bytes each,
+// kept within ~8 GB and at most half the batch, so a batch always takes at
+// least two chunks); it runs the batch's overflowed queries chunk by chunk.
+uint32_t fallback_slots(const mvr_index *h, uint32_t slots, uint32_t rank_stride) {
+  const double per_slot = (double)h->dix.n_item * (12.0 + rank_stride);
+  uint32_t f = std::min((slots + 1) / 2, 2u * (uint32_t)h->n_sm);
+  while (f > 1 && per_slot * f > 8.0 * (1ull << 30)) f--;
+  return std::max(1u, f);
 }
 
 int ensure_scratch(mvr_index *h, uint32_t slots, uint32_t rank_stride) {
@@ -219,17 +226,20 @@ int ensure_scratch(mvr_index *h, uint32_t slots, uint32_t rank_stride) {
   if (w.slots >= slots && w.rank_stride >= rank_stride) return MVR_OK;
   h->free_scratch();
   const size_t n = (size_t)h->dix.n_item;
-  MVR_TRY(dalloc(&w.stamp, slots * n));
-  MVR_TRY(dalloc(&w.rank, slots * n * rank_stride));
-  MVR_TRY(dalloc(&w.key, slots * n));
+  const uint32_t fb = fallback_slots(h, slots, rank_stride);
+  MVR_TRY(dalloc(&w.stamp, fb * n));
+  MVR_TRY(dalloc(&w.rank, fb * n * rank_stride));
+  MVR_TRY(dalloc(&w.key, fb * n));
+  MVR_TRY(dalloc(&w.hkey, (size_t)slots * kHashKeys));
   MVR_TRY(dalloc(&w.qcnt, slots));
   MVR_TRY(dalloc(&w.ovf, slots));
   CUDA_TRY(cudaMemsetAsync(w.qcnt, 0, slots * sizeof(uint32_t), h->stream));
   CUDA_TRY(cudaMemsetAsync(w.ovf, 0, slots * sizeof(uint32_t), h->stream));
-  CUDA_TRY(cudaMemsetAsync(w.stamp, 0, slots * n * sizeof(uint32_t), h->stream));
-  CUDA_TRY(cudaMemsetAsync(w.rank, 0xff, slots * n * rank_stride, h->stream));
+  CUDA_TRY(cudaMemsetAsync(w.stamp, 0, fb * n * sizeof(uint32_t), h->stream));
+  CUDA_TRY(cudaMemsetAsync(w.rank, 0xff, fb * n * rank_stride, h->stream));
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   w.slots = slots;
+  w.fb_slots = fb;
   w.rank_stride = rank_stride;
   h->epoch = 0;
   return MVR_OK;
@@ -417,7 +427,7 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
   CUDA_TRY(cudaMemcpyAsync(w.q_off, w.h_off, ((size_t)n_query + n_batch) * sizeof(uint64_t),
                            cudaMemcpyHostToDevice, st));
 
-  FilterScratch scr{w.stamp, w.rank, w.key, h->dix.n_item, w.rank_stride, w.qcnt, w.ovf};
+  FilterScratch scr{w.stamp, w.rank, w.key, h->dix.n_item, w.rank_stride, w.qcnt, w.ovf, w.hkey};
   int launches = 0;
   uint64_t h2d = ((size_t)n_query + n_batch) * sizeof(uint64_t), d2h = 0;
   auto ev = [&](uint32_t bt, int k) { return h->events[(size_t)bt * kStages + k]; };
@@ -448,12 +458,16 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
                             w.probe_s, st, &launches));
     }
     CUDA_TRY(cudaEventRecord(ev(bt, 2), st));
-    if (++h->epoch == 0) {  // stamps wrapped: clear them
-      CUDA_TRY(cudaMemsetAsync(w.stamp, 0, (size_t)w.slots * h->dix.n_item * sizeof(uint32_t), st));
-      h->epoch = 1;
+    // stamp epochs of the fallback's chunks: epoch .. epoch + n_chunks - 1
+    const uint32_t n_chunks = (nb + w.fb_slots - 1) / w.fb_slots;
+    if (h->epoch > 0xffffffffu - n_chunks - 1) {  // stamps would wrap: clear them
+      CUDA_TRY(cudaMemsetAsync(w.stamp, 0, (size_t)w.fb_slots * h->dix.n_item * sizeof(uint32_t), st));
+      h->epoch = 0;
     }
-    CUDA_TRY(launch_filter_hash(h->dix, w.probe_id, w.probe_s, nprobe, qo, nb, probe_topk, scr,
-                                h->epoch, w.short_id, w.short_approx, w.n_short,
+    const uint32_t epoch = h->epoch + 1;
+    h->epoch += n_chunks;
+    CUDA_TRY(launch_filter_hash(h->dix, w.probe_id, w.probe_s, nprobe, qo, nb, w.fb_slots, probe_topk, scr,
+                                epoch, w.short_id, w.short_approx, w.n_short,
                                 w.qstat + (size_t)s * 3, st, &launches,
                                 (flags & MVR_CAND_IMPUTE) ? 1 : 0));
     CUDA_TRY(cudaEventRecord(ev(bt, 3), st));
@@ -935,8 +949,14 @@ int mvr_search_trace(mvr_index *h, const float *query, uint32_t nq, uint32_t top
   tr->n_cand = n_cand;
   tr->n_short = n_short;
   if (tr->cand_id || tr->cand_score) {
+    // the query's keys: the hash filter's, or the rank-table fallback's when
+    // the query overflowed the hash tables
+    uint32_t ovf = 0;
+    CUDA_TRY(cudaMemcpy(&ovf, w.ovf, sizeof(uint32_t), cudaMemcpyDeviceToHost));
     std::vector<uint64_t> keys(n_cand);
-    if (n_cand) CUDA_TRY(cudaMemcpy(keys.data(), w.key, (size_t)n_cand * 8, cudaMemcpyDeviceToHost));
+    if (n_cand)
+      CUDA_TRY(cudaMemcpy(keys.data(), ovf ? w.key : w.hkey, (size_t)n_cand * 8,
+                          cudaMemcpyDeviceToHost));
     std::sort(keys.begin(), keys.end(),
               [](uint64_t a, uint64_t b) { return key_id(a) < key_id(b); });
     for (uint32_t i = 0; i < n_cand && i < tr->cand_cap; i++) {

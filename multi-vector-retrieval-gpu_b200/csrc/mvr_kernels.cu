@@ -410,7 +410,8 @@ filter_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
   if constexpr (CL > 1) asm volatile("mov.u32 %0, %%cluster_ctarank;\n" : "=r"(cr));
   const uint32_t b = blockIdx.x / CL;
   // fallback use: only the queries whose hash-table filter overflowed (the
-  // flag is the same for every CTA of the cluster, read before any barrier)
+  // flag is the same for every CTA of the cluster, read before any barrier;
+  // it stays set until the next batch's hash filter clears it)
   if (only_if && only_if[b] == 0) return;
   const uint64_t tok0 = q_off[b];
   const uint32_t nq = (uint32_t)(q_off[b + 1] - tok0);
@@ -543,7 +544,6 @@ filter_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
     qstat[b * 3 + 0] = n_cand;
     qstat[b * 3 + 1] = s_entries;
     qstat[b * 3 + 2] = s_stok;
-    if (only_if) only_if[b] = 0;
   }
 }
 
@@ -565,7 +565,8 @@ filter_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
 // scr.ovf and the rank-table filter redoes that query.
 // ---------------------------------------------------------------------
 constexpr uint32_t kHashLog = 13, kHashCap = 1u << kHashLog;  // slots per CTA
-constexpr uint32_t kHashFill = 7168;                          // inserts allowed per CTA
+constexpr uint32_t kHashFill = kHashKeys / kHashParts;         // inserts allowed per CTA
+static_assert(kHashFill + 1024 <= kHashCap, "the fill limit must keep >= 1024 slots empty");
 constexpr uint32_t kEmpty = 0xffffffffu;
 
 __host__ __device__ constexpr size_t hash_smem_bytes(int mw) {
@@ -667,8 +668,8 @@ filter_hash_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
   }
   __syncthreads();
 
-  // emit this CTA's candidates as (score, id) keys
-  uint64_t *key = scr.key + (size_t)b * scr.n_item;
+  // emit this CTA's candidates as (score, id) keys (at most kHashFill per CTA)
+  uint64_t *key = scr.hkey + (size_t)b * kHashKeys;
   for (uint32_t s0 = 0; s0 < kHashCap; s0 += blockDim.x) {
     const uint32_t sl = s0 + tid;
     const uint32_t k = sl < kHashCap ? tkey[sl] : kEmpty;
@@ -728,7 +729,7 @@ filter_select_kernel(DevIndex ix, uint32_t probe_topk, FilterScratch scr,
   if (threadIdx.x == 0) { s_sel = 0; s_stok = 0; }
   __syncthreads();
   SelectSmem sm{hist, &s_digit, &s_need, &s_done};
-  select_emit<1>(ix, scr.key + (size_t)b * scr.n_item, n_cand, probe_topk, b, 0, sm, &s_sel,
+  select_emit<1>(ix, scr.hkey + (size_t)b * kHashKeys, n_cand, probe_topk, b, 0, sm, &s_sel,
                  &s_stok, short_id, short_approx);
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -1029,11 +1030,13 @@ cudaError_t launch_filter_cluster(const DevIndex &ix, const uint32_t *probe_id,
 
 cudaError_t launch_filter_hash(const DevIndex &ix, const uint32_t *probe_id,
                                const float *probe_s, uint32_t nprobe,
-                               const uint64_t *q_off, uint32_t n_query,
+                               const uint64_t *q_off, uint32_t n_query, uint32_t fb_slots,
                                uint32_t probe_topk, const FilterScratch &scr,
                                uint32_t epoch, uint32_t *short_id,
                                float *short_approx, uint32_t *n_short,
                                uint32_t *qstat, cudaStream_t st, int *n_launch, int impute) {
+  cudaError_t e = cudaMemsetAsync(scr.ovf, 0, (size_t)n_query * sizeof(uint32_t), st);
+  if (e != cudaSuccess) return e;
   if (scr.rank_stride <= 32)
     filter_hash_kernel<1><<<n_query * kHashParts, kFilterThreads, hash_smem_bytes(1), st>>>(
         ix, probe_id, probe_s, nprobe, q_off, scr, qstat, impute);
@@ -1043,12 +1046,20 @@ cudaError_t launch_filter_hash(const DevIndex &ix, const uint32_t *probe_id,
   filter_select_kernel<<<n_query, kFilterThreads, 0, st>>>(ix, probe_topk, scr, short_id,
                                                           short_approx, n_short, qstat);
   *n_launch += 2;
-  cudaError_t e = cudaGetLastError();
+  e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  // queries whose candidates overflowed a hash table: rank-table filter
-  return launch_filter_cluster(ix, probe_id, probe_s, nprobe, q_off, n_query, probe_topk, scr,
-                               epoch, short_id, short_approx, n_short, qstat, st, n_launch,
-                               scr.ovf, impute);
+  // queries whose candidates overflowed a hash table: rank-table filter, in
+  // chunks of fb_slots queries over its fb_slots scratch slots; chunk c uses
+  // stamp epoch `epoch + c` (the caller reserves ceil(n_query / fb_slots))
+  for (uint32_t q0 = 0, c = 0; q0 < n_query; q0 += fb_slots, c++) {
+    const uint32_t cnt = n_query - q0 < fb_slots ? n_query - q0 : fb_slots;
+    e = launch_filter_cluster(ix, probe_id, probe_s, nprobe, q_off + q0, cnt, probe_topk, scr,
+                              epoch + c, short_id + (size_t)q0 * probe_topk,
+                              short_approx + (size_t)q0 * probe_topk, n_short + q0,
+                              qstat + (size_t)q0 * 3, st, n_launch, scr.ovf + q0, impute);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 cudaError_t launch_rerank(const DevIndex &ix, const float *q, const uint64_t *q_off,

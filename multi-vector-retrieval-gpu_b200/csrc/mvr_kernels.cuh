@@ -14,8 +14,13 @@ struct FilterScratch {
   uint32_t n_item;
   uint32_t rank_stride;  // 32 or 64 (>= query tokens, multiple of 16)
   uint32_t *qcnt;        // [slots] candidate keys emitted by the hash filter (0 between batches)
-  uint32_t *ovf;         // [slots] 1: the hash filter overflowed (0 between batches)
+  uint32_t *ovf;         // [slots] 1: the hash filter overflowed
+  uint64_t *hkey;        // [slots][kHashKeys] hash-filter candidate keys
 };
+
+// Candidate keys one query can hold in the hash filter: every doc range
+// stops inserting at kHashFill candidates, beyond which the query overflows.
+constexpr uint32_t kHashKeys = 8u * 7168u;
 
 cudaError_t configure_kernels();
 // ivf_part table of an index ([C][kHashParts + 1] u32)
@@ -48,9 +53,11 @@ cudaError_t launch_filter_cluster(const DevIndex &ix, const uint32_t *probe_id,
 // query), a select kernel, and the rank-table filter for overflowed queries.
 // impute: an unmatched query token adds its lowest probed score to a
 // candidate's approximate score (MVR_CAND_IMPUTE) instead of 0.
+// scr: stamp / rank / key hold fb_slots slots of the rank-table fallback,
+// which runs in chunks of fb_slots queries; hkey / qcnt / ovf hold n_query.
 cudaError_t launch_filter_hash(const DevIndex &ix, const uint32_t *probe_id,
                                const float *probe_s, uint32_t nprobe,
-                               const uint64_t *q_off, uint32_t n_query,
+                               const uint64_t *q_off, uint32_t n_query, uint32_t fb_slots,
                                uint32_t probe_topk, const FilterScratch &scr,
                                uint32_t epoch, uint32_t *short_id,
                                float *short_approx, uint32_t *n_short,
