@@ -166,6 +166,17 @@ int mvr_index_set_batch(mvr_index *h, uint32_t max_batch_queries);
  * (0 = default 4 * topk; clamped to [topk, probe_topk]). */
 int mvr_index_set_rescore(mvr_index *h, uint32_t n_rescore);
 
+/* CUDA graphs for repeated device-buffer searches (no counterpart in the
+ * reference, whose search loop launches every stage from the host per
+ * query; enable = 0 by default).  With graphs on, mvr_search_device records
+ * the whole call -- every batch's probe, filter, rerank, re-score and top-k
+ * kernels, on the handle's own stream, ordered after the caller's stream --
+ * as one CUDA graph the first time, and replays it while the call repeats
+ * (same query / result pointers, query count and token offsets, topk,
+ * nprobe, probe_topk, flags, re-score width and batch size); any change
+ * records a new graph.  The host buffers of mvr_search are not captured. */
+int mvr_index_set_graphs(mvr_index *h, int enable);
+
 /* Batched search with HOST buffers (queries in, results out; copies inside).
  * query_l: float32 tokens, query i = rows [tok_off[i], tok_off[i+1]) of a
  * [*, dim] matrix; tok_off == NULL means every query has query_n_vec tokens

@@ -152,7 +152,6 @@ struct mvr_index {
   std::vector<cudaEvent_t> events;
   uint32_t batch_cap = 0;
   uint32_t rescore = 0;          // FP32 re-score count of the BF16 path (0: 4 * topk)
-  uint32_t epoch = 0;
   void *cen_bf16 = nullptr;      // [C][128] BF16 centroid rows
   void *lut_bf16 = nullptr;      // [256][8/b] BF16 decode table
   void *cen_sw = nullptr;        // [C_pad/128][32 KB] swizzled BF16 centroid tiles
@@ -162,13 +161,39 @@ struct mvr_index {
   void *cen8 = nullptr;          // [C][128] E4M3 centroid rows, FP8-rerank K order (b = 2)
   uint32_t wtab8 = 0;            // E4M3 bucket weights in bytes 0..3 (b = 2)
   unsigned *d_err = nullptr;     // device error flags of the tensor-core kernels
+  uint32_t *d_epoch = nullptr;   // stamp-epoch counter of the rank-table fallback (device)
+  uint64_t epoch_used = 0;       // epochs consumed since the stamps were last cleared
+  uint64_t ws_gen = 0;           // bumped whenever a workspace buffer is reallocated
+  // CUDA-graph replay of repeated device-buffer searches (mvr_index_set_graphs)
+  bool graphs = false;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;  // stream handoff (no timing)
+  cudaEvent_t ev_g0 = nullptr, ev_g1 = nullptr;   // device time of a graph launch
+  struct {
+    cudaGraphExec_t exec = nullptr;
+    const float *query = nullptr;
+    float *out_s = nullptr;
+    uint32_t *out_id = nullptr;
+    uint32_t n_query = 0, topk = 0, nprobe = 0, probe_topk = 0, flags = 0, R = 0, B = 0;
+    uint64_t gen = 0;
+    std::vector<uint64_t> off;
+    int launches = 0;
+  } graph;
   Workspace ws;
+
+  void drop_graph() {
+    if (graph.exec) cudaGraphExecDestroy(graph.exec);
+    graph.exec = nullptr;
+  }
 
   ~mvr_index() {
     DeviceGuard g(device);
     if (stream) cudaStreamSynchronize(stream);
     for (void *p : bufs) dfree(p);
     dfree(d_err);
+    dfree(d_epoch);
+    drop_graph();
+    for (cudaEvent_t e : {ev_in, ev_out, ev_g0, ev_g1})
+      if (e) cudaEventDestroy(e);
     free_scratch();
     free_batch();
     dfree(ws.q_off);
@@ -237,11 +262,13 @@ int ensure_scratch(mvr_index *h, uint32_t slots, uint32_t rank_stride) {
   CUDA_TRY(cudaMemsetAsync(w.ovf, 0, slots * sizeof(uint32_t), h->stream));
   CUDA_TRY(cudaMemsetAsync(w.stamp, 0, fb * n * sizeof(uint32_t), h->stream));
   CUDA_TRY(cudaMemsetAsync(w.rank, 0xff, fb * n * rank_stride, h->stream));
+  CUDA_TRY(cudaMemsetAsync(h->d_epoch, 0, sizeof(uint32_t), h->stream));
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   w.slots = slots;
   w.fb_slots = fb;
   w.rank_stride = rank_stride;
-  h->epoch = 0;
+  h->epoch_used = 0;
+  h->ws_gen++;
   return MVR_OK;
 }
 
@@ -262,6 +289,7 @@ int ensure_batch(mvr_index *h, uint32_t slots, uint32_t tok_cap, uint32_t nprobe
   topk = std::max(topk, w.topk_cap);
   part_need = std::max(part_need, w.part_cap);
   h->free_batch();
+  h->ws_gen++;
   MVR_TRY(dalloc(&w.q, (size_t)tok_cap * kDim));
   MVR_TRY(dalloc(&w.probe_id, (size_t)tok_cap * nprobe));
   MVR_TRY(dalloc(&w.probe_s, (size_t)tok_cap * nprobe));
@@ -291,6 +319,7 @@ int ensure_batch(mvr_index *h, uint32_t slots, uint32_t tok_cap, uint32_t nprobe
 
 int ensure_call(mvr_index *h, size_t n_off, size_t n_stat, size_t n_events) {
   Workspace &w = h->ws;
+  if (w.off_cap < n_off || w.stat_cap < n_stat || h->events.size() < n_events) h->ws_gen++;
   if (w.off_cap < n_off) {
     dfree(w.q_off);
     w.q_off = nullptr;
@@ -419,97 +448,161 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
                       (size_t)kStages * n_batch + 1));
   Workspace &w = h->ws;
 
-  // relative token offsets of every batch, uploaded once
+  // stamp epochs this call takes (one per fallback chunk of every batch);
+  // clear the stamps before the device counter could wrap
+  uint64_t call_epochs = 0;
+  for (uint32_t bt = 0; bt < n_batch; bt++) {
+    const uint32_t nb = std::min(n_query, (bt + 1) * B) - bt * B;
+    call_epochs += (nb + w.fb_slots - 1) / w.fb_slots;
+  }
+  if (h->epoch_used + call_epochs >= (1ull << 31)) {
+    CUDA_TRY(cudaStreamSynchronize(st));
+    CUDA_TRY(cudaMemsetAsync(w.stamp, 0, (size_t)w.fb_slots * h->dix.n_item * sizeof(uint32_t),
+                             h->stream));
+    CUDA_TRY(cudaMemsetAsync(h->d_epoch, 0, sizeof(uint32_t), h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    h->epoch_used = 0;
+  }
+  h->epoch_used += call_epochs;
+
+  // relative token offsets of every batch
   for (uint32_t bt = 0, pos = 0; bt < n_batch; bt++) {
     const uint32_t s = bt * B, e = std::min(n_query, s + B);
     for (uint32_t i = s; i <= e; i++) w.h_off[pos++] = off[i] - off[s];
   }
-  CUDA_TRY(cudaMemcpyAsync(w.q_off, w.h_off, ((size_t)n_query + n_batch) * sizeof(uint64_t),
-                           cudaMemcpyHostToDevice, st));
 
   FilterScratch scr{w.stamp, w.rank, w.key, h->dix.n_item, w.rank_stride, w.qcnt, w.ovf, w.hkey};
   int launches = 0;
   uint64_t h2d = ((size_t)n_query + n_batch) * sizeof(uint64_t), d2h = 0;
   auto ev = [&](uint32_t bt, int k) { return h->events[(size_t)bt * kStages + k]; };
-  for (uint32_t bt = 0; bt < n_batch; bt++) {
-    const uint32_t s = bt * B, e = std::min(n_query, s + B), nb = e - s;
-    CUDA_TRY(cudaEventRecord(ev(bt, 0), st));
-    const uint32_t T = (uint32_t)(off[e] - off[s]);
-    const uint64_t *qo = w.q_off + (size_t)s + bt;
-    const float *qp;
-    if (host_io) {
-      CUDA_TRY(cudaMemcpyAsync(w.q, query + off[s] * kDim, (size_t)T * kDim * sizeof(float),
-                               cudaMemcpyHostToDevice, st));
-      h2d += (size_t)T * kDim * sizeof(float);
-      qp = w.q;
-    } else {
-      qp = query + off[s] * kDim;
+  // every device operation of the call, in stream order on `rs`
+  // (events recorded while capturing become external event-record nodes)
+  auto enqueue = [&](cudaStream_t rs, bool capturing) -> int {
+    auto rec = [&](cudaEvent_t e) {
+      return capturing ? cudaEventRecordWithFlags(e, rs, cudaEventRecordExternal)
+                       : cudaEventRecord(e, rs);
+    };
+    CUDA_TRY(cudaMemcpyAsync(w.q_off, w.h_off, ((size_t)n_query + n_batch) * sizeof(uint64_t),
+                             cudaMemcpyHostToDevice, rs));
+    for (uint32_t bt = 0; bt < n_batch; bt++) {
+      const uint32_t s = bt * B, e = std::min(n_query, s + B), nb = e - s;
+      CUDA_TRY(rec(ev(bt, 0)));
+      const uint32_t T = (uint32_t)(off[e] - off[s]);
+      const uint64_t *qo = w.q_off + (size_t)s + bt;
+      const float *qp;
+      if (host_io) {
+        CUDA_TRY(cudaMemcpyAsync(w.q, query + off[s] * kDim, (size_t)T * kDim * sizeof(float),
+                                 cudaMemcpyHostToDevice, rs));
+        h2d += (size_t)T * kDim * sizeof(float);
+        qp = w.q;
+      } else {
+        qp = query + off[s] * kDim;
+      }
+      CUDA_TRY(rec(ev(bt, 1)));
+      if (tc_probe) {
+        uint32_t tsp;
+        probe_tc_cand_per_token(T, h->dix.n_centroid, h->n_sm, &tsp);
+        CUDA_TRY(launch_probe_tc(qp, T, h->cen_sw, h->dix.centroid, h->dix.n_centroid, nprobe,
+                                 tsp, w.cand, w.probe_id, w.probe_s, h->d_err, rs, &launches));
+      } else {
+        int splits;
+        part_entries(h, T, nprobe, &splits);
+        CUDA_TRY(launch_probe(h->dix, qp, T, nprobe, splits, w.part_id, w.part_s, w.probe_id,
+                              w.probe_s, rs, &launches));
+      }
+      CUDA_TRY(rec(ev(bt, 2)));
+      CUDA_TRY(launch_filter_hash(h->dix, w.probe_id, w.probe_s, nprobe, qo, nb, w.fb_slots,
+                                  probe_topk, scr, h->d_epoch, w.short_id, w.short_approx,
+                                  w.n_short, w.qstat + (size_t)s * 3, rs, &launches,
+                                  (flags & MVR_CAND_IMPUTE) ? 1 : 0));
+      CUDA_TRY(rec(ev(bt, 3)));
+      float *os = host_io ? w.out_s : out_s + (size_t)s * topk;
+      uint32_t *oi = host_io ? w.out_id : out_id + (size_t)s * topk;
+      if (bf16) {
+        // tensor-core MaxSim (FP8 or BF16) over the whole shortlist, then the
+        // exact FP32 kernel re-scores its best R docs
+        if (fp8)
+          CUDA_TRY(launch_rerank_tmem(h->dix, h->cen8, h->wtab8, 0u, qp, qo, nb, w.short_id,
+                                      w.n_short, probe_topk, sem, nq_max, h->x_bound, w.exact,
+                                      h->d_err, rs, &launches, true));
+        else if (h->cen_perm)
+          CUDA_TRY(launch_rerank_tmem(h->dix, h->cen_perm, h->wlo, h->whi, qp, qo, nb, w.short_id,
+                                      w.n_short, probe_topk, sem, nq_max, h->x_bound, w.exact,
+                                      h->d_err, rs, &launches, false));
+        else
+          CUDA_TRY(launch_rerank_tc(h->dix, h->cen_bf16, h->lut_bf16, qp, qo, nb, w.short_id,
+                                    w.n_short, probe_topk, sem, nq_max, w.exact, h->d_err, rs,
+                                    &launches));
+        CUDA_TRY(rec(ev(bt, 4)));
+        CUDA_TRY(launch_topk(w.short_id, w.exact, w.n_short, nb, probe_topk, R, w.r_score,
+                             w.r_id, w.n_r, rs, &launches));
+        CUDA_TRY(launch_rerank(h->dix, qp, qo, nb, w.r_id, w.n_r, R, sem, w.r_exact, rs,
+                               &launches));
+        CUDA_TRY(launch_topk(w.r_id, w.r_exact, w.n_r, nb, R, topk, os, oi, nullptr, rs,
+                             &launches));
+      } else {
+        CUDA_TRY(launch_rerank(h->dix, qp, qo, nb, w.short_id, w.n_short, probe_topk, sem,
+                               w.exact, rs, &launches));
+        CUDA_TRY(rec(ev(bt, 4)));
+        CUDA_TRY(launch_topk(w.short_id, w.exact, w.n_short, nb, probe_topk, topk, os, oi,
+                             nullptr, rs, &launches));
+      }
+      CUDA_TRY(rec(ev(bt, 5)));
+      if (host_io) {
+        CUDA_TRY(cudaMemcpyAsync(out_s + (size_t)s * topk, w.out_s,
+                                 (size_t)nb * topk * sizeof(float), cudaMemcpyDeviceToHost, rs));
+        CUDA_TRY(cudaMemcpyAsync(out_id + (size_t)s * topk, w.out_id,
+                                 (size_t)nb * topk * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                 rs));
+        d2h += (size_t)nb * topk * 8;
+      }
     }
-    CUDA_TRY(cudaEventRecord(ev(bt, 1), st));
-    if (tc_probe) {
-      uint32_t tsp;
-      probe_tc_cand_per_token(T, h->dix.n_centroid, h->n_sm, &tsp);
-      CUDA_TRY(launch_probe_tc(qp, T, h->cen_sw, h->dix.centroid, h->dix.n_centroid, nprobe, tsp,
-                               w.cand, w.probe_id, w.probe_s, h->d_err, st, &launches));
-    } else {
-      int splits;
-      part_entries(h, T, nprobe, &splits);
-      CUDA_TRY(launch_probe(h->dix, qp, T, nprobe, splits, w.part_id, w.part_s, w.probe_id,
-                            w.probe_s, st, &launches));
+    CUDA_TRY(rec(h->events[(size_t)n_batch * kStages]));
+    return MVR_OK;
+  };
+
+  const bool use_graph = h->graphs && !host_io;
+  if (!use_graph) {
+    MVR_TRY(enqueue(st, false));
+  } else {
+    // device buffers with graphs on: replay the recorded call when every
+    // argument repeats, else record it (on the handle's stream, ordered
+    // after the caller's stream) and keep the instantiated graph
+    auto &G = h->graph;
+    const bool same = G.exec && G.query == query && G.out_s == out_s && G.out_id == out_id &&
+                      G.n_query == n_query && G.topk == topk && G.nprobe == nprobe &&
+                      G.probe_topk == probe_topk && G.flags == flags && G.R == R && G.B == B &&
+                      G.gen == h->ws_gen && G.off == off;
+    CUDA_TRY(cudaEventRecord(h->ev_in, st));
+    CUDA_TRY(cudaStreamWaitEvent(h->stream, h->ev_in, 0));
+    if (!same) {
+      h->drop_graph();
+      CUDA_TRY(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+      const int rc = enqueue(h->stream, true);
+      cudaGraph_t graph = nullptr;
+      const cudaError_t ec = cudaStreamEndCapture(h->stream, &graph);
+      if (rc != MVR_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+      }
+      if (ec != cudaSuccess) return set_err(MVR_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ec));
+      const cudaError_t ei = cudaGraphInstantiate(&G.exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ei != cudaSuccess) {
+        G.exec = nullptr;
+        return set_err(MVR_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ei));
+      }
+      G.query = query; G.out_s = out_s; G.out_id = out_id; G.n_query = n_query; G.topk = topk;
+      G.nprobe = nprobe; G.probe_topk = probe_topk; G.flags = flags; G.R = R; G.B = B;
+      G.gen = h->ws_gen; G.off = off; G.launches = launches;
     }
-    CUDA_TRY(cudaEventRecord(ev(bt, 2), st));
-    // stamp epochs of the fallback's chunks: epoch .. epoch + n_chunks - 1
-    const uint32_t n_chunks = (nb + w.fb_slots - 1) / w.fb_slots;
-    if (h->epoch > 0xffffffffu - n_chunks - 1) {  // stamps would wrap: clear them
-      CUDA_TRY(cudaMemsetAsync(w.stamp, 0, (size_t)w.fb_slots * h->dix.n_item * sizeof(uint32_t), st));
-      h->epoch = 0;
-    }
-    const uint32_t epoch = h->epoch + 1;
-    h->epoch += n_chunks;
-    CUDA_TRY(launch_filter_hash(h->dix, w.probe_id, w.probe_s, nprobe, qo, nb, w.fb_slots, probe_topk, scr,
-                                epoch, w.short_id, w.short_approx, w.n_short,
-                                w.qstat + (size_t)s * 3, st, &launches,
-                                (flags & MVR_CAND_IMPUTE) ? 1 : 0));
-    CUDA_TRY(cudaEventRecord(ev(bt, 3), st));
-    float *os = host_io ? w.out_s : out_s + (size_t)s * topk;
-    uint32_t *oi = host_io ? w.out_id : out_id + (size_t)s * topk;
-    if (bf16) {
-      // BF16 tensor-core MaxSim over the whole shortlist, then the exact FP32
-      // kernel re-scores its best R docs
-      if (fp8)
-        CUDA_TRY(launch_rerank_tmem(h->dix, h->cen8, h->wtab8, 0u, qp, qo, nb, w.short_id,
-                                    w.n_short, probe_topk, sem, nq_max, h->x_bound, w.exact,
-                                    h->d_err, st, &launches, true));
-      else if (h->cen_perm)
-        CUDA_TRY(launch_rerank_tmem(h->dix, h->cen_perm, h->wlo, h->whi, qp, qo, nb, w.short_id,
-                                    w.n_short, probe_topk, sem, nq_max, h->x_bound, w.exact,
-                                    h->d_err, st, &launches, false));
-      else
-        CUDA_TRY(launch_rerank_tc(h->dix, h->cen_bf16, h->lut_bf16, qp, qo, nb, w.short_id,
-                                  w.n_short, probe_topk, sem, nq_max, w.exact, h->d_err, st,
-                                  &launches));
-      CUDA_TRY(cudaEventRecord(ev(bt, 4), st));
-      CUDA_TRY(launch_topk(w.short_id, w.exact, w.n_short, nb, probe_topk, R, w.r_score, w.r_id,
-                           w.n_r, st, &launches));
-      CUDA_TRY(launch_rerank(h->dix, qp, qo, nb, w.r_id, w.n_r, R, sem, w.r_exact, st, &launches));
-      CUDA_TRY(launch_topk(w.r_id, w.r_exact, w.n_r, nb, R, topk, os, oi, nullptr, st, &launches));
-    } else {
-      CUDA_TRY(launch_rerank(h->dix, qp, qo, nb, w.short_id, w.n_short, probe_topk, sem, w.exact,
-                             st, &launches));
-      CUDA_TRY(cudaEventRecord(ev(bt, 4), st));
-      CUDA_TRY(launch_topk(w.short_id, w.exact, w.n_short, nb, probe_topk, topk, os, oi, nullptr,
-                           st, &launches));
-    }
-    CUDA_TRY(cudaEventRecord(ev(bt, 5), st));
-    if (host_io) {
-      CUDA_TRY(cudaMemcpyAsync(out_s + (size_t)s * topk, w.out_s, (size_t)nb * topk * sizeof(float),
-                               cudaMemcpyDeviceToHost, st));
-      CUDA_TRY(cudaMemcpyAsync(out_id + (size_t)s * topk, w.out_id,
-                               (size_t)nb * topk * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-      d2h += (size_t)nb * topk * 8;
-    }
+    launches = G.launches;
+    CUDA_TRY(cudaEventRecord(h->ev_g0, h->stream));
+    CUDA_TRY(cudaGraphLaunch(G.exec, h->stream));
+    CUDA_TRY(cudaEventRecord(h->ev_g1, h->stream));
+    CUDA_TRY(cudaEventRecord(h->ev_out, h->stream));
+    CUDA_TRY(cudaStreamWaitEvent(st, h->ev_out, 0));
   }
-  CUDA_TRY(cudaEventRecord(h->events[(size_t)n_batch * kStages], st));
   CUDA_TRY(cudaMemcpyAsync(w.h_qstat, w.qstat, (size_t)n_query * 3 * sizeof(uint32_t),
                            cudaMemcpyDeviceToHost, st));
   unsigned herr = 0;
@@ -523,13 +616,25 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
   }
 
   float total_ms = 0.f, max_ms = 0.f;
-  CUDA_TRY(cudaEventElapsedTime(&total_ms, h->events[0], h->events[(size_t)n_batch * kStages]));
+  if (use_graph)  // the graph launch as a whole, bracketed outside the graph
+    CUDA_TRY(cudaEventElapsedTime(&total_ms, h->ev_g0, h->ev_g1));
+  else
+    CUDA_TRY(cudaEventElapsedTime(&total_ms, h->events[0], h->events[(size_t)n_batch * kStages]));
+  // per-batch stage times from the events inside the pipeline (in a replayed
+  // graph: its external event-record nodes; if the runtime cannot time
+  // those, the stage times stay 0 and the total above still holds)
+  auto elapsed = [&](float *ms, cudaEvent_t a, cudaEvent_t b) {
+    if (cudaEventElapsedTime(ms, a, b) != cudaSuccess) {
+      cudaGetLastError();
+      *ms = 0.f;
+    }
+  };
   double stage_tot[kStages] = {0};
   for (uint32_t bt = 0; bt < n_batch; bt++) {
     float ms = 0.f, st_ms[kStages];
-    CUDA_TRY(cudaEventElapsedTime(&ms, ev(bt, 0), h->events[(size_t)(bt + 1) * kStages]));
+    elapsed(&ms, ev(bt, 0), h->events[(size_t)(bt + 1) * kStages]);
     for (int k = 0; k < kStages; k++) {
-      CUDA_TRY(cudaEventElapsedTime(&st_ms[k], ev(bt, k), h->events[(size_t)bt * kStages + k + 1]));
+      elapsed(&st_ms[k], ev(bt, k), h->events[(size_t)bt * kStages + k + 1]);
       stage_tot[k] += st_ms[k];
     }
     max_ms = std::max(max_ms, ms);
@@ -670,6 +775,12 @@ int new_handle(int device, std::unique_ptr<mvr_index> &h) {
   CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
   MVR_TRY(dalloc(&h->d_err, 1));
   CUDA_TRY(cudaMemset(h->d_err, 0, sizeof(unsigned)));
+  MVR_TRY(dalloc(&h->d_epoch, 1));
+  CUDA_TRY(cudaMemset(h->d_epoch, 0, sizeof(uint32_t)));
+  CUDA_TRY(cudaEventCreateWithFlags(&h->ev_in, cudaEventDisableTiming));
+  CUDA_TRY(cudaEventCreateWithFlags(&h->ev_out, cudaEventDisableTiming));
+  CUDA_TRY(cudaEventCreate(&h->ev_g0));
+  CUDA_TRY(cudaEventCreate(&h->ev_g1));
   return MVR_OK;
 }
 
@@ -892,6 +1003,16 @@ int mvr_index_get_info(const mvr_index *h, mvr_index_info *info) {
 int mvr_index_set_batch(mvr_index *h, uint32_t max_batch_queries) {
   if (!h) return set_err(MVR_ERR_INVALID_ARG, "null index handle");
   h->batch_cap = max_batch_queries;
+  return MVR_OK;
+}
+
+int mvr_index_set_graphs(mvr_index *h, int enable) {
+  if (!h) return set_err(MVR_ERR_INVALID_ARG, "null index handle");
+  h->graphs = enable != 0;
+  if (!h->graphs) {
+    DeviceGuard g(h->device);
+    h->drop_graph();
+  }
   return MVR_OK;
 }
 

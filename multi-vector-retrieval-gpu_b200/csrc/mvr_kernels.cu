@@ -391,7 +391,7 @@ __global__ void __launch_bounds__(kFilterThreads, 1)
 filter_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
               const float *__restrict__ probe_s, uint32_t nprobe,
               const uint64_t *__restrict__ q_off, uint32_t probe_topk,
-              FilterScratch scr, uint32_t epoch,
+              FilterScratch scr, const uint32_t *__restrict__ epoch_base, uint32_t epoch_add,
               uint32_t *__restrict__ short_id, float *__restrict__ short_approx,
               uint32_t *__restrict__ n_short_out, uint32_t *__restrict__ qstat,
               uint32_t *__restrict__ only_if, int impute) {
@@ -413,6 +413,9 @@ filter_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
   // flag is the same for every CTA of the cluster, read before any barrier;
   // it stays set until the next batch's hash filter clears it)
   if (only_if && only_if[b] == 0) return;
+  // stamp epoch of this launch: a device counter (so that a replayed CUDA
+  // graph sees a fresh epoch) plus the caller's offset
+  const uint32_t epoch = (epoch_base ? *epoch_base : 0u) + epoch_add;
   const uint64_t tok0 = q_off[b];
   const uint32_t nq = (uint32_t)(q_off[b + 1] - tok0);
   uint32_t *stamp = scr.stamp + (size_t)b * scr.n_item;
@@ -688,6 +691,8 @@ filter_hash_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
     if (part == 0) qstat[b * 3 + 1] = s_entries;
   }
 }
+
+__global__ void advance_epoch_kernel(uint32_t *epoch, uint32_t n) { *epoch += n; }
 
 // ivf_part[c][p] = first position of list c whose doc id is >= p * n_item / P
 // (p = 0..P): the doc-range sub-lists of the hash filter.
@@ -995,7 +1000,7 @@ cudaError_t launch_filter(const DevIndex &ix, const uint32_t *probe_id,
                           float *short_approx, uint32_t *n_short,
                           uint32_t *qstat, cudaStream_t st, int *n_launch) {
   filter_kernel<1><<<n_query, kFilterThreads, 0, st>>>(ix, probe_id, probe_s, nprobe, q_off,
-                                                       probe_topk, scr, epoch, short_id,
+                                                       probe_topk, scr, nullptr, epoch, short_id,
                                                        short_approx, n_short, qstat, nullptr, 0);
   *n_launch += 1;
   return cudaGetLastError();
@@ -1005,8 +1010,8 @@ cudaError_t launch_filter_cluster(const DevIndex &ix, const uint32_t *probe_id,
                                   const float *probe_s, uint32_t nprobe,
                                   const uint64_t *q_off, uint32_t n_query,
                                   uint32_t probe_topk, const FilterScratch &scr,
-                                  uint32_t epoch, uint32_t *short_id,
-                                  float *short_approx, uint32_t *n_short,
+                                  const uint32_t *epoch_base, uint32_t epoch_add,
+                                  uint32_t *short_id, float *short_approx, uint32_t *n_short,
                                   uint32_t *qstat, cudaStream_t st, int *n_launch,
                                   uint32_t *only_if, int impute) {
   cudaLaunchConfig_t cfg = {};
@@ -1022,8 +1027,8 @@ cudaError_t launch_filter_cluster(const DevIndex &ix, const uint32_t *probe_id,
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   cudaError_t e = cudaLaunchKernelEx(&cfg, filter_kernel<kFilterCluster>, ix, probe_id, probe_s,
-                                     nprobe, q_off, probe_topk, scr, epoch, short_id,
-                                     short_approx, n_short, qstat, only_if, impute);
+                                     nprobe, q_off, probe_topk, scr, epoch_base, epoch_add,
+                                     short_id, short_approx, n_short, qstat, only_if, impute);
   *n_launch += 1;
   return e != cudaSuccess ? e : cudaGetLastError();
 }
@@ -1032,7 +1037,7 @@ cudaError_t launch_filter_hash(const DevIndex &ix, const uint32_t *probe_id,
                                const float *probe_s, uint32_t nprobe,
                                const uint64_t *q_off, uint32_t n_query, uint32_t fb_slots,
                                uint32_t probe_topk, const FilterScratch &scr,
-                               uint32_t epoch, uint32_t *short_id,
+                               uint32_t *epoch, uint32_t *short_id,
                                float *short_approx, uint32_t *n_short,
                                uint32_t *qstat, cudaStream_t st, int *n_launch, int impute) {
   cudaError_t e = cudaMemsetAsync(scr.ovf, 0, (size_t)n_query * sizeof(uint32_t), st);
@@ -1050,16 +1055,19 @@ cudaError_t launch_filter_hash(const DevIndex &ix, const uint32_t *probe_id,
   if (e != cudaSuccess) return e;
   // queries whose candidates overflowed a hash table: rank-table filter, in
   // chunks of fb_slots queries over its fb_slots scratch slots; chunk c uses
-  // stamp epoch `epoch + c` (the caller reserves ceil(n_query / fb_slots))
-  for (uint32_t q0 = 0, c = 0; q0 < n_query; q0 += fb_slots, c++) {
+  // stamp epoch *epoch + 1 + c, then the counter advances by the chunk count
+  uint32_t c = 0;
+  for (uint32_t q0 = 0; q0 < n_query; q0 += fb_slots, c++) {
     const uint32_t cnt = n_query - q0 < fb_slots ? n_query - q0 : fb_slots;
     e = launch_filter_cluster(ix, probe_id, probe_s, nprobe, q_off + q0, cnt, probe_topk, scr,
-                              epoch + c, short_id + (size_t)q0 * probe_topk,
+                              epoch, 1u + c, short_id + (size_t)q0 * probe_topk,
                               short_approx + (size_t)q0 * probe_topk, n_short + q0,
                               qstat + (size_t)q0 * 3, st, n_launch, scr.ovf + q0, impute);
     if (e != cudaSuccess) return e;
   }
-  return cudaSuccess;
+  advance_epoch_kernel<<<1, 1, 0, st>>>(epoch, c);
+  *n_launch += 1;
+  return cudaGetLastError();
 }
 
 cudaError_t launch_rerank(const DevIndex &ix, const float *q, const uint64_t *q_off,

@@ -45,8 +45,8 @@ cudaError_t launch_filter_cluster(const DevIndex &ix, const uint32_t *probe_id,
                                   const float *probe_s, uint32_t nprobe,
                                   const uint64_t *q_off, uint32_t n_query,
                                   uint32_t probe_topk, const FilterScratch &scr,
-                                  uint32_t epoch, uint32_t *short_id,
-                                  float *short_approx, uint32_t *n_short,
+                                  const uint32_t *epoch_base, uint32_t epoch_add,
+                                  uint32_t *short_id, float *short_approx, uint32_t *n_short,
                                   uint32_t *qstat, cudaStream_t st, int *n_launch,
                                   uint32_t *only_if, int impute);
 // Main-path filter: shared-memory hash tables over doc ranges (8 CTAs per
@@ -55,11 +55,12 @@ cudaError_t launch_filter_cluster(const DevIndex &ix, const uint32_t *probe_id,
 // candidate's approximate score (MVR_CAND_IMPUTE) instead of 0.
 // scr: stamp / rank / key hold fb_slots slots of the rank-table fallback,
 // which runs in chunks of fb_slots queries; hkey / qcnt / ovf hold n_query.
+// epoch: device counter of the fallback's stamp epochs (advanced on device).
 cudaError_t launch_filter_hash(const DevIndex &ix, const uint32_t *probe_id,
                                const float *probe_s, uint32_t nprobe,
                                const uint64_t *q_off, uint32_t n_query, uint32_t fb_slots,
                                uint32_t probe_topk, const FilterScratch &scr,
-                               uint32_t epoch, uint32_t *short_id,
+                               uint32_t *epoch, uint32_t *short_id,
                                float *short_approx, uint32_t *n_short,
                                uint32_t *qstat, cudaStream_t st, int *n_launch, int impute);
 cudaError_t launch_rerank(const DevIndex &ix, const float *q, const uint64_t *q_off,

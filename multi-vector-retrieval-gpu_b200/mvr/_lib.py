@@ -26,7 +26,8 @@ MVR_CAND_IMPUTE = 8
 EXPORTS = (
     "mvr_last_error", "mvr_device_count", "mvr_index_load", "mvr_index_load_files",
     "mvr_index_from_arrays", "mvr_index_from_device_arrays", "mvr_index_free",
-    "mvr_index_get_info", "mvr_index_set_batch", "mvr_index_set_rescore", "mvr_search", "mvr_search_staged",
+    "mvr_index_get_info", "mvr_index_set_batch", "mvr_index_set_rescore", "mvr_index_set_graphs",
+    "mvr_search", "mvr_search_staged",
     "mvr_search_device", "mvr_search_trace", "mvr_decompress", "mvr_unpack_buckets",
     "mvr_assign_device", "mvr_pack_residual_device", "mvr_kmeans_accumulate_device",
     "mvr_filter_noalloc",
@@ -93,6 +94,7 @@ def lib():
         "mvr_index_get_info": [vp, C.POINTER(IndexInfo)],
         "mvr_index_set_batch": [vp, u32],
         "mvr_index_set_rescore": [vp, u32],
+        "mvr_index_set_graphs": [vp, i32],
         "mvr_search": [vp, vp, vp, u32, u32, u32, u32, u32, u32, vp, vp, vp, C.POINTER(Stats)],
         "mvr_search_staged": [vp, vp, vp, u32, u32, u32, u32, u32, u32, vp, vp, vp, vp,
                               C.POINTER(Stats)],

@@ -118,6 +118,10 @@ class Index:
     def set_rescore(self, n_rescore):
         check(lib().mvr_index_set_rescore(self._h, n_rescore))
 
+    def set_graphs(self, enable=True):
+        """Replay repeated search_device calls as one recorded CUDA graph."""
+        check(lib().mvr_index_set_graphs(self._h, 1 if enable else 0))
+
     # -- search ----------------------------------------------------------
     def search(self, queries, k, nprobe, probe_topk, tok_off=None, semantics=SEM_PP,
                with_stats=False, with_stages=False):

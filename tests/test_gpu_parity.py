@@ -247,6 +247,19 @@ def test_hash_filter_overflow_falls_back_bit_exact():
     qi = q[off[1]:off[2]]
     compare_trace(g.trace(qi, 10, 16, 1000, CAND_IMPUTE),
                   o.search_one(qi, 10, 16, 1000, CAND_IMPUTE))
+    # the fallback's stamp epochs advance on the device: replays of one
+    # recorded graph (two fallback chunks per batch) stay exact
+    import torch
+    dq = torch.from_numpy(q).cuda()
+    g.set_graphs(True)
+    for _ in range(3):
+        ds = torch.empty((4, 10), dtype=torch.float32, device="cuda")
+        di = torch.empty((4, 10), dtype=torch.int32, device="cuda")
+        g.search_device(dq.data_ptr(), off, 4, 0, 10, 16, 1000, ds.data_ptr(), di.data_ptr(), 0)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(di.cpu().numpy().view(np.uint32), ri)
+        np.testing.assert_array_equal(ds.cpu().numpy(), rs)
+    g.set_graphs(False)
     g.close()
 
 
@@ -264,3 +277,35 @@ def test_imputed_candidate_scores_bit_exact(pair, sem):
         for nprobe, ptk, k in ((4, 100, 10), (8, 300, 100)):
             compare_trace(g.trace(qi, k, nprobe, ptk, sem | CAND_IMPUTE),
                           o.search_one(qi, k, nprobe, ptk, sem | CAND_IMPUTE))
+
+
+def test_graph_replay_matches_direct_calls(pair):
+    """mvr_index_set_graphs: repeated mvr_search_device calls replay one
+    recorded CUDA graph; results equal the direct launches' and the oracle's,
+    for ragged queries across several batches, on every replay."""
+    import torch
+    from mvr import PREC_FP8
+    ix, g, o = pair
+    q, off = make_queries(ix, 12, (1, 64), seed=29)
+    rs, ri = o.search(q, off, 10, 6, 120)
+    dq = torch.from_numpy(q).cuda()
+    for flags in (SEM_PP, PREC_FP8):
+        outs = []
+        g.set_batch(5)
+        for graphs in (False, True, True, True):
+            g.set_graphs(graphs)
+            s = torch.empty((12, 10), dtype=torch.float32, device="cuda")
+            i = torch.empty((12, 10), dtype=torch.int32, device="cuda")
+            st = g.search_device(dq.data_ptr(), off, 12, 0, 10, 6, 120, s.data_ptr(), i.data_ptr(),
+                                 0, semantics=flags)
+            assert st.n_batch == 3
+            torch.cuda.synchronize()
+            outs.append((s.cpu().numpy(), i.cpu().numpy().view(np.uint32)))
+        g.set_graphs(False)
+        g.set_batch(0)
+        for s_, i_ in outs[1:]:
+            np.testing.assert_array_equal(i_, outs[0][1])
+            np.testing.assert_array_equal(s_, outs[0][0])
+        if flags == SEM_PP:
+            np.testing.assert_array_equal(outs[0][1], ri)
+            np.testing.assert_array_equal(outs[0][0], rs)
