@@ -435,9 +435,11 @@ def main():
     with ClockSampler(local) as clk:
         fast = measure(FAST, profile=True)
     value = fast["qps"]
-    if not args.no_graphs and fast["stage"].sum() == 0.0:
-        # stage events inside a replayed graph could not be timed: take the
-        # per-stage breakdown from host-launched steps of the same search
+    # stage events inside a replayed graph that could not be timed: take the
+    # per-stage breakdown from host-launched steps of the same search (the
+    # decision is collective, so every rank runs the same barriers)
+    untimed = mdist.max_over_ranks(float(not args.no_graphs and fast["stage"].sum() == 0.0), dev)
+    if untimed > 0.0:
         g.set_graphs(False)
         fast["stage"] = measure(FAST)["stage"]
         g.set_graphs(True)
