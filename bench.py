@@ -40,13 +40,13 @@ CACHE_VERSION = "mvr-index-v1"
 RERANK_DRAM_BYTES_PER_TOKEN = 33.2  # ncu: dram__bytes_read+write of rerank_tmem_kernel (FP8) / token
 
 WORKLOADS = {
-    # 1M docs, 65,536 centroids, nbits 2, 10,000 queries
+    # medium: 1M docs, 65,536 centroids, nbits 2, 10,000 queries (the headline workload)
     # probe_topk: the shortlist tuner's pick for recall@10 >= 0.99 against
     # exhaustive MaxSim over the index's decoded vectors (300 tuning queries)
     "medium": dict(n_doc=1_000_000, n_centroid=65536, n_bit=2, n_query=10_000, n_tok=32,
                    nprobe=8, topk=10, probe_topk=1500, kmeans_iter=4, seed=0, n_gt=100,
                    n_tune=300),
-    # 10k docs, 8,192 centroids, nbits 2, 1,000 queries
+    # small: 10k docs, 8,192 centroids, nbits 2, 1,000 queries (CPU-runnable scale)
     "small": dict(n_doc=10_000, n_centroid=8192, n_bit=2, n_query=1000, n_tok=32, nprobe=4,
                   topk=10, probe_topk=200, kmeans_iter=8, seed=0, n_gt=200, n_tune=300),
 }
