@@ -47,6 +47,11 @@ WORKLOADS = {
                    nprobe=8, topk=10, probe_topk=1500, kmeans_iter=4, seed=0, n_gt=100,
                    n_tune=300),
     # small: 10k docs, 8,192 centroids, nbits 2, 1,000 queries (CPU-runnable scale)
+    # heavy: 4-bit codes, docs up to 300 tokens, queries of 32 or 64 tokens
+    # (the corpus of the 1M-doc workload's size)
+    "heavy": dict(n_doc=1_000_000, n_centroid=65536, n_bit=4, n_query=10_000, n_tok=[32, 64],
+                  nprobe=8, topk=10, probe_topk=1500, kmeans_iter=4, seed=0, n_gt=100,
+                  n_tune=300, len_hi=300),
     "small": dict(n_doc=10_000, n_centroid=8192, n_bit=2, n_query=1000, n_tok=32, nprobe=4,
                   topk=10, probe_topk=200, kmeans_iter=8, seed=0, n_gt=200, n_tune=300),
 }
@@ -115,8 +120,8 @@ class ClockSampler:
 
 
 def cache_dir(w):
-    key = json.dumps({k: w[k] for k in ("n_doc", "n_centroid", "n_bit", "kmeans_iter", "seed")},
-                     sort_keys=True) + CACHE_VERSION
+    key = json.dumps({k: w.get(k) for k in ("n_doc", "n_centroid", "n_bit", "kmeans_iter", "seed",
+                                             "len_hi")}, sort_keys=True) + CACHE_VERSION
     return os.path.join("/tmp", "mvr_bench_cache", hashlib.sha1(key.encode()).hexdigest()[:16])
 
 
@@ -124,7 +129,7 @@ def get_index(w, device, rank, want_tokens):
     """GPU-built index (cached on local disk so both bench arms build once)."""
     import torch
     from mvr import build, formats, synth
-    spec = synth.CorpusSpec(w["n_doc"], seed=w["seed"])
+    spec = synth.CorpusSpec(w["n_doc"], seed=w["seed"], len_hi=w.get("len_hi", 180))
     cdir = cache_dir(w)
     tok = None
     t0 = time.time()
@@ -233,7 +238,8 @@ def run_reference(args, w):
 
 
 def workload_config(w, path, probe_topk):
-    return {"workload": (f"{path}: {w['n_doc']:,} synthetic docs (lognormal 70/35, clipped 8..180), "
+    return {"workload": (f"{path}: {w['n_doc']:,} synthetic docs (lognormal 70/35, clipped "
+                         f"8..{w.get('len_hi', 180)}), "
                          f"{w['n_centroid']:,} centroids, nbits {w['n_bit']}, "
                          f"{w['n_query']:,} queries x {w['n_tok']} tok, nprobe {w['nprobe']}, "
                          f"k {w['topk']}, probe_topk {probe_topk}"),
@@ -345,8 +351,13 @@ def main():
     # configuration); --use-tuned times this run's own picks instead
     ptk = {FAST: w.get("probe_topk_fast", w["probe_topk"]), PLAIN: w["probe_topk"]}
 
+    ragged = isinstance(w["n_tok"], (list, tuple))
+    q_off = off if ragged else None      # token offsets passed only for ragged queries
+    n_vec = 0 if ragged else w["n_tok"]
+    nq_avg = T / n_query                 # query tokens per query
+
     def step(flags):
-        return g.search_device(q.data_ptr(), None, n_query, w["n_tok"], k, nprobe, ptk[flags],
+        return g.search_device(q.data_ptr(), q_off, n_query, n_vec, k, nprobe, ptk[flags],
                                out_s.data_ptr(), out_i.data_ptr(), stream.cuda_stream,
                                semantics=flags)
 
@@ -357,7 +368,7 @@ def main():
     recall, tuning = {}, {}
     if rank == 0:
         n_gt, n_tune = w["n_gt"], w["n_tune"]
-        qg = q[: n_gt * w["n_tok"]]
+        qg = q[: int(off[n_gt])]
         qt, offt = synth.queries(spec, n_tune, w["n_tok"], dev, seed=900)
         _, gi_raw = exhaustive.exhaustive_topk(qg, off[: n_gt + 1], tok, spec.item_n_vec, k)
         del tok
@@ -372,10 +383,11 @@ def main():
         del dec
         torch.cuda.empty_cache()
         gi_eval, gi_tune = gi_idx[:n_gt], gi_idx[n_gt:]
-        qt_np = qt.cpu().numpy().reshape(n_tune, w["n_tok"], 128)
+        qt_np = qt.cpu().numpy() if ragged else qt.cpu().numpy().reshape(n_tune, w["n_tok"], 128)
         if not args.no_tune:
             for name, fl in (("fast", FAST), ("plain", PLAIN)):
-                t = tune.tune(g, qt_np, gi_tune, k, nprobe, args.target, fl)
+                t = tune.tune(g, qt_np, gi_tune, k, nprobe, args.target, fl,
+                              tok_off=offt if ragged else None)
                 tuning[name] = dict(probe_topk=t["probe_topk"], recall_tune=t["recall"],
                                     reached=t["reached"], fixed=ptk[fl],
                                     table=[(x["probe_topk"], round(x["recall"], 4),
@@ -453,7 +465,7 @@ def main():
     for s in range(args.warmup + args.steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        st_e = g.search_host_ptr(hq.data_ptr(), None, n_query, w["n_tok"], k, nprobe, ptk[FAST],
+        st_e = g.search_host_ptr(hq.data_ptr(), q_off, n_query, n_vec, k, nprobe, ptk[FAST],
                                  hs.data_ptr(), hi.data_ptr(), semantics=FAST, qtime=qtime)
         if s >= args.warmup:
             e2e_dt.append(time.perf_counter() - t0)
@@ -477,7 +489,9 @@ def main():
     probe_flop = 2.0 * T * C * D * S
     rerank_bytes = (4.0 + bpv) * fast["n_tok"]           # vq code + residual bytes per token
     filter_bytes = 4.0 * fast["n_ent"] + 16.0 * fast["n_cand"]  # list entries; keys out + in
-    rk = "rerank_tmem_kernel (FP8)" if FAST & PREC_FP8 else "rerank_tmem_kernel (BF16)"
+    fp8_ran = bool(FAST & PREC_FP8) and w["n_bit"] == 2  # FP8 MaxSim decodes 2-bit codes
+    rk = ("rerank_tmem_kernel (FP8)" if fp8_ran else
+          "rerank_tmem_kernel (BF16)" if w["n_bit"] <= 2 else "rerank_tc_kernel (BF16)")
     kern = {1: ("probe_tc_kernel + probe_rescore_kernel", "tensor", probe_flop / 1e12,
                 pk["tc_sus"], "TFLOP/s"),
             2: ("filter_hash_kernel + filter_select_kernel", "hbm", filter_bytes / 1e9, pk["hbm"],
@@ -490,7 +504,7 @@ def main():
     # DRAM bytes per reranked token of the FP8 rerank kernel, measured by ncu
     # on the 200,000-doc profiling case (profiles/ncu_profile_case_fp8.md),
     # scaled to a launch of this workload by its reranked tokens
-    traffic = RERANK_DRAM_BYTES_PER_TOKEN * tok_launch if (dom == 3 and FAST & PREC_FP8) else None
+    traffic = RERANK_DRAM_BYTES_PER_TOKEN * tok_launch if (dom == 3 and fp8_ran) else None
     roof = {"kernel": name, "bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
             "frac": achieved / peak, "traffic": traffic,
             "algorithmic_bytes_per_launch": rerank_bytes / n_launch if dom == 3 else None,
@@ -500,7 +514,7 @@ def main():
                                        "achieved": kern[i][2] / (stage[i] / 1e3),
                                        "frac": kern[i][2] / (stage[i] / 1e3) / kern[i][3],
                                        "unit": kern[i][4]} for i in (1, 2, 3)},
-            "rerank_tflops": 2.0 * w["n_tok"] * D * fast["n_tok"] / 1e12 / (stage[3] / 1e3),
+            "rerank_tflops": 2.0 * nq_avg * D * fast["n_tok"] / 1e12 / (stage[3] / 1e3),
             "rescore_topk_ms_per_step": float(stage[4] / S)}
 
     cpu = None
@@ -513,9 +527,10 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": S,
         "warmup": args.warmup, "ms_per_step": fast["total_ms"] / S, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
-        "config": dict(workload_config(w, f"{args.precision.upper()} tensor-core MaxSim + FP32 "
-                                          "re-score", ptk[FAST]),
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp8" if fp8_ran else "bf16",
+        "data": "synthetic",
+        "config": dict(workload_config(w, f"{'FP8' if fp8_ran else 'BF16'} tensor-core MaxSim + "
+                                          "FP32 re-score", ptk[FAST]),
                        **{"rescore": R, "probe_topk": ptk[FAST], "probe_topk_plain": ptk[PLAIN],
                           "recall@10": recall.get("fast"), "recall@10_plain": recall.get("plain"),
                           "recall@10_vs_raw": recall.get("fast_raw"),

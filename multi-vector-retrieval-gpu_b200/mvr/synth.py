@@ -73,11 +73,14 @@ def tokens(spec, device="cpu", noise=0.45, chunk=1 << 22, out=None):
 
 
 def queries(spec, n_query, n_tok=32, device="cpu", noise=0.55, seed=1):
-    """Queries built from random docs' clusters.  n_tok: int, or (lo, hi) for
-    ragged queries (token counts uniform in [lo, hi]).  Returns
-    (float32 [total_tokens, 128] tensor, uint64 token offsets [n_query+1])."""
+    """Queries built from random docs' clusters.  n_tok: int; a tuple (lo, hi)
+    for ragged queries (token counts uniform in [lo, hi]); or a list of token
+    counts drawn with equal probability.  Returns (float32 [total_tokens, 128]
+    tensor, uint64 token offsets [n_query+1])."""
     g = np.random.default_rng(seed + 7919 * spec.seed)
-    if isinstance(n_tok, (tuple, list)):
+    if isinstance(n_tok, list):
+        counts = g.choice(np.asarray(n_tok), n_query)
+    elif isinstance(n_tok, tuple):
         counts = g.integers(n_tok[0], n_tok[1] + 1, n_query)
     else:
         counts = np.full(n_query, n_tok)

@@ -19,8 +19,10 @@ from .formats import recall_at_k
 
 def tune(index, queries, gnd_ids, k, nprobe, target, semantics,
          probe_topks=(100, 150, 200, 300, 400, 600, 800, 1000, 1500, 2000),
-         rescores=(0,), repeats=3):
-    """queries: float32 [n_query, n_tok, 128] (host); gnd_ids: [n_query, >= k].
+         rescores=(0,), repeats=3, tok_off=None):
+    """queries: float32 [n_query, n_tok, 128] (host), or [total_tokens, 128]
+    with tok_off (uint64 [n_query + 1]) for ragged queries; gnd_ids:
+    [n_query, >= k].
     Returns dict(probe_topk, rescore, recall, ms, table, reached) for the
     smallest setting with mean recall@k >= target (the most accurate one if
     none reaches it); `table` lists every setting measured."""
@@ -34,8 +36,12 @@ def tune(index, queries, gnd_ids, k, nprobe, target, semantics,
             index.set_rescore(r)
             best_ms = None
             for _ in range(repeats):
-                s, i, st = index.search(queries, k, nprobe, ptk, semantics=semantics,
-                                        with_stats=True)
+                if tok_off is None:
+                    s, i, st = index.search(queries, k, nprobe, ptk, semantics=semantics,
+                                            with_stats=True)
+                else:
+                    s, i, st = index.search(queries, k, nprobe, ptk, tok_off=tok_off,
+                                            semantics=semantics, with_stats=True)
                 best_ms = st["device_ms"] if best_ms is None else min(best_ms, st["device_ms"])
             rec = float(recall_at_k(gnd_ids, i, k).mean())
             table.append(dict(probe_topk=ptk, rescore=r, recall=rec, ms=best_ms))
