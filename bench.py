@@ -489,7 +489,7 @@ def main():
     probe_flop = 2.0 * T * C * D * S
     rerank_bytes = (4.0 + bpv) * fast["n_tok"]           # vq code + residual bytes per token
     filter_bytes = 4.0 * fast["n_ent"] + 16.0 * fast["n_cand"]  # list entries; keys out + in
-    fp8_ran = bool(FAST & PREC_FP8) and w["n_bit"] == 2  # FP8 MaxSim decodes 2-bit codes
+    fp8_ran = bool(FAST & PREC_FP8) and w["n_bit"] in (2, 4)  # FP8 MaxSim: 2- and 4-bit codes
     rk = ("rerank_tmem_kernel (FP8)" if fp8_ran else
           "rerank_tmem_kernel (BF16)" if w["n_bit"] <= 2 else "rerank_tc_kernel (BF16)")
     kern = {1: ("probe_tc_kernel + probe_rescore_kernel", "tensor", probe_flop / 1e12,
@@ -501,10 +501,12 @@ def main():
     name, bound, work, peak, unit = kern[dom]
     achieved = work / (stage[dom] / 1e3)
     names = ("query_copy", "probe", "filter", "rerank", "rescore_topk", "result_copy")
-    # DRAM bytes per reranked token of the FP8 rerank kernel, measured by ncu
-    # on the 200,000-doc profiling case (profiles/ncu_profile_case_fp8.md),
-    # scaled to a launch of this workload by its reranked tokens
-    traffic = RERANK_DRAM_BYTES_PER_TOKEN * tok_launch if (dom == 3 and fp8_ran) else None
+    # DRAM bytes per reranked token of the FP8 rerank kernel on 2-bit codes,
+    # measured by ncu on the 200,000-doc profiling case
+    # (profiles/ncu_profile_case_fp8.md), scaled to a launch of this workload
+    # by its reranked tokens
+    traffic = (RERANK_DRAM_BYTES_PER_TOKEN * tok_launch
+               if (dom == 3 and fp8_ran and w["n_bit"] == 2) else None)
     roof = {"kernel": name, "bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
             "frac": achieved / peak, "traffic": traffic,
             "algorithmic_bytes_per_launch": rerank_bytes / n_launch if dom == 3 else None,

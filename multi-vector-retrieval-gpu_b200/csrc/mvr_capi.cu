@@ -3,7 +3,6 @@
 // pipeline and the index-build entry points.
 #include "mvr.h"
 
-#include <cuda_fp8.h>
 
 #include <algorithm>
 #include <chrono>
@@ -77,14 +76,6 @@ void dfree(void *p) {
   if (p) cudaFree(p);
 }
 
-// FP32 -> BF16 bits, round to nearest even (finite inputs).
-uint16_t bf16_bits(float f) {
-  uint32_t u;
-  std::memcpy(&u, &f, 4);
-  u += 0x7fffu + ((u >> 16) & 1u);
-  return (uint16_t)(u >> 16);
-}
-
 // One decode-table row per byte value: weights of its 8/b values, MSB-first
 // (SQInfoPP ctor, DataStructPP.hpp:150-187).
 std::vector<float> make_lut(uint32_t n_bit, const float *weight) {
@@ -135,7 +126,8 @@ struct Workspace {
   float *r_score = nullptr, *r_exact = nullptr;
   // per call
   size_t off_cap = 0, stat_cap = 0;
-  uint64_t *q_off = nullptr;    // device, all batches' relative offsets
+  uint64_t *q_off = nullptr;    // device, all batches' relative token offsets, then
+                                // their hash-filter CTA offsets (same layout)
   uint64_t *h_off = nullptr;    // pinned mirror
   uint32_t *qstat = nullptr;    // device [n_query][3]
   uint32_t *h_qstat = nullptr;  // pinned mirror
@@ -156,10 +148,10 @@ struct mvr_index {
   void *lut_bf16 = nullptr;      // [256][8/b] BF16 decode table
   void *cen_sw = nullptr;        // [C_pad/128][32 KB] swizzled BF16 centroid tiles
   void *cen_perm = nullptr;      // [C][64] bf16x2 centroid rows, TMEM-rerank K order (b <= 2)
-  uint32_t wlo = 0, whi = 0;     // low / high bytes of the BF16 bucket weights (b <= 2)
+  TmWeights tw_bf16{};           // weight tables of the BF16 tensor-memory MaxSim (b <= 2)
   float x_bound = 0.f;           // bound on the norm of every decoded doc token
-  void *cen8 = nullptr;          // [C][128] E4M3 centroid rows, FP8-rerank K order (b = 2)
-  uint32_t wtab8 = 0;            // E4M3 bucket weights in bytes 0..3 (b = 2)
+  void *cen8 = nullptr;          // [C][128] E4M3 centroid rows, FP8-rerank K order (b = 2, 4)
+  TmWeights tw_fp8{};            // E4M3 weight tables of the FP8 MaxSim (b = 2, 4)
   unsigned *d_err = nullptr;     // device error flags of the tensor-core kernels
   uint32_t *d_epoch = nullptr;   // stamp-epoch counter of the rank-table fallback (device)
   uint64_t epoch_used = 0;       // epochs consumed since the stamps were last cleared
@@ -444,7 +436,7 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
   MVR_TRY(ensure_scratch(h, std::min(B, n_query), rank_stride));
   MVR_TRY(ensure_batch(h, std::min(B, n_query), tok_cap, nprobe, probe_topk, topk, part_need, R,
                        cand_need));
-  MVR_TRY(ensure_call(h, (size_t)n_query + n_batch, (size_t)n_query * 3,
+  MVR_TRY(ensure_call(h, 2 * ((size_t)n_query + n_batch), (size_t)n_query * 3,
                       (size_t)kStages * n_batch + 1));
   Workspace &w = h->ws;
 
@@ -465,15 +457,24 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
   }
   h->epoch_used += call_epochs;
 
-  // relative token offsets of every batch
+  // relative token offsets of every batch, then the first hash-filter CTA
+  // of every query of the batch (prefix sum of hash_parts)
+  const size_t n_off = (size_t)n_query + n_batch;
+  std::vector<uint32_t> n_cta(n_batch);
   for (uint32_t bt = 0, pos = 0; bt < n_batch; bt++) {
     const uint32_t s = bt * B, e = std::min(n_query, s + B);
-    for (uint32_t i = s; i <= e; i++) w.h_off[pos++] = off[i] - off[s];
+    uint64_t cta = 0;
+    for (uint32_t i = s; i <= e; i++, pos++) {
+      w.h_off[pos] = off[i] - off[s];
+      w.h_off[n_off + pos] = cta;
+      if (i < e) cta += hash_parts((uint32_t)(off[i + 1] - off[i]), nprobe);
+    }
+    n_cta[bt] = (uint32_t)cta;
   }
 
   FilterScratch scr{w.stamp, w.rank, w.key, h->dix.n_item, w.rank_stride, w.qcnt, w.ovf, w.hkey};
   int launches = 0;
-  uint64_t h2d = ((size_t)n_query + n_batch) * sizeof(uint64_t), d2h = 0;
+  uint64_t h2d = 2 * n_off * sizeof(uint64_t), d2h = 0;
   auto ev = [&](uint32_t bt, int k) { return h->events[(size_t)bt * kStages + k]; };
   // every device operation of the call, in stream order on `rs`
   // (events recorded while capturing become external event-record nodes)
@@ -482,7 +483,7 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
       return capturing ? cudaEventRecordWithFlags(e, rs, cudaEventRecordExternal)
                        : cudaEventRecord(e, rs);
     };
-    CUDA_TRY(cudaMemcpyAsync(w.q_off, w.h_off, ((size_t)n_query + n_batch) * sizeof(uint64_t),
+    CUDA_TRY(cudaMemcpyAsync(w.q_off, w.h_off, 2 * n_off * sizeof(uint64_t),
                              cudaMemcpyHostToDevice, rs));
     for (uint32_t bt = 0; bt < n_batch; bt++) {
       const uint32_t s = bt * B, e = std::min(n_query, s + B), nb = e - s;
@@ -511,7 +512,8 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
                               w.probe_s, rs, &launches));
       }
       CUDA_TRY(rec(ev(bt, 2)));
-      CUDA_TRY(launch_filter_hash(h->dix, w.probe_id, w.probe_s, nprobe, qo, nb, w.fb_slots,
+      CUDA_TRY(launch_filter_hash(h->dix, w.probe_id, w.probe_s, nprobe, qo, qo + n_off,
+                                  n_cta[bt], nb, w.fb_slots,
                                   probe_topk, scr, h->d_epoch, w.short_id, w.short_approx,
                                   w.n_short, w.qstat + (size_t)s * 3, rs, &launches,
                                   (flags & MVR_CAND_IMPUTE) ? 1 : 0));
@@ -522,11 +524,11 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
         // tensor-core MaxSim (FP8 or BF16) over the whole shortlist, then the
         // exact FP32 kernel re-scores its best R docs
         if (fp8)
-          CUDA_TRY(launch_rerank_tmem(h->dix, h->cen8, h->wtab8, 0u, qp, qo, nb, w.short_id,
+          CUDA_TRY(launch_rerank_tmem(h->dix, h->cen8, h->tw_fp8, qp, qo, nb, w.short_id,
                                       w.n_short, probe_topk, sem, nq_max, h->x_bound, w.exact,
                                       h->d_err, rs, &launches, true));
         else if (h->cen_perm)
-          CUDA_TRY(launch_rerank_tmem(h->dix, h->cen_perm, h->wlo, h->whi, qp, qo, nb, w.short_id,
+          CUDA_TRY(launch_rerank_tmem(h->dix, h->cen_perm, h->tw_bf16, qp, qo, nb, w.short_id,
                                       w.n_short, probe_topk, sem, nq_max, h->x_bound, w.exact,
                                       h->d_err, rs, &launches, false));
         else
@@ -690,32 +692,27 @@ int finish_index(mvr_index *h, const uint32_t *item_n_vec_host, const uint32_t *
   MVR_TRY(dalloc(&sw, (size_t)d.n_centroid_pad * 256, &h->bufs));
   CUDA_TRY(make_centroid_tiles(d.centroid, d.n_centroid, d.n_centroid_pad / 64, sw, h->stream));
   h->cen_sw = sw;
-  if (tmem_rerank_supported(d.n_bit)) {
-    uint32_t *cp;
-    MVR_TRY(dalloc(&cp, (size_t)d.n_centroid * 64, &h->bufs));
-    CUDA_TRY(make_centroid_perm(d.centroid, d.n_centroid, d.n_bit, cp, h->stream));
-    h->cen_perm = cp;
-    h->wlo = h->whi = 0;
+  if (tmem_rerank_supported(d.n_bit) || fp8_rerank_supported(d.n_bit)) {
     float wmax = 0.f;
     for (uint32_t k = 0; k < (1u << d.n_bit); k++) wmax = std::max(wmax, std::fabs(weight[k]));
     float cmax = 0.f;
     CUDA_TRY(max_centroid_norm(d.centroid, d.n_centroid, h->d_err, &cmax, h->stream));
     CUDA_TRY(cudaMemsetAsync(h->d_err, 0, sizeof(unsigned), h->stream));  // was scratch
     h->x_bound = cmax + std::sqrt((float)kDim) * wmax;
-    if (fp8_rerank_supported(d.n_bit)) {
-      uint8_t *c8;
-      MVR_TRY(dalloc(&c8, (size_t)d.n_centroid * kDim, &h->bufs));
-      CUDA_TRY(make_centroid_fp8(d.centroid, d.n_centroid, c8, h->stream));
-      h->cen8 = c8;
-      h->wtab8 = 0;
-      for (uint32_t k = 0; k < 4; k++)
-        h->wtab8 |= (uint32_t)__nv_cvt_float_to_fp8(weight[k], __NV_SATFINITE, __NV_E4M3) << (8 * k);
-    }
-    for (uint32_t k = 0; k < (1u << d.n_bit); k++) {
-      const uint16_t wb = bf16_bits(weight[k]);
-      h->wlo |= (uint32_t)(wb & 0xffu) << (8 * k);
-      h->whi |= (uint32_t)(wb >> 8) << (8 * k);
-    }
+  }
+  if (tmem_rerank_supported(d.n_bit)) {
+    uint32_t *cp;
+    MVR_TRY(dalloc(&cp, (size_t)d.n_centroid * 64, &h->bufs));
+    CUDA_TRY(make_centroid_perm(d.centroid, d.n_centroid, d.n_bit, cp, h->stream));
+    h->cen_perm = cp;
+    h->tw_bf16 = make_tm_weights(d.n_bit, weight, false);
+  }
+  if (fp8_rerank_supported(d.n_bit)) {
+    uint8_t *c8;
+    MVR_TRY(dalloc(&c8, (size_t)d.n_centroid * kDim, &h->bufs));
+    CUDA_TRY(make_centroid_fp8(d.centroid, d.n_centroid, d.n_bit, c8, h->stream));
+    h->cen8 = c8;
+    h->tw_fp8 = make_tm_weights(d.n_bit, weight, true);
   }
   uint32_t *ipart;
   MVR_TRY(dalloc(&ipart, (size_t)d.n_centroid * (kHashParts + 1), &h->bufs));

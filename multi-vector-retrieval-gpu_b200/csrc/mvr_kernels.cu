@@ -551,8 +551,8 @@ filter_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
 }
 
 // ---------------------------------------------------------------------
-// Hash-table filter (main search path).  kHashParts CTAs share a query; CTA
-// p owns the docs [p * n_item / P, (p + 1) * n_item / P) and keeps one
+// Hash-table filter (main search path).  P = hash_parts(nq, nprobe) CTAs
+// share a query; CTA p owns the docs [p * n_item / P, (p + 1) * n_item / P) and keeps one
 // shared-memory hash-table slot per candidate doc of its range: doc id, the
 // mask of query tokens that have visited it and the exact fixed-point sum of
 // the first-visit probe scores.  The IVF lists are sorted by doc id, so the
@@ -568,7 +568,6 @@ filter_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
 // scr.ovf and the rank-table filter redoes that query.
 // ---------------------------------------------------------------------
 constexpr uint32_t kHashLog = 13, kHashCap = 1u << kHashLog;  // slots per CTA
-constexpr uint32_t kHashFill = kHashKeys / kHashParts;         // inserts allowed per CTA
 static_assert(kHashFill + 1024 <= kHashCap, "the fill limit must keep >= 1024 slots empty");
 constexpr uint32_t kEmpty = 0xffffffffu;
 
@@ -580,8 +579,8 @@ template <int MW>
 __global__ void __launch_bounds__(kFilterThreads, 1)
 filter_hash_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
                    const float *__restrict__ probe_s, uint32_t nprobe,
-                   const uint64_t *__restrict__ q_off, FilterScratch scr,
-                   uint32_t *__restrict__ qstat, int impute) {
+                   const uint64_t *__restrict__ q_off, const uint64_t *__restrict__ cta_off,
+                   uint32_t n_query, FilterScratch scr, uint32_t *__restrict__ qstat, int impute) {
   extern __shared__ __align__(16) uint8_t hsm[];
   uint32_t *tkey = reinterpret_cast<uint32_t *>(hsm);                      // [cap]
   uint32_t *tmask = tkey + kHashCap;                                       // [cap][MW]
@@ -591,11 +590,17 @@ filter_hash_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
   __shared__ uint64_t lof[kMaxQueryTok * kMaxProbe];   // and offsets in ivf_ids
   __shared__ long long impf[kMaxQueryTok];  // imputed score of an unmatched token (0: off)
   __shared__ long long s_imp;               // sum of impf over the query's tokens
-  __shared__ uint32_t s_fill, s_ovf, s_entries;
+  __shared__ uint32_t s_fill, s_ovf, s_entries, s_b;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int n_warp = blockDim.x >> 5;
-  const uint32_t b = blockIdx.x / kHashParts, part = blockIdx.x % kHashParts;
+  // this CTA's query and doc range: cta_off[b] <= blockIdx.x < cta_off[b + 1]
+  for (uint32_t i = tid; i < n_query; i += blockDim.x)
+    if (cta_off[i] <= blockIdx.x && blockIdx.x < cta_off[i + 1]) s_b = i;
+  __syncthreads();
+  const uint32_t b = s_b;
+  const uint32_t part = blockIdx.x - (uint32_t)cta_off[b];
+  const uint32_t pstep = (uint32_t)kHashParts / (uint32_t)(cta_off[b + 1] - cta_off[b]);
   const uint64_t tok0 = q_off[b];
   const uint32_t nq = (uint32_t)(q_off[b + 1] - tok0);
   const unsigned lt_mask = (1u << lane) - 1u;
@@ -622,9 +627,9 @@ filter_hash_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
     uint32_t p0 = 0, p1 = 0;
     uint64_t o = 0;
     if (c < ix.n_centroid) {
-      const uint32_t *pt = ix.ivf_part + (size_t)c * (kHashParts + 1) + part;
+      const uint32_t *pt = ix.ivf_part + (size_t)c * (kHashParts + 1) + part * pstep;
       p0 = pt[0];
-      p1 = pt[1];
+      p1 = pt[pstep];
       o = ix.ivf_off[c];
       ent += ix.ivf_size[c];
     }
@@ -1035,7 +1040,8 @@ cudaError_t launch_filter_cluster(const DevIndex &ix, const uint32_t *probe_id,
 
 cudaError_t launch_filter_hash(const DevIndex &ix, const uint32_t *probe_id,
                                const float *probe_s, uint32_t nprobe,
-                               const uint64_t *q_off, uint32_t n_query, uint32_t fb_slots,
+                               const uint64_t *q_off, const uint64_t *cta_off, uint32_t n_cta,
+                               uint32_t n_query, uint32_t fb_slots,
                                uint32_t probe_topk, const FilterScratch &scr,
                                uint32_t *epoch, uint32_t *short_id,
                                float *short_approx, uint32_t *n_short,
@@ -1043,11 +1049,11 @@ cudaError_t launch_filter_hash(const DevIndex &ix, const uint32_t *probe_id,
   cudaError_t e = cudaMemsetAsync(scr.ovf, 0, (size_t)n_query * sizeof(uint32_t), st);
   if (e != cudaSuccess) return e;
   if (scr.rank_stride <= 32)
-    filter_hash_kernel<1><<<n_query * kHashParts, kFilterThreads, hash_smem_bytes(1), st>>>(
-        ix, probe_id, probe_s, nprobe, q_off, scr, qstat, impute);
+    filter_hash_kernel<1><<<n_cta, kFilterThreads, hash_smem_bytes(1), st>>>(
+        ix, probe_id, probe_s, nprobe, q_off, cta_off, n_query, scr, qstat, impute);
   else
-    filter_hash_kernel<2><<<n_query * kHashParts, kFilterThreads, hash_smem_bytes(2), st>>>(
-        ix, probe_id, probe_s, nprobe, q_off, scr, qstat, impute);
+    filter_hash_kernel<2><<<n_cta, kFilterThreads, hash_smem_bytes(2), st>>>(
+        ix, probe_id, probe_s, nprobe, q_off, cta_off, n_query, scr, qstat, impute);
   filter_select_kernel<<<n_query, kFilterThreads, 0, st>>>(ix, probe_topk, scr, short_id,
                                                           short_approx, n_short, qstat);
   *n_launch += 2;

@@ -20,7 +20,16 @@ struct FilterScratch {
 
 // Candidate keys one query can hold in the hash filter: every doc range
 // stops inserting at kHashFill candidates, beyond which the query overflows.
-constexpr uint32_t kHashKeys = 8u * 7168u;
+constexpr uint32_t kHashFill = 7168u;
+constexpr uint32_t kHashKeys = (uint32_t)kHashParts * kHashFill;
+
+// Doc ranges (CTAs) of one query in the hash filter: 8, or 16 when the
+// query probes more than 256 lists (nq * nprobe), whose candidate sets
+// outgrow 8 * kHashFill.  Each range is a union of kHashParts / P
+// consecutive ranges of the partition table.
+inline uint32_t hash_parts(uint32_t nq, uint32_t nprobe) {
+  return (uint64_t)nq * nprobe > 256u ? 16u : 8u;
+}
 
 cudaError_t configure_kernels();
 // ivf_part table of an index ([C][kHashParts + 1] u32)
@@ -49,8 +58,10 @@ cudaError_t launch_filter_cluster(const DevIndex &ix, const uint32_t *probe_id,
                                   uint32_t *short_id, float *short_approx, uint32_t *n_short,
                                   uint32_t *qstat, cudaStream_t st, int *n_launch,
                                   uint32_t *only_if, int impute);
-// Main-path filter: shared-memory hash tables over doc ranges (8 CTAs per
-// query), a select kernel, and the rank-table filter for overflowed queries.
+// Main-path filter: shared-memory hash tables over doc ranges (hash_parts
+// CTAs per query), a select kernel, and the rank-table filter for overflowed
+// queries.  cta_off[0..n_query]: first CTA of every query (prefix sum of
+// hash_parts), n_cta = cta_off[n_query].
 // impute: an unmatched query token adds its lowest probed score to a
 // candidate's approximate score (MVR_CAND_IMPUTE) instead of 0.
 // scr: stamp / rank / key hold fb_slots slots of the rank-table fallback,
@@ -58,7 +69,8 @@ cudaError_t launch_filter_cluster(const DevIndex &ix, const uint32_t *probe_id,
 // epoch: device counter of the fallback's stamp epochs (advanced on device).
 cudaError_t launch_filter_hash(const DevIndex &ix, const uint32_t *probe_id,
                                const float *probe_s, uint32_t nprobe,
-                               const uint64_t *q_off, uint32_t n_query, uint32_t fb_slots,
+                               const uint64_t *q_off, const uint64_t *cta_off, uint32_t n_cta,
+                               uint32_t n_query, uint32_t fb_slots,
                                uint32_t probe_topk, const FilterScratch &scr,
                                uint32_t *epoch, uint32_t *short_id,
                                float *short_approx, uint32_t *n_short,

@@ -512,9 +512,22 @@ __device__ __forceinline__ void tm_decode16(const uint32_t *res, const uint4 *ce
 // the centroid row goes from its loads to TMEM unchanged.  Query tokens are
 // quantized with per-token power-of-two scales (their largest entry maps into
 // [112, 224]), removed from the per-doc maxima at the end.
+//
+// 4-bit codes: the residual word's nibbles are PRMT selectors themselves
+// (selector nibble e of a word holds the code of dim e ^ 1, the high nibble of
+// each byte being its first dim), but 16 weights do not fit PRMT's 8-byte
+// table.  Three PRMTs per 4 dims cover them: the magnitudes |W[0..7]| with
+// the codes as selectors, |W[8..15]| with the codes ^ 8; a selector >= 8
+// makes PRMT return the sign of the addressed byte replicated, 0x00 for a
+// magnitude, so OR-ing the two picks the right one.  A third table holds the
+// signs: byte j has bit 6 = sign of W[j], bit 7 = sign of W[8 + j], so with
+// the codes as selectors bit 6 of the result is the sign of W[code] in both
+// halves; shifted to bit 7 it completes the E4M3 byte.  K position kappa of
+// an 8-dim word block holds dim kappa ^ 1.
+template <int NBIT>
 __host__ __device__ constexpr uint32_t fp8_dim_of(uint32_t kappa) {
   constexpr uint8_t kFp8Dim[16] = {3, 1, 7, 5, 11, 9, 15, 13, 2, 0, 6, 4, 10, 8, 14, 12};
-  return (kappa & ~15u) + kFp8Dim[kappa & 15u];
+  return NBIT == 4 ? kappa ^ 1u : (kappa & ~15u) + kFp8Dim[kappa & 15u];
 }
 
 // kind::f8f6f4 instruction descriptor: E4M3 A/B, FP32 D, both K-major.
@@ -543,16 +556,36 @@ __device__ __forceinline__ void fp8_decode16(const uint32_t *res, uint32_t wtab,
   }
 }
 
+// 4 E4M3 weights of the 4 codes in the low 16 bits of s (x = s ^ 0x8888)
+__device__ __forceinline__ uint32_t fp8_pick4(uint32_t s, uint32_t x, const TmWeights &t) {
+  const uint32_t a = prmt(t.w[0], t.w[1], s);  // |W[c]| for c < 8, else 0
+  const uint32_t b = prmt(t.w[2], t.w[3], x);  // |W[c]| for c >= 8, else 0
+  const uint32_t g = prmt(t.w[4], t.w[5], s);  // bit 6 of each byte: sign of W[c]
+  return a | b | ((g << 1) & 0x80808080u);
+}
+
+// 16 A_r columns of one 64-dim half row from its 8 residual words (4-bit)
+__device__ __forceinline__ void fp8_decode16_b4(const uint32_t *res, const TmWeights &t,
+                                                uint32_t (&out)[16]) {
+#pragma unroll
+  for (int wi = 0; wi < 8; wi++) {
+    const uint32_t s = res[wi], x = s ^ 0x88888888u;
+    out[2 * wi] = fp8_pick4(s, x, t);
+    out[2 * wi + 1] = fp8_pick4(s >> 16, x >> 16, t);
+  }
+}
+
 template <int NBIT, bool FP8>
 __global__ void __launch_bounds__(kTmThreads, 2)
-rerank_tmem_kernel(DevIndex ix, const uint32_t *__restrict__ cen_perm, uint32_t wlo, uint32_t whi,
+rerank_tmem_kernel(DevIndex ix, const uint32_t *__restrict__ cen_perm, TmWeights tw,
                    const float *__restrict__ q, const uint64_t *__restrict__ q_off,
                    const uint32_t *__restrict__ short_id, const uint32_t *__restrict__ n_short,
                    uint32_t probe_topk, int semantics, uint32_t n_max, float x_bound,
                    float *__restrict__ approx, unsigned *__restrict__ err) {
-  static_assert(!FP8 || NBIT == 2, "the FP8 rerank decodes 2-bit codes");
+  static_assert(FP8 ? (NBIT == 2 || NBIT == 4) : (NBIT == 1 || NBIT == 2),
+                "BF16 decodes 1- and 2-bit codes, FP8 2- and 4-bit codes");
   constexpr int VPB = 8 / NBIT;
-  constexpr int HW = 64 / (4 * VPB);  // residual words of a 64-dim half row (4 or 2)
+  constexpr int HW = 64 / (4 * VPB);  // residual words of a 64-dim half row (8, 4 or 2)
   constexpr int CW = FP8 ? 16 : 32;   // centroid words (TMEM columns) of a half row
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -609,7 +642,7 @@ rerank_tmem_kernel(DevIndex ix, const uint32_t *__restrict__ cen_perm, uint32_t 
       float amax = 0.0f, ss = 0.0f;
 #pragma unroll
       for (int u = 0; u < 16; u++) {
-        x[u] = (uint32_t)row < nq ? __ldg(q + (tok0 + row) * kDim + fp8_dim_of(16 * ch + u)) : 0.0f;
+        x[u] = (uint32_t)row < nq ? __ldg(q + (tok0 + row) * kDim + fp8_dim_of<NBIT>(16 * ch + u)) : 0.0f;
         amax = fmaxf(amax, fabsf(x[u]));
         ss = fmaf(x[u], x[u], ss);
       }
@@ -696,7 +729,12 @@ rerank_tmem_kernel(DevIndex ix, const uint32_t *__restrict__ cen_perm, uint32_t 
   };
   auto load_res = [&](uint64_t v, uint32_t (&r)[HW]) {
     const uint8_t *p = ix.residual + v * ix.bytes_per_vec + hf * (HW * 4);
-    if constexpr (HW == 4) {
+    if constexpr (HW == 8) {
+      const uint4 t0 = __ldg(reinterpret_cast<const uint4 *>(p));
+      const uint4 t1 = __ldg(reinterpret_cast<const uint4 *>(p) + 1);
+      r[0] = t0.x; r[1] = t0.y; r[2] = t0.z; r[3] = t0.w;
+      r[4] = t1.x; r[5] = t1.y; r[6] = t1.z; r[7] = t1.w;
+    } else if constexpr (HW == 4) {
       const uint4 t = __ldg(reinterpret_cast<const uint4 *>(p));
       r[0] = t.x; r[1] = t.y; r[2] = t.z; r[3] = t.w;
     } else {
@@ -787,7 +825,8 @@ rerank_tmem_kernel(DevIndex ix, const uint32_t *__restrict__ cen_perm, uint32_t 
       }
       tmem_st16(acol, out);
       if (doc_c >= 0) {
-        fp8_decode16(res_c, wlo, out);
+        if constexpr (NBIT == 4) fp8_decode16_b4(res_c, tw, out);
+        else fp8_decode16(res_c, tw.w[0], out);
       } else {
 #pragma unroll
         for (int u = 0; u < 16; u++) out[u] = 0u;
@@ -799,7 +838,7 @@ rerank_tmem_kernel(DevIndex ix, const uint32_t *__restrict__ cen_perm, uint32_t 
       for (int part = 0; part < 2; part++) {
         uint32_t out[16];
         if (doc_c >= 0) {
-          tm_decode16<NBIT>(res_c + part * (HW / 2), cen + part * 4, wlo, whi, out);
+          tm_decode16<NBIT>(res_c + part * (HW / 2), cen + part * 4, tw.w[0], tw.w[1], out);
         } else {
 #pragma unroll
           for (int u = 0; u < 16; u++) out[u] = 0u;
@@ -1235,6 +1274,8 @@ cudaError_t configure_tc_kernels() {
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(rerank_tmem_kernel<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tm_smem_bytes(64));
   if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(rerank_tmem_kernel<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tm_smem_bytes(64));
+  if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(rerank_tc_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem_bytes(8, 64));
 }
 
@@ -1260,22 +1301,50 @@ cudaError_t launch_rerank_tc(const DevIndex &ix, const void *cen_bf16, const voi
 }
 
 bool tmem_rerank_supported(uint32_t n_bit) { return n_bit == 1 || n_bit == 2; }
-bool fp8_rerank_supported(uint32_t n_bit) { return n_bit == 2; }
+bool fp8_rerank_supported(uint32_t n_bit) { return n_bit == 2 || n_bit == 4; }
+
+TmWeights make_tm_weights(uint32_t n_bit, const float *weight, bool fp8) {
+  TmWeights t{};
+  auto e4m3 = [](float v) { return (uint32_t)__nv_cvt_float_to_fp8(v, __NV_SATFINITE, __NV_E4M3); };
+  if (fp8 && n_bit == 4) {
+    for (uint32_t k = 0; k < 16; k++) {
+      const uint32_t e = e4m3(weight[k]);
+      const uint32_t j = k & 7u, sh = 8u * (j & 3u);
+      t.w[(k >> 3) * 2 + (j >> 2)] |= (e & 0x7fu) << sh;          // magnitude tables
+      t.w[4 + (j >> 2)] |= ((e >> 7) << (k < 8 ? 6u : 7u)) << sh;  // sign table
+    }
+  } else if (fp8) {
+    for (uint32_t k = 0; k < (1u << n_bit); k++) t.w[0] |= e4m3(weight[k]) << (8 * k);
+  } else {
+    for (uint32_t k = 0; k < (1u << n_bit) && k < 4; k++) {
+      const __nv_bfloat16 b = __float2bfloat16_rn(weight[k]);
+      const uint16_t wb = *reinterpret_cast<const uint16_t *>(&b);
+      t.w[0] |= (uint32_t)(wb & 0xffu) << (8 * k);
+      t.w[1] |= (uint32_t)(wb >> 8) << (8 * k);
+    }
+  }
+  return t;
+}
 
 // cen8[c][k] = E4M3 of centroid c at K position k of the FP8 rerank order
+template <int NBIT>
 __global__ void perm_centroid_fp8_kernel(const float *__restrict__ cen, uint32_t n_cent,
                                          uint8_t *__restrict__ out) {
   const size_t n = (size_t)n_cent * kDim;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
     const size_t c = i / kDim;
-    out[i] = __nv_cvt_float_to_fp8(cen[c * kDim + fp8_dim_of((uint32_t)(i % kDim))], __NV_SATFINITE,
-                                   __NV_E4M3);
+    out[i] = __nv_cvt_float_to_fp8(cen[c * kDim + fp8_dim_of<NBIT>((uint32_t)(i % kDim))],
+                                   __NV_SATFINITE, __NV_E4M3);
   }
 }
 
-cudaError_t make_centroid_fp8(const float *cen, uint32_t n_cent, void *out, cudaStream_t st) {
-  perm_centroid_fp8_kernel<<<592, 256, 0, st>>>(cen, n_cent, reinterpret_cast<uint8_t *>(out));
+cudaError_t make_centroid_fp8(const float *cen, uint32_t n_cent, uint32_t n_bit, void *out,
+                              cudaStream_t st) {
+  uint8_t *o = reinterpret_cast<uint8_t *>(out);
+  if (n_bit == 2) perm_centroid_fp8_kernel<2><<<592, 256, 0, st>>>(cen, n_cent, o);
+  else if (n_bit == 4) perm_centroid_fp8_kernel<4><<<592, 256, 0, st>>>(cen, n_cent, o);
+  else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
 
@@ -1316,27 +1385,27 @@ cudaError_t make_centroid_perm(const float *cen, uint32_t n_cent, uint32_t n_bit
   return cudaGetLastError();
 }
 
-cudaError_t launch_rerank_tmem(const DevIndex &ix, const void *cen_perm, uint32_t wlo, uint32_t whi,
+cudaError_t launch_rerank_tmem(const DevIndex &ix, const void *cen_perm, const TmWeights &tw,
                                const float *q, const uint64_t *q_off, uint32_t n_query,
                                const uint32_t *short_id, const uint32_t *n_short,
                                uint32_t probe_topk, int semantics, uint32_t nq_max, float x_bound,
                                float *approx, unsigned *err, cudaStream_t st, int *n_launch,
                                bool fp8) {
-  if (fp8 && ix.n_bit != 2) return cudaErrorInvalidValue;
+  if (fp8 ? !fp8_rerank_supported(ix.n_bit) : !tmem_rerank_supported(ix.n_bit))
+    return cudaErrorInvalidValue;
   dim3 grid((probe_topk + kTmDocs - 1) / kTmDocs, n_query);
   const uint32_t n_max = nq_max <= 32 ? 32u : 64u;
   const size_t sm = tm_smem_bytes(n_max);
   const uint32_t *c = reinterpret_cast<const uint32_t *>(cen_perm);
-  switch (ix.n_bit) {
-    case 1: rerank_tmem_kernel<1, false><<<grid, kTmThreads, sm, st>>>(ix, c, wlo, whi, q, q_off, short_id, n_short, probe_topk, semantics, n_max, x_bound, approx, err); break;
-    case 2:
-      if (fp8)
-        rerank_tmem_kernel<2, true><<<grid, kTmThreads, sm, st>>>(ix, c, wlo, whi, q, q_off, short_id, n_short, probe_topk, semantics, n_max, x_bound, approx, err);
-      else
-        rerank_tmem_kernel<2, false><<<grid, kTmThreads, sm, st>>>(ix, c, wlo, whi, q, q_off, short_id, n_short, probe_topk, semantics, n_max, x_bound, approx, err);
-      break;
-    default: return cudaErrorInvalidValue;
-  }
+#define MVR_TM_LAUNCH(NB, F8)                                                                   \
+  rerank_tmem_kernel<NB, F8><<<grid, kTmThreads, sm, st>>>(ix, c, tw, q, q_off, short_id, n_short, \
+                                                           probe_topk, semantics, n_max, x_bound, \
+                                                           approx, err)
+  if (fp8 && ix.n_bit == 4) MVR_TM_LAUNCH(4, true);
+  else if (fp8) MVR_TM_LAUNCH(2, true);
+  else if (ix.n_bit == 2) MVR_TM_LAUNCH(2, false);
+  else MVR_TM_LAUNCH(1, false);
+#undef MVR_TM_LAUNCH
   *n_launch += 1;
   return cudaGetLastError();
 }

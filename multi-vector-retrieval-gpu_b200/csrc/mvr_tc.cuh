@@ -13,27 +13,38 @@ cudaError_t launch_rerank_tc(const DevIndex &ix, const void *cen_bf16, const voi
                              uint32_t probe_topk, int semantics, uint32_t nq_max, float *approx,
                              unsigned *err, cudaStream_t st, int *n_launch);
 
+// bucket-weight tables of the tensor-memory MaxSim kernels (make_tm_weights):
+//  BF16 (1-, 2-bit): w[0] / w[1] = low / high bytes of the BF16 weights;
+//  FP8 2-bit: w[0] = the 4 E4M3 weights;
+//  FP8 4-bit: w[0..1] = |E4M3| of weights 0..7, w[2..3] of weights 8..15,
+//             w[4..5] byte j: bit 6 = sign of weight j, bit 7 = of weight 8 + j
+struct TmWeights {
+  uint32_t w[6];
+};
+TmWeights make_tm_weights(uint32_t n_bit, const float *weight, bool fp8);
+
 // BF16 MaxSim with the decoded doc tokens in tensor memory (1- and 2-bit
 // codes); cen_perm: [C][64] bf16x2 centroid rows in the kernel's K order
-// (make_centroid_perm); wlo / whi: low / high bytes of the BF16 bucket weights;
-// x_bound: upper bound on the norm of every decoded doc token
+// (make_centroid_perm); x_bound: upper bound on the norm of every decoded
+// doc token
 bool tmem_rerank_supported(uint32_t n_bit);
 // largest L2 norm of the centroid rows (d_tmp: one device word of scratch)
 cudaError_t max_centroid_norm(const float *cen, uint32_t n_cent, unsigned *d_tmp, float *out,
                               cudaStream_t st);
 cudaError_t make_centroid_perm(const float *cen, uint32_t n_cent, uint32_t n_bit, void *out,
                                cudaStream_t st);
-cudaError_t launch_rerank_tmem(const DevIndex &ix, const void *cen_perm, uint32_t wlo, uint32_t whi,
+cudaError_t launch_rerank_tmem(const DevIndex &ix, const void *cen_perm, const TmWeights &tw,
                                const float *q, const uint64_t *q_off, uint32_t n_query,
                                const uint32_t *short_id, const uint32_t *n_short,
                                uint32_t probe_topk, int semantics, uint32_t nq_max, float x_bound,
                                float *approx, unsigned *err, cudaStream_t st, int *n_launch,
                                bool fp8);
-// FP8 (E4M3) MaxSim for 2-bit codes: cen8 [C][128] E4M3 centroid rows in
-// the FP8 kernel's K order (make_centroid_fp8); pass it as cen_perm and the 4
-// E4M3 bucket weights in the bytes of wlo, with fp8 = true
+// FP8 (E4M3) MaxSim for 2- and 4-bit codes: cen8 [C][128] E4M3 centroid
+// rows in the FP8 kernel's K order for n_bit (make_centroid_fp8); pass it as
+// cen_perm with fp8 = true
 bool fp8_rerank_supported(uint32_t n_bit);
-cudaError_t make_centroid_fp8(const float *cen, uint32_t n_cent, void *out, cudaStream_t st);
+cudaError_t make_centroid_fp8(const float *cen, uint32_t n_cent, uint32_t n_bit, void *out,
+                              cudaStream_t st);
 
 // tensor-core centroid scoring: candidates per token = splits * 16; the
 // centroid tiles hold 64 centroids each (n_tiles = C_pad / 64)

@@ -118,9 +118,20 @@ def test_tensor_core_probe_matches_exact(n_centroid):
     g.close()
 
 
-@pytest.fixture(scope="module")
-def pair2():
-    ix = tiny_index(n_doc=600, n_centroid=96, n_bit=2, seed=77)
+@pytest.fixture(scope="module", params=["b2", "b4", "b4mixed"])
+def pair2(request):
+    """2- and 4-bit indexes for the FP8 kernel; b4mixed permutes the 16 bucket
+    weights so that both halves of the code range hold weights of both signs
+    (the 4-bit decode's sign table)."""
+    n_bit = 2 if request.param == "b2" else 4
+    ix = tiny_index(n_doc=600, n_centroid=96, n_bit=n_bit, seed=77 if n_bit == 2 else 81)
+    if request.param == "b4mixed":
+        w = np.asarray(ix["weight"], np.float32)
+        perm = np.random.default_rng(3).permutation(len(w))
+        while (np.sign(w[perm[:8]]).min() >= 0 or np.sign(w[perm[:8]]).max() <= 0 or
+               np.sign(w[perm[8:]]).min() >= 0 or np.sign(w[perm[8:]]).max() <= 0):
+            perm = np.random.default_rng(int(perm[0]) + 11).permutation(len(w))
+        ix["weight"] = w[perm].copy()
     g = gpu_index(ix)
     yield ix, g, oracle_of(ix)
     g.close()
@@ -172,13 +183,14 @@ def test_fp8_rescore_all_equals_plain_and_other_widths_run(pair2):
     g.set_batch(0)
     np.testing.assert_array_equal(i, ref_i)
     np.testing.assert_array_equal(s, ref_s)
-    # a 4-bit index takes the BF16 kernel under MVR_PREC_FP8
-    ix4 = tiny_index(n_doc=200, n_centroid=40, n_bit=4, seed=78)
-    g4, o4 = gpu_index(ix4), oracle_of(ix4)
-    q4, off4 = make_queries(ix4, 3, 32, seed=56)
-    s4, i4 = g4.search(q4.reshape(3, 32, 128), 10, 4, 60, semantics=PREC_FP8)
-    for k in range(3):
-        for d, sc in zip(i4[k], s4[k]):
-            if d != 0xFFFFFFFF:
-                assert sc == o4.maxsim_item(q4[off4[k]:off4[k + 1]], d, SEM_PP)
-    g4.close()
+    # 1- and 8-bit indexes take the BF16 kernels under MVR_PREC_FP8
+    for n_bit in (1, 8):
+        ixb = tiny_index(n_doc=200, n_centroid=40, n_bit=n_bit, seed=78)
+        gb, ob = gpu_index(ixb), oracle_of(ixb)
+        qb, offb = make_queries(ixb, 3, 32, seed=56)
+        sb, ib = gb.search(qb.reshape(3, 32, 128), 10, 4, 60, semantics=PREC_FP8)
+        for k in range(3):
+            for d, sc in zip(ib[k], sb[k]):
+                if d != 0xFFFFFFFF:
+                    assert sc == ob.maxsim_item(qb[offb[k]:offb[k + 1]], d, SEM_PP)
+        gb.close()

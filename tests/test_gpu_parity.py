@@ -220,15 +220,41 @@ def test_config1_scale_gpu_built_index_bit_exact():
     torch.cuda.empty_cache()
 
 
-def test_hash_filter_overflow_falls_back_bit_exact():
-    """The main filter keeps each query's candidates in per-CTA shared-memory
-    hash tables over 8 doc ranges (at most 7,168 candidates per range).  With
-    80,000 short docs and half the centroids probed, every range overflows and
-    the rank-table filter redoes the query; with one probe nothing overflows.
-    Both must match the oracle bit for bit, and queries of the two kinds mixed
-    in one batch must not disturb each other."""
+def test_hash_filter_sixteen_ranges_bit_exact():
+    """A query that probes more than 256 lists (tokens x nprobe) spreads its
+    hash tables over 16 doc ranges instead of 8 (at most 7,168 candidates per
+    range).  With 80,000 short docs, 32 tokens at nprobe 16 give more
+    candidates than 8 ranges hold but fewer than 16 do: no overflow, and the
+    result matches the oracle bit for bit; so do 64-token queries at nprobe 4
+    (8 ranges) and 8 (16 ranges), and a ragged batch mixing both kinds."""
     lens = np.random.default_rng(11).integers(6, 12, 80_000)
     ix = tiny_index(n_doc=80_000, n_centroid=32, n_bit=2, seed=12, lengths=lens, n_latent=64)
+    g, o = gpu_index(ix), oracle_of(ix)
+    q, off = make_queries(ix, 2, 32, seed=13)
+    qi = q[off[0]:off[1]]
+    t = g.trace(qi, 10, 16, 1000)
+    compare_trace(t, o.search_one(qi, 10, 16, 1000))
+    assert 8 * 7168 < len(t["cand_id"]) <= 16 * 7168
+    q64, off64 = make_queries(ix, 2, 64, seed=14)
+    for nprobe in (4, 8):
+        qi = q64[off64[1]:off64[2]]
+        compare_trace(g.trace(qi, 10, nprobe, 800), o.search_one(qi, 10, nprobe, 800))
+    qr, offr = make_queries(ix, 6, (4, 64), seed=15)
+    s, i = g.search(qr, 10, 8, 800, tok_off=offr)
+    rs, ri = o.search(qr, offr, 10, 8, 800)
+    np.testing.assert_array_equal(i, ri)
+    np.testing.assert_array_equal(s, rs)
+    g.close()
+
+
+def test_hash_filter_overflow_falls_back_bit_exact():
+    """With 130,000 short docs and half the centroids probed, a query has more
+    candidates than even 16 hash-table ranges hold (16 x 7,168): the rank-table
+    filter redoes it; with one probe nothing overflows.  Both must match the
+    oracle bit for bit, and queries of the two kinds mixed in one batch must
+    not disturb each other."""
+    lens = np.random.default_rng(11).integers(6, 12, 130_000)
+    ix = tiny_index(n_doc=130_000, n_centroid=32, n_bit=2, seed=12, lengths=lens, n_latent=64)
     g, o = gpu_index(ix), oracle_of(ix)
     q, off = make_queries(ix, 4, 32, seed=13)
     for nprobe in (16, 1):
@@ -236,7 +262,7 @@ def test_hash_filter_overflow_falls_back_bit_exact():
         t = g.trace(qi, 10, nprobe, 1000)
         compare_trace(t, o.search_one(qi, 10, nprobe, 1000))
         if nprobe == 16:
-            assert len(t["cand_id"]) > 8 * 7168
+            assert len(t["cand_id"]) > 16 * 7168
     # mixed batch: the same queries at nprobe 16 in one call
     s, i = g.search(q, 10, 16, 1000, tok_off=off)
     rs, ri = o.search(q, off, 10, 16, 1000)
