@@ -249,16 +249,16 @@ def workload_config(w, path, probe_topk):
             "l2": "flushed (256 MiB write) between timed steps"}
 
 
-def run_profile_case(fast_flag):
+def run_profile_case(fast_flag, n_bit=2):
     """A case small enough for ncu (a few GB on the device, one batch per
     search, inputs larger than L2): the raw tokens are freed before searching,
-    so only the compressed index (~0.5 GB) and the working set are resident.
-    296 queries = 2 filter CTAs per SM."""
+    so only the compressed index (~0.5 GB at nbits 2, ~1 GB at 4) and the
+    working set are resident.  296 queries = 2 filter CTAs per SM."""
     import torch
     from mvr import build, synth
     spec = synth.CorpusSpec(200_000, seed=0)
     tok = synth.tokens(spec, "cuda")
-    ix = build.build_index(tok, spec.item_n_vec, 16384, 2, kmeans_iter=2)
+    ix = build.build_index(tok, spec.item_n_vec, 16384, n_bit, kmeans_iter=2)
     del tok
     g = build.load_built(ix)
     del ix
@@ -301,6 +301,8 @@ def main():
     ap.add_argument("--profile-case", action="store_true",
                     help="small profiling target instead of the bench: 200,000 docs, 16,384 "
                          "centroids, one mixed-precision and one plain search of 296 queries")
+    ap.add_argument("--profile-bits", type=int, choices=[1, 2, 4, 8], default=2,
+                    help="residual code width of the profiling case")
     ap.add_argument("--no-tune", action="store_true",
                     help="skip the shortlist tuner (it only reports unless --use-tuned)")
     ap.add_argument("--use-tuned", action="store_true",
@@ -316,7 +318,8 @@ def main():
         return run_reference(args, w)
     if args.profile_case:
         from mvr import PREC_BF16, PREC_FP8
-        return run_profile_case(PREC_FP8 if args.precision == "fp8" else PREC_BF16)
+        return run_profile_case(PREC_FP8 if args.precision == "fp8" else PREC_BF16,
+                                args.profile_bits)
 
     import torch
     import torch.distributed as dist
