@@ -54,6 +54,19 @@ WORKLOADS = {
                   n_tune=300, len_hi=300),
     "small": dict(n_doc=10_000, n_centroid=8192, n_bit=2, n_query=1000, n_tok=32, nprobe=4,
                   topk=10, probe_topk=200, kmeans_iter=8, seed=0, n_gt=200, n_tune=300),
+    # corpora larger than the device holds as raw tokens, built by streaming
+    # (block-keyed generator, tensor-core assignment) and scanned piecewise for
+    # the ground truths; probe_topk: starting point, the tuner reports its pick
+    # large: 4M docs, 262,144 centroids, nbits 2, ragged 8..32-token queries in
+    # batches of 4,096
+    "large": dict(n_doc=4_000_000, n_centroid=262_144, n_bit=2, n_query=16_384, n_tok=(8, 32),
+                  nprobe=8, topk=10, probe_topk=1500, kmeans_iter=4, seed=0, n_gt=100,
+                  n_tune=200, stream=True, batch=4096),
+    # xl: 8M docs up to 300 tokens, 262,144 centroids, nbits 4, 32- or 64-token
+    # queries in batches of 1,024
+    "xl": dict(n_doc=8_000_000, n_centroid=262_144, n_bit=4, n_query=10_240, n_tok=[32, 64],
+               nprobe=8, topk=10, probe_topk=1500, kmeans_iter=4, seed=0, n_gt=100, n_tune=200,
+               len_hi=300, stream=True, batch=1024),
 }
 
 
@@ -160,6 +173,41 @@ def get_index(w, device, rank, want_tokens):
     return spec, host, tok, built_s
 
 
+def get_index_stream(w, device):
+    """Index of a streamed workload, built on the device one doc range at a
+    time (the raw corpus is never resident); returns (spec, device arrays,
+    build seconds)."""
+    import torch
+    from mvr import build, synth
+    spec = synth.CorpusSpec(w["n_doc"], seed=w["seed"], len_hi=w.get("len_hi", 180))
+    t0 = time.time()
+    ix = build.build_index_stream(spec, w["n_centroid"], w["n_bit"], kmeans_iter=w["kmeans_iter"],
+                                  seed=123 + w["seed"], device=device)
+    torch.cuda.synchronize()
+    return spec, ix, time.time() - t0
+
+
+def gt_chunks(spec, tokens_of, n_q_tok):
+    """(d0, lens, tokens) pieces of the corpus for exhaustive_topk_stream:
+    generator blocks (or index ranges) of synth.BLOCK_DOCS docs, cut into
+    pieces whose FP64 score matrix stays under ~8 GB."""
+    from mvr import synth
+    lens = spec.item_n_vec.astype(np.int64)
+    max_tok = int(max(1 << 14, min(1 << 18, 8e9 / (8.0 * max(1, n_q_tok)))))
+    for b0 in range(0, spec.n_doc, synth.BLOCK_DOCS):
+        b1 = min(spec.n_doc, b0 + synth.BLOCK_DOCS)
+        x = tokens_of(b0, b1)
+        toff = np.zeros(b1 - b0 + 1, np.int64)
+        toff[1:] = np.cumsum(lens[b0:b1])
+        d0 = 0
+        while d0 < b1 - b0:
+            d1 = int(np.searchsorted(toff, toff[d0] + max_tok, side="right")) - 1
+            d1 = min(max(d1, d0 + 1), b1 - b0)
+            yield b0 + d0, lens[b0 + d0:b0 + d1], x[toff[d0]:toff[d1]]
+            d0 = d1
+        del x
+
+
 def load_gpu_index(host, device_idx):
     from mvr import Index
     return Index.from_arrays(host["item_n_vec"], host["centroid"], host["vq_code"],
@@ -192,6 +240,10 @@ def run_reference(args, w):
     import torch
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
+        return
+    if w.get("stream"):
+        print(json.dumps({"impl": "reference", "unavailable": "streamed workload: the CPU port "
+                          "needs the whole index in host memory; timed on the default workloads"}))
         return
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
@@ -286,6 +338,9 @@ def main():
     ap.add_argument("--impl", choices=["mvr", "reference"], default="mvr")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="medium")
     ap.add_argument("--probe-topk", type=int, default=None)
+    ap.add_argument("--n-doc", type=int, default=None, help="override the workload's corpus size")
+    ap.add_argument("--n-centroid", type=int, default=None,
+                    help="override the workload's centroid count")
     ap.add_argument("--rescore", type=int, default=0, help="FP32 re-score width (0: 4*k)")
     ap.add_argument("--no-graphs", action="store_true",
                     help="launch every kernel from the host instead of replaying the recorded "
@@ -314,6 +369,10 @@ def main():
     w = dict(WORKLOADS[args.workload])
     if args.probe_topk:
         w["probe_topk"] = w["probe_topk_fast"] = args.probe_topk
+    if args.n_doc:
+        w["n_doc"] = args.n_doc
+    if args.n_centroid:
+        w["n_centroid"] = args.n_centroid
     if args.impl == "reference":
         return run_reference(args, w)
     if args.profile_case:
@@ -334,11 +393,18 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(minutes=20))
 
-    spec, host, tok, built_s = get_index(w, dev, rank, want_tokens=(rank == 0))
-    g = load_gpu_index(host, local)
+    streamed = bool(w.get("stream"))
+    if streamed:
+        from mvr import build
+        spec, dix, built_s = get_index_stream(w, dev)
+        host, tok = None, None
+        g = build.load_built(dix, local)
+    else:
+        spec, host, tok, built_s = get_index(w, dev, rank, want_tokens=(rank == 0))
+        g = load_gpu_index(host, local)
     g.set_rescore(args.rescore)
-    if args.batch:
-        g.set_batch(args.batch)
+    if args.batch or w.get("batch"):
+        g.set_batch(args.batch or w["batch"])
     g.set_graphs(not args.no_graphs)
     q, off = synth.queries(spec, w["n_query"], w["n_tok"], dev, seed=100 + rank)
     n_query, T = w["n_query"], q.shape[0]
@@ -373,17 +439,33 @@ def main():
         n_gt, n_tune = w["n_gt"], w["n_tune"]
         qg = q[: int(off[n_gt])]
         qt, offt = synth.queries(spec, n_tune, w["n_tok"], dev, seed=900)
-        _, gi_raw = exhaustive.exhaustive_topk(qg, off[: n_gt + 1], tok, spec.item_n_vec, k)
-        del tok
-        torch.cuda.empty_cache()
-        dec = exhaustive.decode_tokens(torch.from_numpy(host["centroid"]).to(dev),
-                                       torch.from_numpy(host["vq_code"].view(np.int32)).to(dev),
-                                       torch.from_numpy(host["residual"]).to(dev).view(-1, 128 * host["n_bit"] // 8),
-                                       torch.from_numpy(host["weight"]), host["n_bit"])
         both = torch.cat([qg, qt])
         both_off = np.concatenate([off[: n_gt + 1], off[n_gt] + offt[1:]]).astype(np.uint64)
-        _, gi_idx = exhaustive.exhaustive_topk(both, both_off, dec, spec.item_n_vec, k)
-        del dec
+        if streamed:  # raw tokens regenerated and index vectors decoded piece by piece
+            bpv = 128 * w["n_bit"] // 8
+            toff = np.zeros(spec.n_doc + 1, np.int64)
+            toff[1:] = np.cumsum(spec.item_n_vec.astype(np.int64))
+            _, gi_raw = exhaustive.exhaustive_topk_stream(
+                qg, off[: n_gt + 1],
+                gt_chunks(spec, lambda a, b: synth.tokens_range(spec, a, b, dev), qg.shape[0]), k)
+            res2 = dix["residual"].view(-1, bpv)
+
+            def decoded(a, b):
+                return exhaustive.decode_tokens(dix["centroid"], dix["vq_code"][toff[a]:toff[b]],
+                                                res2[toff[a]:toff[b]], dix["weight"], w["n_bit"])
+            _, gi_idx = exhaustive.exhaustive_topk_stream(
+                both, both_off, gt_chunks(spec, decoded, both.shape[0]), k)
+            del dix, res2
+        else:
+            _, gi_raw = exhaustive.exhaustive_topk(qg, off[: n_gt + 1], tok, spec.item_n_vec, k)
+            del tok
+            torch.cuda.empty_cache()
+            dec = exhaustive.decode_tokens(torch.from_numpy(host["centroid"]).to(dev),
+                                           torch.from_numpy(host["vq_code"].view(np.int32)).to(dev),
+                                           torch.from_numpy(host["residual"]).to(dev).view(-1, 128 * host["n_bit"] // 8),
+                                           torch.from_numpy(host["weight"]), host["n_bit"])
+            _, gi_idx = exhaustive.exhaustive_topk(both, both_off, dec, spec.item_n_vec, k)
+            del dec
         torch.cuda.empty_cache()
         gi_eval, gi_tune = gi_idx[:n_gt], gi_idx[n_gt:]
         qt_np = qt.cpu().numpy() if ragged else qt.cpu().numpy().reshape(n_tune, w["n_tok"], 128)
@@ -523,7 +605,11 @@ def main():
             "rescore_topk_ms_per_step": float(stage[4] / S)}
 
     cpu = None
-    if world == 1 and not args.no_cpu_baseline:
+    if streamed:
+        cpu = {"value": None, "unit": "queries/s", "cores": 0, "kind": "port",
+               "sample": "not run: the streamed index lives on the device only (the CPU port "
+                         "is timed on the default workloads)"}
+    elif world == 1 and not args.no_cpu_baseline:
         qps_cpu, n_s, dt_s, _ = cpu_port_qps(host, hq.numpy(), off, w, os.cpu_count(), ptk[PLAIN])
         cpu = {"value": qps_cpu, "unit": "queries/s", "cores": os.cpu_count(), "kind": "port",
                "sample": f"first {n_s} of the {n_query} queries ({dt_s:.1f} s)"}
@@ -554,7 +640,11 @@ def main():
                           "parallelism": f"replica x{world}, queries split by rank",
                           "launch": "host launches" if args.no_graphs else
                           "one recorded CUDA graph per step (replayed)",
-                          "index_build_s": built_s, "cand_per_query": fast["n_cand"] / (S * n_query),
+                          "index_build_s": built_s,
+                          "index_build": "streamed: block-keyed generator, tensor-core assignment"
+                          if streamed else "resident corpus, FP32 assignment",
+                          "queries_per_batch": args.batch or w.get("batch") or "8 per SM",
+                          "cand_per_query": fast["n_cand"] / (S * n_query),
                           "rerank_tok_per_query": fast["n_tok"] / (S * n_query)}),
         "e2e": {"value": e2e, "unit": "queries/s",
                 "h2d_bytes_per_step": int(st_e.h2d_bytes), "d2h_bytes_per_step": int(st_e.d2h_bytes)},

@@ -268,6 +268,16 @@ int mvr_assign_device(const float *d_vec, uint64_t n_vec,
                       uint32_t dim, uint32_t *d_code, float *d_score,
                       void *cuda_stream);
 
+/* mvr_assign_device on the tensor cores, for large builds: BF16 tcgen05
+ * scoring keeps each vector's 16 best centroids per centroid split, which are
+ * re-scored with the canonical FP32 dot; code[i] is the best of those (equal
+ * to mvr_assign_device's unless the true best missed the BF16 candidates),
+ * score[i] (nullable) its FP32 score + 1. */
+int mvr_assign_tc_device(const float *d_vec, uint64_t n_vec,
+                         const float *d_centroid, uint32_t n_centroid,
+                         uint32_t dim, uint32_t *d_code, float *d_score,
+                         void *cuda_stream);
+
 /* Packed residual bytes (MSB-first, bucket = #cutoffs <= vec - centroid):
  * out [n_vec * dim*n_bit/8]. */
 int mvr_pack_residual_device(const float *d_vec, uint64_t n_vec,

@@ -1176,6 +1176,61 @@ int mvr_assign_device(const float *d_vec, uint64_t n_vec, const float *d_centroi
   return MVR_OK;
 }
 
+int mvr_assign_tc_device(const float *d_vec, uint64_t n_vec, const float *d_centroid,
+                         uint32_t n_centroid, uint32_t dim, uint32_t *d_code, float *d_score,
+                         void *cuda_stream) {
+  if (dim != (uint32_t)kDim) return set_err(MVR_ERR_UNSUPPORTED, "dim %u not supported", dim);
+  if (!d_vec || !d_centroid || !d_code || n_centroid == 0)
+    return set_err(MVR_ERR_INVALID_ARG, "null argument or no centroids");
+  if (mvr_device_count() == 0) return set_err(MVR_ERR_CUDA, "no CUDA device available");
+  cudaStream_t st = (cudaStream_t)cuda_stream;
+  CUDA_TRY(configure_tc_kernels());
+  int dev = 0, n_sm = 148;
+  CUDA_TRY(cudaGetDevice(&dev));
+  CUDA_TRY(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+  // swizzled BF16 centroid tiles (64 centroids x 256 B each)
+  const uint32_t n_tiles = (n_centroid + 63u) / 64u;
+  uint8_t *sw;
+  MVR_TRY(dalloc(&sw, (size_t)n_tiles * 64 * 256));
+  std::unique_ptr<void, void (*)(void *)> swg(sw, dfree);
+  CUDA_TRY(make_centroid_tiles(d_centroid, n_centroid, n_tiles, sw, st));
+  // token chunks of <= 1M (probe grid.y <= 8192); candidate lists sized
+  // for the largest chunk's split count
+  const uint64_t kChunk = 1ull << 20;
+  size_t cand_need = 1;
+  for (uint64_t s = 0; s < n_vec; s += kChunk) {
+    const uint32_t T = (uint32_t)std::min<uint64_t>(kChunk, n_vec - s);
+    uint32_t sp;
+    cand_need = std::max(cand_need, (size_t)T * probe_tc_cand_per_token(T, n_centroid, n_sm, &sp));
+  }
+  uint32_t *cand;
+  MVR_TRY(dalloc(&cand, cand_need));
+  std::unique_ptr<void, void (*)(void *)> cg(cand, dfree);
+  float *score = d_score;
+  std::unique_ptr<void, void (*)(void *)> sg(nullptr, dfree);
+  if (!score) {
+    MVR_TRY(dalloc(&score, std::min<uint64_t>(std::max<uint64_t>(n_vec, 1), kChunk)));
+    sg.reset(score);
+  }
+  unsigned *err;
+  MVR_TRY(dalloc(&err, 1));
+  std::unique_ptr<void, void (*)(void *)> eg(err, dfree);
+  CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(unsigned), st));
+  int launches = 0;
+  for (uint64_t s = 0; s < n_vec; s += kChunk) {
+    const uint32_t T = (uint32_t)std::min<uint64_t>(kChunk, n_vec - s);
+    uint32_t sp;
+    probe_tc_cand_per_token(T, n_centroid, n_sm, &sp);
+    CUDA_TRY(launch_probe_tc(d_vec + s * kDim, T, sw, d_centroid, n_centroid, 1, sp, cand,
+                             d_code + s, d_score ? d_score + s : score, err, st, &launches));
+  }
+  unsigned herr = 0;
+  CUDA_TRY(cudaMemcpyAsync(&herr, err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  if (herr) return set_err(MVR_ERR_CUDA, "tensor-core scoring gave up waiting (flags %u)", herr);
+  return MVR_OK;
+}
+
 int mvr_pack_residual_device(const float *d_vec, uint64_t n_vec, const float *d_centroid,
                              uint32_t dim, const uint32_t *d_code, const float *cutoff_l,
                              uint32_t n_bit, uint8_t *d_out, void *cuda_stream) {

@@ -29,7 +29,8 @@ EXPORTS = (
     "mvr_index_get_info", "mvr_index_set_batch", "mvr_index_set_rescore", "mvr_index_set_graphs",
     "mvr_search", "mvr_search_staged",
     "mvr_search_device", "mvr_search_trace", "mvr_decompress", "mvr_unpack_buckets",
-    "mvr_assign_device", "mvr_pack_residual_device", "mvr_kmeans_accumulate_device",
+    "mvr_assign_device", "mvr_assign_tc_device", "mvr_pack_residual_device",
+    "mvr_kmeans_accumulate_device",
     "mvr_filter_noalloc",
 )
 
@@ -104,6 +105,7 @@ def lib():
         "mvr_decompress": [vp, vp, u64, vp],
         "mvr_unpack_buckets": [vp, vp, u64, vp],
         "mvr_assign_device": [vp, u64, vp, u32, u32, vp, vp, vp],
+        "mvr_assign_tc_device": [vp, u64, vp, u32, u32, vp, vp, vp],
         "mvr_pack_residual_device": [vp, u64, vp, u32, vp, vp, u32, vp, vp],
         "mvr_kmeans_accumulate_device": [vp, u64, u32, vp, vp, vp, vp],
         "mvr_filter_noalloc": [vp, vp, vp, u32, u32, u32, vp, vp, vp, vp],

@@ -14,6 +14,8 @@ vq_sq_pack.vq_sq_ivf, script/evaluation/technique/vq_sq_pack.py:91-109):
  4. assignment of every token + residual packing (libmvr kernels);
  5. doc -> unique-centroid IVF lists, ascending doc ids (IVFIndex.hpp:92-166).
 Returns CUDA tensors; `to_host` gives numpy arrays for formats.write_index_dir.
+`build_index_stream` runs the same pipeline over a corpus generated (or read)
+one doc range at a time, with the tensor-core assignment by default.
 """
 import ctypes as C
 import math
@@ -49,6 +51,17 @@ def assign(vec, centroid, stream=None):
     return code, score
 
 
+def assign_tc(vec, centroid, stream=None):
+    """assign() on the tensor cores (mvr_assign_tc_device): BF16 candidates,
+    exact FP32 re-score; for builds over hundreds of millions of vectors."""
+    code = torch.empty(vec.shape[0], dtype=torch.int32, device=vec.device)
+    score = torch.empty(vec.shape[0], dtype=torch.float32, device=vec.device)
+    st = C.c_void_p(stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream)
+    check(lib().mvr_assign_tc_device(_p(vec), vec.shape[0], _p(centroid), centroid.shape[0],
+                                     centroid.shape[1], _p(code), _p(score), st))
+    return code, score
+
+
 def _ord_keys(x):
     b = x.contiguous().view(torch.int32).to(torch.int64)
     return torch.where(b < 0, -(b & 0x7FFFFFFF) - 1, b)  # signed-order of floats
@@ -81,7 +94,7 @@ def quantize_params(err_flat, n_bit):
     return np.asarray(cut, np.float32), np.asarray(w, np.float32)
 
 
-def kmeans(sample, n_centroid, n_iter=20, seed=123):
+def kmeans(sample, n_centroid, n_iter=20, seed=123, assign_fn=assign):
     dev = sample.device
     g = torch.Generator(device=dev).manual_seed(seed)
     idx = torch.randperm(sample.shape[0], device=dev, generator=g)[:n_centroid]
@@ -90,7 +103,7 @@ def kmeans(sample, n_centroid, n_iter=20, seed=123):
     cnt = torch.empty(n_centroid, dtype=torch.int64, device=dev)
     st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
     for _ in range(n_iter):
-        code, _ = assign(sample, cen)
+        code, _ = assign_fn(sample, cen)
         sums.zero_()
         cnt.zero_()
         check(lib().mvr_kmeans_accumulate_device(_p(sample), sample.shape[0], sample.shape[1],
@@ -115,33 +128,100 @@ def ivf_build(code, item_n_vec, n_centroid):
     return off, size, ids
 
 
-def build_index(tokens, item_n_vec, n_centroid, n_bit, kmeans_iter=20, seed=123):
+def _doc_offsets(item_n_vec):
+    off = np.zeros(len(item_n_vec) + 1, np.int64)
+    off[1:] = np.cumsum(np.asarray(item_n_vec, np.int64))
+    return off
+
+
+def train(sample, n_centroid, n_bit, kmeans_iter=20, seed=123, assign_fn=assign):
+    """Centroids, quantile cutoffs and bucket weights from the k-means sample."""
+    cen = kmeans(sample, n_centroid, kmeans_iter, seed, assign_fn)
+    s_code, _ = assign_fn(sample, cen)
+    err = (sample - cen[s_code.long()]).reshape(-1)
+    cutoff, weight = quantize_params(err, n_bit)
+    return cen, cutoff, weight
+
+
+def encode(tokens, cen, cutoff, n_bit, code_out, residual_out, assign_fn=assign):
+    """Codes and packed residuals of `tokens` into the given slices
+    (int32 [n], uint8 [n * 128 * n_bit / 8])."""
+    code, _ = assign_fn(tokens, cen)
+    code_out.copy_(code)
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    cut = np.ascontiguousarray(cutoff, np.float32)
+    check(lib().mvr_pack_residual_device(_p(tokens), tokens.shape[0], _p(cen), 128, _p(code_out),
+                                         C.c_void_p(cut.ctypes.data), n_bit, _p(residual_out), st))
+
+
+def _finish(item_n_vec, cen, code, weight, residual, cutoff, n_bit, n_centroid):
+    ivf_off, ivf_size, ivf_ids = ivf_build(code, item_n_vec, n_centroid)
+    dev = code.device
+    return dict(item_n_vec=torch.from_numpy(item_n_vec.view(np.int32)).to(dev),
+                centroid=cen, vq_code=code, weight=torch.from_numpy(weight).to(dev),
+                residual=residual, ivf_off=ivf_off, ivf_size=ivf_size, ivf_ids=ivf_ids,
+                cutoff=cutoff, n_bit=n_bit)
+
+
+def build_index(tokens, item_n_vec, n_centroid, n_bit, kmeans_iter=20, seed=123,
+                assign_fn=assign):
     """tokens: CUDA float32 [n_vec, 128]; item_n_vec: numpy uint32 [n_item]."""
     assert tokens.is_cuda and tokens.dtype == torch.float32 and tokens.shape[1] == 128
     item_n_vec = np.asarray(item_n_vec, np.uint32)
-    n_item = len(item_n_vec)
-    off = np.zeros(n_item + 1, np.int64)
-    off[1:] = np.cumsum(item_n_vec.astype(np.int64))
-    pids = np.asarray(sample_items(n_item), np.int64)
+    off = _doc_offsets(item_n_vec)
+    pids = np.asarray(sample_items(len(item_n_vec)), np.int64)
     tok_idx = np.concatenate([np.arange(off[p], off[p + 1]) for p in pids])
     sample = tokens[torch.from_numpy(tok_idx).to(tokens.device)].contiguous()
-    cen = kmeans(sample, n_centroid, kmeans_iter, seed)
-    s_code, _ = assign(sample, cen)
-    err = (sample - cen[s_code.long()]).reshape(-1)
-    cutoff, weight = quantize_params(err, n_bit)
-    del err, sample
-    code, _ = assign(tokens, cen)
+    cen, cutoff, weight = train(sample, n_centroid, n_bit, kmeans_iter, seed, assign_fn)
+    del sample
+    n = tokens.shape[0]
+    code = torch.empty(n, dtype=torch.int32, device=tokens.device)
+    residual = torch.empty(n * (128 * n_bit // 8), dtype=torch.uint8, device=tokens.device)
+    encode(tokens, cen, cutoff, n_bit, code, residual, assign_fn)
+    return _finish(item_n_vec, cen, code, weight, residual, cutoff, n_bit, n_centroid)
+
+
+def build_index_stream(spec, n_centroid, n_bit, kmeans_iter=20, seed=123, device="cuda",
+                       chunk_docs=1 << 17, assign_fn=assign_tc, tokens_fn=None):
+    """build_index over a corpus that is never resident as a whole: the
+    tokens of doc range [d0, d1) come from tokens_fn(spec, d0, d1, device)
+    (default: synth.tokens_range, the block-keyed synthetic stream), one
+    range of chunk_docs docs at a time -- once to gather the k-means sample,
+    once to encode.  Only the compressed index and the sample stay on the
+    device, so corpora of hundreds of millions of tokens fit.  With the same
+    tokens and assign_fn the result equals build_index's."""
+    from . import synth
+    if tokens_fn is None:
+        tokens_fn = synth.tokens_range
+    item_n_vec = np.asarray(spec.item_n_vec, np.uint32)
+    n_item = len(item_n_vec)
+    off = _doc_offsets(item_n_vec)
+    pids = np.asarray(sample_items(n_item), np.int64)
+    ranges = [(d0, min(n_item, d0 + chunk_docs)) for d0 in range(0, n_item, chunk_docs)]
+    parts = []
+    for d0, d1 in ranges:
+        p = pids[(pids >= d0) & (pids < d1)]
+        if len(p) == 0:
+            continue
+        tok = tokens_fn(spec, d0, d1, device)
+        idx = np.concatenate([np.arange(off[i], off[i + 1]) for i in p]) - off[d0]
+        parts.append(tok[torch.from_numpy(idx).to(tok.device)])
+        del tok
+    sample = torch.cat(parts).contiguous()
+    del parts
+    cen, cutoff, weight = train(sample, n_centroid, n_bit, kmeans_iter, seed, assign_fn)
+    del sample
+    torch.cuda.empty_cache()
+    n = int(off[-1])
     bpv = 128 * n_bit // 8
-    residual = torch.empty(tokens.shape[0] * bpv, dtype=torch.uint8, device=tokens.device)
-    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
-    cut = np.ascontiguousarray(cutoff, np.float32)
-    check(lib().mvr_pack_residual_device(_p(tokens), tokens.shape[0], _p(cen), 128, _p(code),
-                                         C.c_void_p(cut.ctypes.data), n_bit, _p(residual), st))
-    ivf_off, ivf_size, ivf_ids = ivf_build(code, item_n_vec, n_centroid)
-    return dict(item_n_vec=torch.from_numpy(item_n_vec.view(np.int32)).to(tokens.device),
-                centroid=cen, vq_code=code, weight=torch.from_numpy(weight).to(tokens.device),
-                residual=residual, ivf_off=ivf_off, ivf_size=ivf_size, ivf_ids=ivf_ids,
-                cutoff=cutoff, n_bit=n_bit)
+    code = torch.empty(n, dtype=torch.int32, device=device)
+    residual = torch.empty(n * bpv, dtype=torch.uint8, device=device)
+    for d0, d1 in ranges:
+        t0, t1 = int(off[d0]), int(off[d1])
+        tok = tokens_fn(spec, d0, d1, device)
+        encode(tok, cen, cutoff, n_bit, code[t0:t1], residual[t0 * bpv:t1 * bpv], assign_fn)
+        del tok
+    return _finish(item_n_vec, cen, code, weight, residual, cutoff, n_bit, n_centroid)
 
 
 def to_host(ix):

@@ -72,6 +72,67 @@ def tokens(spec, device="cpu", noise=0.45, chunk=1 << 22, out=None):
     return out
 
 
+BLOCK_DOCS = 1 << 15  # docs per generator block of the block-keyed token stream
+
+
+def n_vec_range(spec, d0, d1):
+    return int(spec.item_n_vec[d0:d1].sum(dtype=np.int64))
+
+
+def _block_tokens(spec, k, dev, noise):
+    """Tokens of doc block k (docs [k * BLOCK_DOCS, (k + 1) * BLOCK_DOCS)) from
+    the block's own generator."""
+    d0 = k * BLOCK_DOCS
+    d1 = min(spec.n_doc, d0 + BLOCK_DOCS)
+    gen = torch.Generator(device=dev).manual_seed(spec.seed * 1000003 + 104729 * (k + 1))
+    lens = torch.from_numpy(spec.item_n_vec[d0:d1].astype(np.int64)).to(dev)
+    doc_of = torch.repeat_interleave(torch.arange(d1 - d0, device=dev), lens)
+    n = doc_of.shape[0]
+    doc_k = torch.from_numpy(spec.doc_k[d0:d1]).to(dev)
+    clusters = torch.from_numpy(spec.doc_clusters[d0:d1]).to(dev)
+    k_max = spec.doc_clusters.shape[1] - 1
+    slot = (torch.rand(n, device=dev, generator=gen) * doc_k[doc_of]).long().clamp_max_(k_max)
+    latent = torch.from_numpy(spec.latent).to(dev)
+    x = latent[clusters[doc_of, slot]]
+    x += (noise / math.sqrt(DIM)) * torch.randn((n, DIM), device=dev, generator=gen)
+    return _normalize_(x)
+
+
+def tokens_range(spec, d0, d1, device="cpu", noise=0.45):
+    """Tokens of docs [d0, d1), float32 [n_vec_range(spec, d0, d1), 128], from
+    the block-keyed stream: every block of BLOCK_DOCS docs draws from its own
+    generator, so any doc range is generated without the docs before it and
+    corpora far larger than device memory can be built and scanned in
+    pieces.  (A different stream from `tokens`, which draws the whole corpus
+    from one generator; same distribution.)"""
+    dev = torch.device(device)
+    parts = []
+    k_end = (d1 + BLOCK_DOCS - 1) // BLOCK_DOCS if d1 > d0 else 0
+    for k in range(d0 // BLOCK_DOCS, k_end):
+        b0 = k * BLOCK_DOCS
+        x = _block_tokens(spec, k, dev, noise)
+        s = n_vec_range(spec, b0, max(d0, b0))
+        e = n_vec_range(spec, b0, min(d1, b0 + BLOCK_DOCS))
+        parts.append(x[s:e])
+    if not parts:
+        return torch.empty((0, DIM), dtype=torch.float32, device=dev)
+    return parts[0] if len(parts) == 1 else torch.cat(parts)
+
+
+def doc_chunks(spec, max_tokens):
+    """[d0, d1) ranges covering the corpus, each <= max_tokens tokens (one
+    doc may exceed it alone)."""
+    off = np.zeros(spec.n_doc + 1, np.int64)
+    off[1:] = np.cumsum(spec.item_n_vec, dtype=np.int64)
+    out, d0 = [], 0
+    while d0 < spec.n_doc:
+        d1 = int(np.searchsorted(off, off[d0] + max_tokens, side="right")) - 1
+        d1 = min(spec.n_doc, max(d1, d0 + 1))
+        out.append((d0, d1))
+        d0 = d1
+    return out
+
+
 def queries(spec, n_query, n_tok=32, device="cpu", noise=0.55, seed=1):
     """Queries built from random docs' clusters.  n_tok: int; a tuple (lo, hi)
     for ragged queries (token counts uniform in [lo, hi]); or a list of token

@@ -196,6 +196,50 @@ def test_gpu_builder_matches_oracle_codec():
     torch.cuda.empty_cache()
 
 
+def test_streaming_builder_and_tensor_core_assignment():
+    """build_index_stream generates and encodes the corpus one doc range at a
+    time (ranges not aligned with the generator's blocks); with the same
+    tokens and the FP32 assignment it equals build_index over the resident
+    corpus, array for array.  The tensor-core assignment
+    (mvr_assign_tc_device) returns the FP32 argmax for nearly every vector
+    and the exact FP32 score wherever the codes agree; an index streamed with
+    it searches bit-exactly like the oracle on the same arrays."""
+    import torch
+    from mvr import build, synth
+    old = synth.BLOCK_DOCS
+    synth.BLOCK_DOCS = 1000
+    try:
+        spec = synth.CorpusSpec(5000, seed=5, n_latent=400)
+        tok = synth.tokens_range(spec, 0, spec.n_doc, "cuda")
+        a = build.build_index(tok, spec.item_n_vec, 256, 2, kmeans_iter=2)
+        b = build.build_index_stream(spec, 256, 2, kmeans_iter=2, chunk_docs=1500,
+                                     assign_fn=build.assign)
+        for key in ("centroid", "vq_code", "weight", "residual", "ivf_off", "ivf_size", "ivf_ids"):
+            assert torch.equal(a[key], b[key]), key
+        np.testing.assert_array_equal(a["cutoff"], b["cutoff"])
+        c32, s32 = build.assign(tok, a["centroid"])
+        ctc, stc = build.assign_tc(tok, a["centroid"])
+        agree = c32 == ctc
+        assert agree.float().mean().item() > 0.999
+        assert torch.equal(s32[agree], stc[agree])
+        assert bool((stc[~agree] <= s32[~agree]).all())
+        del tok
+        c = build.build_index_stream(spec, 256, 2, kmeans_iter=2, chunk_docs=1500)
+        g, h = build.load_built(c), build.to_host(c)
+        o = pyoracle.Oracle(h["item_n_vec"], h["centroid"], h["vq_code"], h["residual"],
+                            h["weight"], h["ivf_off"], h["ivf_size"], h["ivf_ids"], 2)
+        q, off = synth.queries(spec, 6, 32, "cpu", seed=4)
+        q = q.numpy()
+        s, i = g.search(q.reshape(6, 32, 128), 10, 4, 150)
+        rs, ri = o.search(q, off, 10, 4, 150)
+        np.testing.assert_array_equal(i, ri)
+        np.testing.assert_array_equal(s, rs)
+        g.close()
+    finally:
+        synth.BLOCK_DOCS = old
+        torch.cuda.empty_cache()
+
+
 def test_config1_scale_gpu_built_index_bit_exact():
     """10,000 docs / 8,192 centroids / nbits 2 (the small synthetic config),
     built on the GPU; 16 queries x (nprobe 4, k 10 and 100) vs the oracle."""

@@ -63,3 +63,47 @@ def test_exhaustive_topk_matches_oracle_f64():
     rs, ri = pyoracle.exhaustive_f64(q.numpy(), off, ix["tokens"], ix["item_n_vec"], 7)
     np.testing.assert_array_equal(i, ri)
     np.testing.assert_allclose(s, rs, rtol=1e-12)
+
+
+def test_block_keyed_tokens_any_range():
+    """tokens_range: any doc range equals the matching slice of the whole
+    corpus (each block of docs has its own generator), across block edges."""
+    old = synth.BLOCK_DOCS
+    synth.BLOCK_DOCS = 500
+    try:
+        spec = synth.CorpusSpec(1700, seed=6, n_latent=300)
+        full = synth.tokens_range(spec, 0, spec.n_doc)
+        assert full.shape == (spec.n_vec, 128)
+        assert torch.allclose(torch.linalg.vector_norm(full, dim=1), torch.ones(spec.n_vec))
+        for d0, d1 in ((0, 1), (499, 501), (500, 1000), (1234, 1700), (1699, 1700), (7, 7)):
+            t0, t1 = synth.n_vec_range(spec, 0, d0), synth.n_vec_range(spec, 0, d1)
+            assert torch.equal(synth.tokens_range(spec, d0, d1), full[t0:t1])
+        ch = synth.doc_chunks(spec, 10_000)
+        assert ch[0][0] == 0 and ch[-1][1] == spec.n_doc
+        assert all(a[1] == b[0] for a, b in zip(ch, ch[1:]))
+        assert all(synth.n_vec_range(spec, a, b) <= 10_000 for a, b in ch)
+    finally:
+        synth.BLOCK_DOCS = old
+
+
+def test_exhaustive_stream_equals_whole_corpus():
+    """exhaustive_topk_stream over doc pieces (the way corpora larger than the
+    device are scanned) gives the whole-corpus top-k, ties by lower id."""
+    ix = tiny_index(n_doc=300, n_centroid=16, seed=8)
+    q, off = synth.queries(ix["spec"], 4, (3, 20), "cpu", seed=2)
+    tok = torch.from_numpy(ix["tokens"])
+    lens = ix["item_n_vec"].astype(np.int64)
+    s, i = exhaustive.exhaustive_topk(q, off, tok, ix["item_n_vec"], 9)
+    toff = np.concatenate([[0], np.cumsum(lens)])
+    for cut in ((0, 300), (0, 1, 150, 151, 300), (0, 97, 203, 300)):
+        chunks = ((a, lens[a:b], tok[toff[a]:toff[b]]) for a, b in zip(cut, cut[1:]))
+        s2, i2 = exhaustive.exhaustive_topk_stream(q, off, chunks, 9)
+        np.testing.assert_array_equal(i2, i)
+        np.testing.assert_allclose(s2, s, rtol=1e-12)
+    # duplicated docs: equal scores keep the lower id across pieces
+    dup = torch.cat([tok[toff[5]:toff[6]], tok[toff[5]:toff[6]]])
+    l2 = np.array([lens[5], lens[5]])
+    _, idup = exhaustive.exhaustive_topk_stream(q, off, [(0, l2[:1], dup[:lens[5]]),
+                                                         (1, l2[1:], dup[lens[5]:])], 2)
+    assert (idup == np.array([0, 1])).all()
+
