@@ -1,17 +1,22 @@
-// ref_shim.cpp -- binds the reference's own codec and IVF code, compiled from
-// its unmodified headers where they lie (see oracle/Makefile, target `ref`),
+// ref_shim.cpp -- binds the reference's own codec, IVF and MaxSim code,
+// compiled from its unmodified headers where they lie (see oracle/Makefile,
+// target `ref`),
 // into a Python module used only to pin the oracle and to generate the golden
 // fixtures under tests/golden/.  This file adds no arithmetic of its own: every
 // result below is produced by reference code.
 #include <pybind11/pybind11.h>
 #include <pybind11/numpy.h>
 #include <pybind11/stl.h>
+#include <algorithm>
 #include <cstring>
+#include <limits>
+#include <memory>
 #include <vector>
 
 #include "include/struct/TypeDef.hpp"
 #include "include/alg/refine/ResidualScalarQuantizationPack.hpp"
 #include "include/struct/IVFIndex.hpp"
+#include "include/alg/Distance.hpp"
 
 namespace py = pybind11;
 using namespace VectorSetSearch;
@@ -63,6 +68,13 @@ static py::tuple ivf_build(const std::vector<uint32_t> &code,
   return py::make_tuple(ivf.ivf_offset_l_, ivf.ivf_size_l_, ivf.ivf_);
 }
 
+// Distance.hpp's vectorSetDistance (sum over query vectors of the max inner
+// product over the item's vectors) of one query set and one item set.
+static float vector_set_distance(const pyarray_float &query, const pyarray_float &item) {
+  return vectorSetDistance(query.data(), (uint32_t)query.shape(0), item.data(),
+                           (uint32_t)item.shape(0), (uint32_t)query.shape(1));
+}
+
 PYBIND11_MODULE(mvr_ref, m) {
   m.def("compute_quantized_scalar", &ComputeQuantizedScalarPack,
         py::arg("item_vec_l"), py::arg("centroid_l"), py::arg("code_l"), py::arg("n_bit"));
@@ -75,4 +87,5 @@ PYBIND11_MODULE(mvr_ref, m) {
   m.def("decode_table", &decode_table);
   m.def("ivf_build", &ivf_build);
   m.def("read_ivf_index", &Method::readIVFIndex);
+  m.def("vector_set_distance", &vector_set_distance, py::arg("query"), py::arg("item"));
 }

@@ -2,13 +2,16 @@
 
 Runs only where the reference sources exist: it imports the module that
 oracle/Makefile (target `ref`) compiles from the reference's unmodified
-ResidualScalarQuantizationPack.hpp and IVFIndex.hpp.  The fixtures freeze, per
-case, the reference's quantile cutoffs/weights, packed residual codes, decode
-table, decoded vectors, IVF lists and ivf.index bytes for seeded synthetic
-inputs, so that the oracle and the CUDA path can be checked against the
-reference where the reference itself cannot travel.
+ResidualScalarQuantizationPack.hpp, IVFIndex.hpp and Distance.hpp.  The codec
+fixtures freeze, per case, the reference's quantile cutoffs/weights, packed
+residual codes, decode table, decoded vectors, IVF lists and ivf.index bytes
+for seeded synthetic inputs; the MaxSim fixtures freeze the reference's
+vectorSetDistance of seeded query sets against every item, over the decoded
+vectors (the rerank's MaxSim) and over the raw vectors (the exhaustive
+ground truth's).  The oracle and the CUDA path are checked against them where
+the reference itself cannot travel.
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref && python tests/golden/make_golden.py [codec|maxsim]
 """
 import glob
 import os
@@ -48,10 +51,41 @@ def make_inputs(n_bit, dim, n_item, max_len, n_centroid, seed, coarse):
     return item_n_vec, vec, cen, code
 
 
+def make_maxsim(mvr_ref):
+    """maxsim_<case>.npz: 3 seeded query sets (32 vectors at dim 128, 8 at
+    dim 36) and the reference's vectorSetDistance of each against every item's
+    decoded vectors and raw vectors of the codec case."""
+    for name, n_bit, dim, n_item, max_len, n_cent, seed, coarse in CASES:
+        z = np.load(os.path.join(HERE, f"codec_{name}.npz"))
+        rng = np.random.default_rng(seed + 1000)
+        nq = 32 if dim == 128 else 8
+        q = rng.standard_normal((3, nq, dim)).astype(np.float32)
+        q /= np.linalg.norm(q, axis=2, keepdims=True)
+        q = q.astype(np.float32)
+        off = np.concatenate([[0], np.cumsum(z["item_n_vec"].astype(np.int64))])
+        dec, raw = z["decoded"], z["vec"]
+        ms_dec = np.array([[mvr_ref.vector_set_distance(q[i], dec[off[j]:off[j + 1]])
+                            for j in range(n_item)] for i in range(3)], np.float32)
+        ms_raw = np.array([[mvr_ref.vector_set_distance(q[i], raw[off[j]:off[j + 1]])
+                            for j in range(n_item)] for i in range(3)], np.float32)
+        np.savez_compressed(os.path.join(HERE, f"maxsim_{name}.npz"), query=q,
+                            maxsim_decoded=ms_dec, maxsim_raw=ms_raw)
+        print(name, "maxsim", ms_dec[0, :4])
+
+
 def main():
     sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))
     import mvr_ref  # noqa: E402  (reference code, compiled from its sources)
 
+    what = sys.argv[1] if len(sys.argv) > 1 else "all"
+    if what in ("all", "codec"):
+        make_codec(mvr_ref)
+    if what in ("all", "maxsim"):
+        make_maxsim(mvr_ref)
+    print("fixtures:", sorted(os.path.basename(p) for p in glob.glob(os.path.join(HERE, "*.npz"))))
+
+
+def make_codec(mvr_ref):
     for name, n_bit, dim, n_item, max_len, n_cent, seed, coarse in CASES:
         item_n_vec, vec, cen, code = make_inputs(n_bit, dim, n_item, max_len, n_cent,
                                                  seed, coarse)
@@ -77,7 +111,6 @@ def main():
             ivf_size=np.asarray(size, np.uint32), ivf_ids=np.asarray(ids, np.uint32),
             ivf_bytes=ivf_bytes)
         print(name, "n_vec", len(code), "cutoff", cutoff, "weight", weight)
-    print("fixtures:", sorted(os.path.basename(p) for p in glob.glob(os.path.join(HERE, "*.npz"))))
 
 
 if __name__ == "__main__":
