@@ -225,7 +225,7 @@ namespace {
 
 // Queries per device batch: 8 per SM (1,184 on B200) -- large batches fill
 // the tensor-core probe's token tiles and the re-score's CTAs; the hash
-// filter's key space is kHashKeys * 8 B = 459 KB per query.
+// filter's key space is kHashKeys * 8 B = 917 KB per query.
 uint32_t default_batch(const mvr_index *h) { return 8u * (uint32_t)h->n_sm; }
 
 // Slots of the rank-table fallback (n_item * (4 + 32|64 + 8) bytes each,

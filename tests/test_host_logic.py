@@ -107,3 +107,32 @@ def test_exhaustive_stream_equals_whole_corpus():
                                                          (1, l2[1:], dup[lens[5]:])], 2)
     assert (idup == np.array([0, 1])).all()
 
+
+
+def test_bench_ground_truth_pieces_cover_the_corpus():
+    """bench.gt_chunks: consecutive doc pieces, each within its generator
+    block and the score-matrix budget, whose tokens are the corpus's."""
+    import importlib.util
+    import os
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    spec_b = importlib.util.spec_from_file_location("bench_mod", os.path.join(root, "bench.py"))
+    bench = importlib.util.module_from_spec(spec_b)
+    spec_b.loader.exec_module(bench)
+    old = synth.BLOCK_DOCS
+    synth.BLOCK_DOCS = 400
+    try:
+        spec = synth.CorpusSpec(1000, seed=2, n_latent=100)
+        full = synth.tokens_range(spec, 0, spec.n_doc)
+        pieces = list(bench.gt_chunks(spec, lambda a, b: synth.tokens_range(spec, a, b),
+                                      n_q_tok=2_000_000))  # budget -> 16,384-token floor
+        d, t = 0, 0
+        for d0, lens, x in pieces:
+            assert d0 == d and x.shape[0] == int(lens.sum())
+            assert d0 // 400 == (d0 + len(lens) - 1) // 400      # within one block
+            assert x.shape[0] <= 16_384 or len(lens) == 1
+            assert torch.equal(x, full[t:t + x.shape[0]])
+            d += len(lens)
+            t += x.shape[0]
+        assert d == spec.n_doc and t == spec.n_vec
+    finally:
+        synth.BLOCK_DOCS = old
