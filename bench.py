@@ -360,6 +360,9 @@ def main():
                     help="residual code width of the profiling case")
     ap.add_argument("--no-tune", action="store_true",
                     help="skip the shortlist tuner (it only reports unless --use-tuned)")
+    ap.add_argument("--tune-batch", action="store_true",
+                    help="also time the headline search at several queries-per-batch sizes "
+                         "(with --use-tuned, run at the fastest)")
     ap.add_argument("--use-tuned", action="store_true",
                     help="time this run's tuned shortlist sizes instead of the workload's")
     ap.add_argument("--target", type=float, default=0.99,
@@ -479,6 +482,13 @@ def main():
                                             round(x["ms"], 3)) for x in t["table"]])
                 if args.use_tuned:
                     ptk[fl] = t["probe_topk"]
+            if args.tune_batch:  # queries per device batch of the headline path (all queries)
+                qh = q.cpu().numpy() if ragged else q.cpu().numpy().reshape(n_query, w["n_tok"], 128)
+                tb = tune.tune_batch(g, qh, k, nprobe, ptk[FAST], FAST,
+                                     tok_off=off if ragged else None)
+                tuning["batch"] = dict(batch=tb["batch"], table=[(x["batch"], round(x["ms"], 3))
+                                                                 for x in tb["table"]])
+                g.set_batch(tb["batch"] if args.use_tuned else (args.batch or w.get("batch", 0)))
         for name, fl in (("fast", FAST), ("plain", PLAIN)):
             step(fl)
             est = out_i[:n_gt].cpu().numpy().view(np.uint32)

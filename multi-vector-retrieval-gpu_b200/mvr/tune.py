@@ -50,3 +50,30 @@ def tune(index, queries, gnd_ids, k, nprobe, target, semantics,
     pick = (min(ok, key=lambda t: (t["probe_topk"], t["rescore"])) if ok
             else max(table, key=lambda t: (t["recall"], -t["probe_topk"])))
     return dict(pick, table=table, reached=bool(ok))
+
+
+def tune_batch(index, queries, k, nprobe, probe_topk, semantics,
+               batches=(296, 592, 1184, 2368, 4096), repeats=3, tok_off=None):
+    """Queries per device batch: every candidate size is set on the index
+    (set_batch) and the same search timed (best device time of `repeats`);
+    returns dict(batch, ms, qps, table) for the fastest, then restores the
+    library default (set_batch(0)).  Results do not depend on the batch
+    size, only the time does (larger batches fill the tensor-core tiles and
+    amortise launches; smaller ones shorten each batch's latency)."""
+    n_query = len(tok_off) - 1 if tok_off is not None else len(queries)
+    table = []
+    for b in batches:
+        index.set_batch(b)
+        best = None
+        for _ in range(repeats):
+            if tok_off is None:
+                st = index.search(queries, k, nprobe, probe_topk, semantics=semantics,
+                                  with_stats=True)[2]
+            else:
+                st = index.search(queries, k, nprobe, probe_topk, tok_off=tok_off,
+                                  semantics=semantics, with_stats=True)[2]
+            best = st["device_ms"] if best is None else min(best, st["device_ms"])
+        table.append(dict(batch=b, ms=best, qps=n_query / (best / 1e3) if best else None))
+    index.set_batch(0)
+    pick = min(table, key=lambda t: (t["ms"], t["batch"]))
+    return dict(pick, table=table)

@@ -42,3 +42,25 @@ def test_most_accurate_when_target_unreachable():
                   probe_topks=(5, 100, 600, 800), repeats=1)
     assert not t["reached"] and t["probe_topk"] == 600 and t["recall"] == 0.5
     assert 5 not in [x["probe_topk"] for x in t["table"]]  # below k: skipped
+
+
+def test_batch_tuner_picks_the_fastest_and_restores_the_default():
+    class BatchIndex:
+        def __init__(self):
+            self.batch, self.sets = 0, []
+
+        def set_batch(self, b):
+            self.batch = b
+            self.sets.append(b)
+
+        def search(self, queries, k, nprobe, probe_topk, semantics=0, with_stats=False,
+                   tok_off=None):
+            ms = {296: 9.0, 592: 7.0, 1184: 5.0, 2368: 5.0, 4096: 6.0}[self.batch]
+            return None, None, dict(device_ms=ms)
+
+    idx = BatchIndex()
+    t = tune.tune_batch(idx, np.zeros((100, 32, 128), np.float32), 10, 8, 1500, 4, repeats=2)
+    assert t["batch"] == 1184 and t["ms"] == 5.0 and abs(t["qps"] - 100 / 5e-3) < 1e-6
+    assert [x["batch"] for x in t["table"]] == [296, 592, 1184, 2368, 4096]
+    assert idx.sets[-1] == 0
+
