@@ -236,6 +236,37 @@ def cpu_port_qps(host, q_np, off, w, n_threads, probe_topk, budget_s=15.0):
     return n / dt, n, dt, o
 
 
+def plaid_cpu_baseline(host, q_np, off, k, n_threads, gi_eval, gi_raw, budget_s=10.0):
+    """The reference's own PLAID CPU search (its compiled extensions, oracle/
+    plaid_cpu.py) over this index re-laid in PLAID's layout, at PLAID's
+    defaults for k, on a bounded sample of the workload's queries; recall@k
+    on the first len(gi_eval) queries."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import plaid_cpu
+    if not plaid_cpu.available():
+        return {"value": None, "sample": "not run: reference PLAID extensions not built"}
+    p = plaid_cpu.PlaidCPU(host["item_n_vec"], host["centroid"], host["vq_code"],
+                           host["residual"], host["weight"], host["ivf_off"], host["ivf_size"],
+                           host["ivf_ids"], host["n_bit"], n_threads=n_threads)
+    n_q = len(off) - 1
+    est, t, n = [], time.perf_counter(), 0
+    while n < n_q and (n < len(gi_eval) or time.perf_counter() - t < budget_s):
+        est.append(p.search_one(q_np[off[n]:off[n + 1]], k)[0])
+        n += 1
+    dt = time.perf_counter() - t
+    m = min(len(gi_eval), len(est))
+    return {"value": n / dt, "unit": "queries/s", "cores": n_threads, "kind": "reference",
+            "sample": f"first {n} of the {n_q} queries ({dt:.1f} s)",
+            "params": plaid_cpu.defaults(k),
+            "recall@10": float(formats_recall(gi_eval[:m], est[:m], k)),
+            "recall@10_vs_raw": float(formats_recall(gi_raw[:m], est[:m], k))}
+
+
+def formats_recall(gnd, est, k):
+    from mvr import formats
+    return formats.recall_at_k(gnd, est, k).mean()
+
+
 def run_reference(args, w):
     import torch
     rank = int(os.environ.get("RANK", "0"))
@@ -353,6 +384,9 @@ def main():
     ap.add_argument("--precision", choices=["bf16", "fp8"], default="fp8",
                     help="tensor-core MaxSim precision of the headline path")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plaid-baseline", action="store_true",
+                    help="also time the reference's PLAID CPU search (its compiled extensions) "
+                         "on this index, with its recall")
     ap.add_argument("--profile-case", action="store_true",
                     help="small profiling target instead of the bench: 200,000 docs, 16,384 "
                          "centroids, one mixed-precision and one plain search of 296 queries")
@@ -623,6 +657,9 @@ def main():
         qps_cpu, n_s, dt_s, _ = cpu_port_qps(host, hq.numpy(), off, w, os.cpu_count(), ptk[PLAIN])
         cpu = {"value": qps_cpu, "unit": "queries/s", "cores": os.cpu_count(), "kind": "port",
                "sample": f"first {n_s} of the {n_query} queries ({dt_s:.1f} s)"}
+    plaid = None
+    if args.plaid_baseline and not streamed and world == 1:
+        plaid = plaid_cpu_baseline(host, hq.numpy(), off, k, os.cpu_count(), gi_eval, gi_raw)
 
     R = args.rescore or 4 * k
     line = {
@@ -660,6 +697,7 @@ def main():
                 "h2d_bytes_per_step": int(st_e.h2d_bytes), "d2h_bytes_per_step": int(st_e.d2h_bytes)},
         "roofline": roof,
         "cpu_baseline": cpu,
+        **({"cpu_baseline_plaid": plaid} if plaid is not None else {}),
         "clocks": clk.summary(),
         "gpu_launches": int(fast["launches"]),
         "p99_ms": p99,

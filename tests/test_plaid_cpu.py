@@ -53,3 +53,21 @@ def test_plaid_search_ranks_by_normalized_maxsim():
             x /= np.linalg.norm(x, axis=1, keepdims=True)
             ref = (qi.astype(np.float64) @ x.T).max(1).sum()
             assert abs(s - ref) < 1e-4 * max(1.0, abs(ref))
+
+
+def test_bench_plaid_baseline_line():
+    """bench.py --plaid-baseline: the reported object (QPS on a bounded sample,
+    recall against the given ground truths)."""
+    import importlib.util
+    import os
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sb = importlib.util.spec_from_file_location("bench_mod2", os.path.join(root, "bench.py"))
+    bench = importlib.util.module_from_spec(sb)
+    sb.loader.exec_module(bench)
+    ix = tiny_index(n_doc=300, n_centroid=48, n_bit=2, seed=71)
+    q, off = make_queries(ix, 6, 32, seed=72)
+    o = oracle_of(ix)
+    _, gt = o.search(q, off, 10, 48, 300)  # every list probed: the exact top-10
+    r = bench.plaid_cpu_baseline(dict(ix), q, off, 10, 2, gt, gt, budget_s=0.5)
+    assert r["kind"] == "reference" and r["value"] > 0 and 0.0 <= r["recall@10"] <= 1.0
+    assert r["params"] == {"ncells": 1, "centroid_score_threshold": 0.5, "ndocs": 256}
