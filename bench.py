@@ -37,7 +37,9 @@ sys.path.insert(0, os.path.join(ROOT, "multi-vector-retrieval-gpu_b200"))
 METRIC = ("QPS & p99 ms at recall@10>=0.99 vs exact MaxSim: learned+BF16/FP8 vs plain, "
           "1 B200")
 CACHE_VERSION = "mvr-index-v1"
-RERANK_DRAM_BYTES_PER_TOKEN = 33.2  # ncu: dram__bytes_read+write of rerank_tmem_kernel (FP8) / token
+# ncu: dram__bytes_read + dram__bytes_write of rerank_tmem_kernel (FP8) per
+# reranked token on the 200,000-doc profiling case (--profile-case), by nbits
+RERANK_DRAM_BYTES_PER_TOKEN = {2: 33.2, 4: 65.2}
 
 WORKLOADS = {
     # medium: 1M docs, 65,536 centroids, nbits 2, 10,000 queries (the headline workload)
@@ -630,12 +632,11 @@ def main():
     name, bound, work, peak, unit = kern[dom]
     achieved = work / (stage[dom] / 1e3)
     names = ("query_copy", "probe", "filter", "rerank", "rescore_topk", "result_copy")
-    # DRAM bytes per reranked token of the FP8 rerank kernel on 2-bit codes,
-    # measured by ncu on the 200,000-doc profiling case
-    # (profiles/ncu_profile_case_fp8.md), scaled to a launch of this workload
+    # DRAM bytes per reranked token of the FP8 rerank kernel, measured by ncu
+    # on the 200,000-doc profiling case, scaled to a launch of this workload
     # by its reranked tokens
-    traffic = (RERANK_DRAM_BYTES_PER_TOKEN * tok_launch
-               if (dom == 3 and fp8_ran and w["n_bit"] == 2) else None)
+    per_tok = RERANK_DRAM_BYTES_PER_TOKEN.get(w["n_bit"])
+    traffic = per_tok * tok_launch if (dom == 3 and fp8_ran and per_tok) else None
     roof = {"kernel": name, "bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
             "frac": achieved / peak, "traffic": traffic,
             "algorithmic_bytes_per_launch": rerank_bytes / n_launch if dom == 3 else None,
