@@ -52,3 +52,44 @@ def test_recall_metric():
     gnd = [np.array([1, 2, 3]), np.array([4, 5, 6])]
     est = [np.array([3, 2, 9]), np.array([7, 8, 9])]
     np.testing.assert_allclose(formats.recall_at_k(gnd, est, 3), [2 / 3, 0.0])
+
+
+def test_plaid_igp_conversion_round_trip_and_chunks(tmp_path):
+    """mvr.convert: IGP dir -> PLAID dir -> IGP dir keeps codes, residual
+    bytes and lists exactly (centroids and weights pass through fp16); a
+    PLAID directory split into two chunks reads back the same."""
+    import json
+    import torch
+    from mvr import convert, formats
+    from helpers import tiny_index
+    ix = tiny_index(n_doc=120, n_centroid=16, n_bit=4, seed=9)
+    a, p, b = tmp_path / "igp", tmp_path / "plaid", tmp_path / "igp2"
+    formats.write_index_dir(str(a), ix["item_n_vec"], ix["centroid"], ix["vq_code"],
+                            ix["weight"], ix["residual"], ix["ivf_off"], ix["ivf_size"],
+                            ix["ivf_ids"])
+    assert convert.main(["igp2plaid", str(a), str(p), "4"]) == 0
+    assert convert.main(["plaid2igp", str(p), str(b)]) == 0
+    x, y = formats.read_index_dir(str(a)), formats.read_index_dir(str(b))
+    for k in ("item_n_vec", "vq_code", "residual", "ivf_off", "ivf_size", "ivf_ids"):
+        np.testing.assert_array_equal(x[k], y[k], err_msg=k)
+    np.testing.assert_array_equal(y["centroid"], x["centroid"].astype(np.float16).astype(np.float32))
+    np.testing.assert_array_equal(y["weight"], x["weight"].astype(np.float16).astype(np.float32))
+    # two chunks: docs [0, 50) and [50, 120)
+    one = formats.read_plaid_index(str(p))
+    n0 = int(ix["item_n_vec"][:50].sum())
+    codes = torch.load(p / "0.codes.pt")
+    res = torch.load(p / "0.residuals.pt")
+    dl = json.load(open(p / "doclens.0.json"))
+    torch.save(codes[:n0].clone(), p / "0.codes.pt")
+    torch.save(res[:n0].clone(), p / "0.residuals.pt")
+    json.dump(dl[:50], open(p / "doclens.0.json", "w"))
+    torch.save(codes[n0:].clone(), p / "1.codes.pt")
+    torch.save(res[n0:].clone(), p / "1.residuals.pt")
+    json.dump(dl[50:], open(p / "doclens.1.json", "w"))
+    meta = json.load(open(p / "metadata.json"))
+    meta["num_chunks"] = 2
+    json.dump(meta, open(p / "metadata.json", "w"))
+    two = formats.read_plaid_index(str(p))
+    for k, v in one.items():
+        np.testing.assert_array_equal(np.asarray(two[k]), np.asarray(v), err_msg=k)
+    assert convert.main(["bogus"]) == 2
