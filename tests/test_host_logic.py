@@ -136,3 +136,20 @@ def test_bench_ground_truth_pieces_cover_the_corpus():
         assert d == spec.n_doc and t == spec.n_vec
     finally:
         synth.BLOCK_DOCS = old
+
+
+def test_bench_reference_arm_declines_streamed_workloads():
+    """bench.py --impl reference on a streamed workload prints its
+    `unavailable` line (the CPU port needs the whole index in host memory)
+    without touching a GPU."""
+    import json
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    for wl in ("large", "xl"):
+        out = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl",
+                              "reference", "--workload", wl], capture_output=True, text=True,
+                             timeout=120, check=True).stdout.strip().splitlines()[-1]
+        line = json.loads(out)
+        assert line["impl"] == "reference" and "unavailable" in line
