@@ -74,6 +74,17 @@ class Index:
         return cls(h)
 
     @classmethod
+    def from_plaid_dir(cls, path, device=0):
+        """A PLAID index directory (the reference's ColBERT baseline) loaded
+        as an IGP index: its centroids, codes, bucket weights and IVF lists,
+        residual bits re-laid (formats.read_plaid_index)."""
+        from . import formats
+        ix = formats.read_plaid_index(path)
+        return cls.from_arrays(ix["item_n_vec"], ix["centroid"], ix["vq_code"], ix["ivf_off"],
+                               ix["ivf_size"], ix["ivf_ids"], ix["weight"], ix["n_bit"],
+                               ix["residual"], device=device)
+
+    @classmethod
     def from_device_arrays(cls, item_n_vec, centroid, vq_code, ivf_off, ivf_size, ivf_ids, weight,
                            n_bit, residual, device=0):
         """Arguments are CUDA tensors (uint32 as int32 storage is accepted)."""

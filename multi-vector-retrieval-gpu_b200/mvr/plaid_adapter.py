@@ -15,8 +15,6 @@ un-normalized decoded vectors, not PLAID's normalized ones.
 """
 import numpy as np
 
-from . import formats
-
 # PLAID's defaults by k (searcher.py:291-312)
 _DEFAULTS = ((10, (1, 0.5, 256)), (100, (2, 0.45, 1024)))
 
@@ -67,10 +65,7 @@ class Searcher:
         self.config = SearchConfig()
         if engine is None:
             from .index import Index
-            ix = formats.read_plaid_index(index)
-            engine = Index.from_arrays(ix["item_n_vec"], ix["centroid"], ix["vq_code"],
-                                       ix["ivf_off"], ix["ivf_size"], ix["ivf_ids"], ix["weight"],
-                                       ix["n_bit"], ix["residual"], device=device)
+            engine = Index.from_plaid_dir(index, device=device)
         self.engine = engine
 
     def configure(self, **kw):
