@@ -53,8 +53,8 @@ def main():
     cen = sample[rng.choice(len(sample), a.n_centroid, replace=False)].copy()
     for _ in range(a.kmeans_iter):
         c = pyoracle.assign(sample, cen).astype(np.int64)
-        sums = np.zeros((a.n_centroid, sample.shape[1]))
-        np.add.at(sums, c, sample)
+        sums = np.stack([np.bincount(c, weights=sample[:, d], minlength=a.n_centroid)
+                         for d in range(sample.shape[1])], axis=1)
         nz = np.bincount(c, minlength=a.n_centroid) > 0
         cen[nz] = (sums[nz] / np.linalg.norm(sums[nz], axis=1, keepdims=True)).astype(np.float32)
     code = pyoracle.assign(tok, cen)
