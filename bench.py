@@ -396,6 +396,9 @@ def main():
                     help="residual code width of the profiling case")
     ap.add_argument("--no-tune", action="store_true",
                     help="skip the shortlist tuner (it only reports unless --use-tuned)")
+    ap.add_argument("--gt-dtype", choices=["f64", "f32"], default="f64",
+                    help="streamed workloads: arithmetic of the exhaustive ground truths "
+                         "(f32 adds an FP64 spot check of 8 queries)")
     ap.add_argument("--tune-batch", action="store_true",
                     help="also time the headline search at several queries-per-batch sizes "
                          "(with --use-tuned, run at the fastest)")
@@ -484,16 +487,29 @@ def main():
             bpv = 128 * w["n_bit"] // 8
             toff = np.zeros(spec.n_doc + 1, np.int64)
             toff[1:] = np.cumsum(spec.item_n_vec.astype(np.int64))
+            gdt = torch.float32 if args.gt_dtype == "f32" else torch.float64
+
+            def raw(a, b):
+                return synth.tokens_range(spec, a, b, dev)
             _, gi_raw = exhaustive.exhaustive_topk_stream(
-                qg, off[: n_gt + 1],
-                gt_chunks(spec, lambda a, b: synth.tokens_range(spec, a, b, dev), qg.shape[0]), k)
+                qg, off[: n_gt + 1], gt_chunks(spec, raw, qg.shape[0]), k, dtype=gdt)
             res2 = dix["residual"].view(-1, bpv)
 
             def decoded(a, b):
                 return exhaustive.decode_tokens(dix["centroid"], dix["vq_code"][toff[a]:toff[b]],
                                                 res2[toff[a]:toff[b]], dix["weight"], w["n_bit"])
             _, gi_idx = exhaustive.exhaustive_topk_stream(
-                both, both_off, gt_chunks(spec, decoded, both.shape[0]), k)
+                both, both_off, gt_chunks(spec, decoded, both.shape[0]), k, dtype=gdt)
+            if gdt == torch.float32:  # FP64 spot check of the FP32 ground truths
+                m = min(8, n_gt)
+                qs = qg[: int(off[m])]
+                _, c_raw = exhaustive.exhaustive_topk_stream(
+                    qs, off[: m + 1], gt_chunks(spec, raw, qs.shape[0]), k)
+                _, c_dec = exhaustive.exhaustive_topk_stream(
+                    qs, off[: m + 1], gt_chunks(spec, decoded, qs.shape[0]), k)
+                recall["gt_f32_spot_check"] = float(
+                    (np.mean(np.all(c_raw == gi_raw[:m], axis=1)) +
+                     np.mean(np.all(c_dec == gi_idx[:m], axis=1))) / 2)
             del dix, res2
         else:
             _, gi_raw = exhaustive.exhaustive_topk(qg, off[: n_gt + 1], tok, spec.item_n_vec, k)
@@ -677,6 +693,8 @@ def main():
                           "recall_ground_truth": "exhaustive FP64 MaxSim over the index's decoded "
                           "vectors (recall@10); over the raw synthetic tokens (..._vs_raw)",
                           "recall_queries": w["n_gt"], "tuning": tuning,
+                          "ground_truth_dtype": args.gt_dtype if streamed else "f64",
+                          "gt_f32_spot_check": recall.get("gt_f32_spot_check"),
                           "plain_fp32_qps": plain["qps"],
                           ("bf16_qps" if other & PREC_BF16 else "fp8_qps"): alt["qps"],
                           "candidate_scores": "imputed (MVR_CAND_IMPUTE)" if args.impute

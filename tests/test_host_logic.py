@@ -153,3 +153,22 @@ def test_bench_reference_arm_declines_streamed_workloads():
                              timeout=120, check=True).stdout.strip().splitlines()[-1]
         line = json.loads(out)
         assert line["impl"] == "reference" and "unavailable" in line
+
+
+def test_exhaustive_stream_fp32_screen_matches_fp64():
+    """The FP32 variant of the piecewise ground truth (bench --gt-dtype f32)
+    ranks like FP64 on a corpus without near-ties."""
+    ix = tiny_index(n_doc=250, n_centroid=16, seed=12)
+    q, off = synth.queries(ix["spec"], 5, 24, "cpu", seed=3)
+    tok = torch.from_numpy(ix["tokens"])
+    lens = ix["item_n_vec"].astype(np.int64)
+    toff = np.concatenate([[0], np.cumsum(lens)])
+    cuts = (0, 90, 250)
+
+    def pieces():
+        return ((a, lens[a:b], tok[toff[a]:toff[b]]) for a, b in zip(cuts, cuts[1:]))
+    s64, i64 = exhaustive.exhaustive_topk_stream(q, off, pieces(), 10)
+    s32, i32 = exhaustive.exhaustive_topk_stream(q, off, pieces(), 10, dtype=torch.float32)
+    np.testing.assert_array_equal(i32, i64)
+    np.testing.assert_allclose(s32, s64, rtol=1e-5)
+
