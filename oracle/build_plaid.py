@@ -6,10 +6,12 @@ recipe the reference's own loaders use (index_storage.py:37-61,
 colbert.py:39-50), pointed at a build folder inside this repository.  Test
 and baseline infrastructure only: plaid_cpu.py loads the built modules.
 
-    python oracle/build_plaid.py [reference root]
+    python oracle/build_plaid.py [reference root, default MVR_REFERENCE_ROOT]
 """
 import os
 import sys
+
+from refroot import REF_ROOT
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref", "plaid")
@@ -20,7 +22,7 @@ SOURCES = {
 }
 
 
-def main(ref_root="/root/reference"):
+def main(ref_root=REF_ROOT):
     from torch.utils.cpp_extension import load
     for name, rel in SOURCES.items():
         src = os.path.join(ref_root, rel)

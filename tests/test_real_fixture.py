@@ -20,8 +20,9 @@ import pytest
 
 import pyoracle
 from mvr import formats
+from refroot import ref_path
 
-DATA = "/root/reference/multi-vector-retrieval-data"
+DATA = ref_path("multi-vector-retrieval-data")
 IDX = os.path.join(DATA, "Index", "lotte-500-gnd", "plaid")
 pytestmark = pytest.mark.skipif(not os.path.isdir(IDX), reason="reference data tree absent")
 
