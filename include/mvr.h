@@ -239,7 +239,10 @@ int mvr_search_trace(mvr_index *h, const float *query, uint32_t nq,
  * MVR_ERR_INVALID_ARG.  Runs asynchronously on cuda_stream.  All calls on a
  * device share the array: calls whose GPU work overlaps race -- serialise
  * them.  The first call on a device does the one-time set-up (looks up the
- * array's device address); make it before any stream capture. */
+ * array's device address); make it before any stream capture.  The address
+ * is cached for the life of the process: after a cudaDeviceReset on that
+ * device it no longer points at the array, so do not call this entry point
+ * again in a process that has reset the device. */
 int mvr_filter_noalloc(mvr_index *h, const uint32_t *d_probe_id,
                        const float *d_probe_score, uint32_t nq,
                        uint32_t nprobe, uint32_t probe_topk,

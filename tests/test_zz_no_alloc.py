@@ -5,7 +5,9 @@ host's own pool allocator, or a latency-critical caller that cannot take
 cudaMalloc's implicit synchronisation).
 
 Checked through the C ABI against the regular filter stage of mvr_search
-(via mvr_search_trace) on two calls in a row: same shortlist, same
+(via mvr_search_trace) on two calls in a row, and against the oracle's filter
+(fed the oracle's own probe lists) at a small size and at the largest size the
+array accepts (262,144 docs, 32 query tokens): same shortlist, same
 approximate scores, bit for bit (the tolerance of every other filter test).
 This file is collected last on purpose."""
 import ctypes as C
@@ -13,7 +15,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
-from helpers import make_queries, tiny_index
+from helpers import make_queries, oracle_of, tiny_index
 from mvr import Index, _lib
 
 pytestmark = pytest.mark.gpu
@@ -56,6 +58,35 @@ def test_noalloc_filter_matches_search_filter_two_calls():
         np.testing.assert_array_equal(ids, t["short_id"])
         np.testing.assert_array_equal(approx, t["short_approx"])
     g.close()
+
+
+def _vs_oracle(ix, n_query, nprobe, ptk, seed):
+    g, o = _index(ix), oracle_of(ix)
+    q, off = make_queries(ix, n_query, 32, seed=seed)
+    for i in range(n_query):
+        qi = q[off[i]:off[i + 1]]
+        r = o.search_one(qi, 10, nprobe, ptk)
+        ids, approx = _noalloc(g, r["probe_id"], r["probe_score"], nprobe, ptk)
+        order = np.argsort(r["short_id"])
+        np.testing.assert_array_equal(ids, r["short_id"][order])
+        np.testing.assert_array_equal(approx, r["short_approx"][order])
+        t = g.trace(qi, 10, nprobe, ptk)
+        np.testing.assert_array_equal(ids, t["short_id"])
+    g.close()
+
+
+def test_noalloc_filter_matches_oracle_filter():
+    _vs_oracle(tiny_index(n_doc=900, n_centroid=96, n_bit=2, seed=31), 2, 5, 200, 32)
+
+
+def test_noalloc_filter_at_the_size_limit():
+    """Exactly 262,144 one-token docs (the array's doc limit) and 32 query
+    tokens (its token limit); every doc of a probed list ties with the others
+    of that list, so the shortlist's cut exercises the (score desc, id asc)
+    order."""
+    n = 1 << 18
+    ix = tiny_index(n_doc=n, n_centroid=64, n_bit=2, seed=33, lengths=np.ones(n, np.uint32))
+    _vs_oracle(ix, 2, 4, 3000, 34)
 
 
 def test_noalloc_filter_rejects_oversize():
