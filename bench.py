@@ -238,7 +238,81 @@ def cpu_port_qps(host, q_np, off, w, n_threads, probe_topk, budget_s=15.0):
     return n / dt, n, dt, o
 
 
-def plaid_cpu_baseline(host, q_np, off, k, n_threads, gi_eval, gi_raw, budget_s=10.0):
+def score_error_f64(q, off, ids, scores, arrays, n_bit, n_check):
+    """Relative error of the returned FP32 scores against FP64 MaxSim of the
+    same docs over the index's decoded vectors (GPUComputeScore.hpp:193-282
+    semantics, applied to x = centroid + weight[bucket]): max and mean over
+    the first n_check queries' returned docs.  arrays: the index's arrays, as
+    numpy (host) or torch tensors on the GPU."""
+    import torch
+    from mvr import exhaustive
+    dev = q.device
+
+    def t(a):
+        return a if isinstance(a, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(a))
+    lens = t(arrays["item_n_vec"]).cpu().numpy().view(np.uint32).astype(np.int64)
+    start = np.concatenate([[0], np.cumsum(lens)])
+    bpv = 128 * n_bit // 8
+    cen = t(arrays["centroid"]).to(dev)
+    code_all, res_all = t(arrays["vq_code"]), t(arrays["residual"]).view(-1)
+    errs = []
+    for i in range(n_check):
+        docs = [int(d) for d in ids[i] if d != 0xFFFFFFFF]
+        if not docs:
+            continue
+        tok = np.concatenate([np.arange(start[d], start[d + 1]) for d in docs])
+        ti = torch.from_numpy(tok).to(code_all.device)
+        code = code_all[ti].to(dev)
+        res = res_all.view(-1, bpv)[ti].to(dev)
+        x = exhaustive.decode_tokens(cen, code, res, t(arrays["weight"]), n_bit).double()
+        s = q[int(off[i]):int(off[i + 1])].double() @ x.T
+        seg = torch.repeat_interleave(torch.arange(len(docs), device=dev),
+                                      torch.from_numpy(lens[docs]).to(dev))
+        m = torch.full((s.shape[0], len(docs)), -torch.inf, dtype=torch.float64, device=dev)
+        m.scatter_reduce_(1, seg.expand(s.shape[0], -1), s, reduce="amax")
+        ref = m.sum(0).cpu().numpy()
+        got = np.asarray([float(sc) for d, sc in zip(ids[i], scores[i]) if d != 0xFFFFFFFF])
+        errs.append(np.abs(got - ref) / np.maximum(np.abs(ref), 1e-12))
+    e = np.concatenate(errs) if errs else np.zeros(0)
+    return {"max_rel": float(e.max()) if len(e) else None,
+            "mean_rel": float(e.mean()) if len(e) else None, "results": int(len(e))}
+
+
+def plain_parity(g, o, q_np, off, w, probe_topk, n_check, gpu_ids, gpu_scores, n_threads):
+    """Part of the CPU-baseline leg: the first n_check workload queries traced
+    stage by stage through the GPU's plain FP32 path (mvr_search_trace) and
+    searched by the oracle's CPU port, with the timed plain-path top-k of the
+    same queries; counts the queries whose probe lists, candidate sets with
+    approximate scores, shortlists with exact scores, and final top-k are
+    bit-identical."""
+    from concurrent.futures import ThreadPoolExecutor
+    k, nprobe = w["topk"], w["nprobe"]
+    qs = [np.ascontiguousarray(q_np[off[i]:off[i + 1]]) for i in range(n_check)]
+    with ThreadPoolExecutor(n_threads) as ex:  # the oracle's C calls release the GIL
+        refs = list(ex.map(lambda qi: o.search_one(qi, k, nprobe, probe_topk), qs))
+    cnt = dict(probe=0, candidates=0, shortlist=0, topk=0, topk_timed=0)
+    for i, (qi, r) in enumerate(zip(qs, refs)):
+        t = g.trace(qi, k, nprobe, probe_topk)
+        cnt["probe"] += bool(np.array_equal(t["probe_id"], r["probe_id"]) and
+                             np.array_equal(t["probe_score"], r["probe_score"]))
+        cnt["candidates"] += bool(np.array_equal(t["cand_id"], r["cand_id"]) and
+                                  np.array_equal(t["cand_score"], r["cand_score"]))
+        o_ = np.argsort(r["short_id"])
+        cnt["shortlist"] += bool(np.array_equal(t["short_id"], r["short_id"][o_]) and
+                                 np.array_equal(t["short_approx"], r["short_approx"][o_]) and
+                                 np.array_equal(t["short_exact"], r["short_exact"][o_]))
+        cnt["topk"] += bool(np.array_equal(t["id"], r["id"]) and np.array_equal(t["score"], r["score"]))
+        cnt["topk_timed"] += bool(np.array_equal(gpu_ids[i], r["id"]) and
+                                  np.array_equal(gpu_scores[i], r["score"]))
+    exact = min(cnt.values())
+    return {"queries": n_check, "bit_exact": exact, "per_stage": cnt,
+            "path": "plain FP32 GPU path vs the oracle's CPU port, same index and queries",
+            "checked": "probe ids+scores, candidate ids+approximate scores, shortlist ids+"
+                       "approximate+exact scores, top-k ids+scores (traced and timed runs)"}
+
+
+def plaid_cpu_baseline(host, q_np, off, k, n_threads, gi_eval, gi_raw, budget_s=10.0,
+                       sweep_q=30):
     """The reference's own PLAID CPU search (its compiled extensions, oracle/
     plaid_cpu.py) over this index re-laid in PLAID's layout, at PLAID's
     defaults for k, on a bounded sample of the workload's queries; recall@k
@@ -257,11 +331,24 @@ def plaid_cpu_baseline(host, q_np, off, k, n_threads, gi_eval, gi_raw, budget_s=
         n += 1
     dt = time.perf_counter() - t
     m = min(len(gi_eval), len(est))
+    # wider settings (PLAID's k=100 defaults, then 4x its candidate budget)
+    # on the first sweep_q queries: how far PLAID's recall goes and at what rate
+    sweep = []
+    for prm in (dict(ncells=2, centroid_score_threshold=0.45, ndocs=1024),
+                dict(ncells=4, centroid_score_threshold=0.4, ndocs=4096)):
+        ns_ = min(sweep_q, n_q, len(gi_eval))
+        t0 = time.perf_counter()
+        e2 = [p.search_one(q_np[off[i]:off[i + 1]], k, **prm)[0] for i in range(ns_)]
+        d2 = time.perf_counter() - t0
+        sweep.append({"params": prm, "queries": ns_, "queries/s": ns_ / d2,
+                      "recall@10": float(formats_recall(gi_eval[:ns_], e2, k)),
+                      "recall@10_vs_raw": float(formats_recall(gi_raw[:ns_], e2, k))})
     return {"value": n / dt, "unit": "queries/s", "cores": n_threads, "kind": "reference",
             "sample": f"first {n} of the {n_q} queries ({dt:.1f} s)",
             "params": plaid_cpu.defaults(k),
             "recall@10": float(formats_recall(gi_eval[:m], est[:m], k)),
-            "recall@10_vs_raw": float(formats_recall(gi_raw[:m], est[:m], k))}
+            "recall@10_vs_raw": float(formats_recall(gi_raw[:m], est[:m], k)),
+            "sweep": sweep}
 
 
 def formats_recall(gnd, est, k):
@@ -280,8 +367,22 @@ def run_reference(args, w):
         return
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    from mvr import synth
-    spec, host, _, _ = get_index(w, f"cuda:{local}", rank, want_tokens=False)
+    from mvr import formats, synth
+    # the index is built (once, cached on local disk) by a child process, so
+    # this process maps no library of the GPU engine: it reads the cached
+    # index files and runs only the CPU port
+    cdir = cache_dir(w)
+    if not os.path.exists(os.path.join(cdir, "DONE")):
+        cmd = [sys.executable, os.path.abspath(__file__), "--build-index-only",
+               "--workload", args.workload]
+        if args.n_doc:
+            cmd += ["--n-doc", str(args.n_doc)]
+        if args.n_centroid:
+            cmd += ["--n-centroid", str(args.n_centroid)]
+        subprocess.run(cmd, check=True, env=dict(os.environ, CUDA_VISIBLE_DEVICES=str(local)))
+    host = formats.read_index_dir(cdir)
+    host["n_bit"] = w["n_bit"]
+    spec = synth.CorpusSpec(w["n_doc"], seed=w["seed"], len_hi=w.get("len_hi", 180))
     q, off = synth.queries(spec, w["n_query"], w["n_tok"], f"cuda:{local}", seed=100)
     q_np = q.cpu().numpy()
     del q
@@ -313,7 +414,9 @@ def run_reference(args, w):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": workload_config(w, "CPU port of the reference path (oracle)", w["probe_topk"]),
+        "config": dict(workload_config(w, w["probe_topk"]),
+                       path="the oracle's CPU port of the reference's IGP GPU search path "
+                            "(same index files and queries as the GPU arm)"),
         "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": n_threads, "kind": "port",
                          "sample": f"{n} queries per step of the {w['n_query']}-query workload"},
         "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0,
@@ -322,8 +425,9 @@ def run_reference(args, w):
     print(json.dumps(line))
 
 
-def workload_config(w, path, probe_topk):
-    return {"workload": (f"{path}: {w['n_doc']:,} synthetic docs (lognormal 70/35, clipped "
+def workload_config(w, probe_topk):
+    """The workload's description, the same for both arms."""
+    return {"workload": (f"{w['n_doc']:,} synthetic docs (lognormal 70/35, clipped "
                          f"8..{w.get('len_hi', 180)}), "
                          f"{w['n_centroid']:,} centroids, nbits {w['n_bit']}, "
                          f"{w['n_query']:,} queries x {w['n_tok']} tok, nprobe {w['nprobe']}, "
@@ -385,10 +489,22 @@ def main():
                          "(MVR_CAND_IMPUTE); the plain path keeps the reference's scores")
     ap.add_argument("--precision", choices=["bf16", "fp8"], default="fp8",
                     help="tensor-core MaxSim precision of the headline path")
+    ap.add_argument("--build-index-only", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--prune", action="store_true",
+                    help="also train the learned candidate pruner on plain-path traces of this "
+                         "corpus and time the pruned FP8 search (MVR_PRUNE)")
+    ap.add_argument("--prune-queries", type=int, default=50000,
+                    help="training queries traced through the plain path (40 traces each)")
+    ap.add_argument("--prune-keep", type=int, default=400,
+                    help="shortlisted docs the pruned search scores per confident query")
+    ap.add_argument("--prune-epochs", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--plaid-baseline", action="store_true",
-                    help="also time the reference's PLAID CPU search (its compiled extensions) "
-                         "on this index, with its recall")
+    ap.add_argument("--parity-queries", type=int, default=50,
+                    help="queries of the workload checked stage by stage against the oracle's "
+                         "CPU port inside the CPU-baseline leg (0: none)")
+    ap.add_argument("--no-plaid-baseline", action="store_true",
+                    help="skip the reference's PLAID CPU search (cpu_baseline_plaid; run by "
+                         "default at N=1 on the resident workloads)")
     ap.add_argument("--profile-case", action="store_true",
                     help="small profiling target instead of the bench: 200,000 docs, 16,384 "
                          "centroids, one mixed-precision and one plain search of 296 queries")
@@ -415,6 +531,10 @@ def main():
         w["n_doc"] = args.n_doc
     if args.n_centroid:
         w["n_centroid"] = args.n_centroid
+    if args.build_index_only:  # child of the reference arm: build and cache the index
+        import torch
+        get_index(w, "cuda:0", 0, want_tokens=False)
+        return
     if args.impl == "reference":
         return run_reference(args, w)
     if args.profile_case:
@@ -476,7 +596,10 @@ def main():
     # over the index's own decoded tokens (what candidate generation can
     # reach); the shortlist sizes are tuned on a separate query sample against
     # the latter, then recall is measured on the first n_gt workload queries
-    recall, tuning = {}, {}
+    recall, tuning, score_err = {}, {}, {}
+    # the other tensor-core precision (timed beside the headline path)
+    other = (FAST ^ PREC_FP8 ^ PREC_BF16) if FAST & (PREC_FP8 | PREC_BF16) else PREC_BF16
+    ptk[other] = ptk[FAST]
     if rank == 0:
         n_gt, n_tune = w["n_gt"], w["n_tune"]
         qg = q[: int(off[n_gt])]
@@ -510,7 +633,7 @@ def main():
                 recall["gt_f32_spot_check"] = float(
                     (np.mean(np.all(c_raw == gi_raw[:m], axis=1)) +
                      np.mean(np.all(c_dec == gi_idx[:m], axis=1))) / 2)
-            del dix, res2
+            del res2
         else:
             _, gi_raw = exhaustive.exhaustive_topk(qg, off[: n_gt + 1], tok, spec.item_n_vec, k)
             del tok
@@ -541,16 +664,23 @@ def main():
                 tuning["batch"] = dict(batch=tb["batch"], table=[(x["batch"], round(x["ms"], 3))
                                                                  for x in tb["table"]])
                 g.set_batch(tb["batch"] if args.use_tuned else (args.batch or w.get("batch", 0)))
-        for name, fl in (("fast", FAST), ("plain", PLAIN)):
+        arrays = dix if streamed else host
+        ptk[other] = ptk[FAST]
+        for name, fl in (("fast", FAST), ("plain", PLAIN), ("other", other)):
             step(fl)
             est = out_i[:n_gt].cpu().numpy().view(np.uint32)
             recall[name] = float(formats.recall_at_k(gi_eval, est, k).mean())
             recall[name + "_raw"] = float(formats.recall_at_k(gi_raw, est, k).mean())
+            score_err[name] = score_error_f64(q, off, est, out_s[:n_gt].cpu().numpy(), arrays,
+                                              w["n_bit"], n_gt)
+        if streamed:
+            del dix, arrays
         torch.cuda.empty_cache()
     if world > 1:  # every rank serves at rank 0's tuned shortlist sizes
         pt = torch.tensor([ptk[FAST], ptk[PLAIN]], dtype=torch.int64, device=dev)
         dist.broadcast(pt, 0)
         ptk[FAST], ptk[PLAIN] = int(pt[0]), int(pt[1])
+        ptk[other] = ptk[FAST]
 
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
@@ -564,7 +694,8 @@ def main():
             torch.cuda.profiler.start()
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
               for _ in range(args.steps)]
-        acc = dict(stage=np.zeros(6), launches=0, n_cand=0, n_tok=0, n_ent=0, n_batch=0)
+        acc = dict(stage=np.zeros(6), launches=0, n_cand=0, n_tok=0, n_ent=0, n_batch=0,
+                   fallback=0)
         for s in range(args.steps):
             flush.fill_(s & 0xFF)
             ev[s][0].record(stream)
@@ -576,6 +707,7 @@ def main():
             acc["n_tok"] += st.n_rerank_tok
             acc["n_ent"] += st.n_list_ent
             acc["n_batch"] += st.n_batch
+            acc["fallback"] += st.n_prune_fallback
         torch.cuda.synchronize()
         if profile:
             torch.cuda.profiler.stop()
@@ -587,9 +719,6 @@ def main():
         return acc
 
     plain = measure(PLAIN)
-    other = (FAST ^ PREC_FP8 ^ PREC_BF16) if FAST & (PREC_FP8 | PREC_BF16) else PREC_BF16
-    # (the other tensor-core precision, same candidate scoring)
-    ptk[other] = ptk[FAST]
     alt = measure(other)
     with ClockSampler(local) as clk:
         fast = measure(FAST, profile=True)
@@ -602,6 +731,54 @@ def main():
         g.set_graphs(False)
         fast["stage"] = measure(FAST)["stage"]
         g.set_graphs(True)
+
+    # learned candidate pruner (config-4 protocol): traces of the plain path
+    # on this corpus, training with libmvr's kernels, the pruned FP8 search
+    # timed and its recall measured like the headline path's
+    prune_rec = None
+    if args.prune and rank == 0 and world == 1 and not streamed and not ragged:
+        from mvr import PRUNE
+        from mvr import prune as mprune
+        t0 = time.time()
+        qtr, offtr = synth.queries(spec, args.prune_queries, w["n_tok"], dev, seed=700)
+        X, y, qid = mprune.traces(g, qtr.cpu().numpy(), offtr, nprobe, ptk[PLAIN],
+                                  per_query=40, seed=1)
+        t_trace = time.time() - t0
+        hold = qid >= int(0.95 * args.prune_queries)
+        t0 = time.time()
+        params, hist = mprune.train(X[~hold], y[~hold], epochs=args.prune_epochs)
+        t_train = time.time() - t0
+        margin = mprune.margin_for(X[hold], y[hold], params)
+        keep = min(args.prune_keep, ptk[FAST])
+        g.set_pruner(params, keep, margin)
+        PR = FAST | PRUNE
+        ptk[PR] = ptk[FAST]
+        step(PR)
+        est = out_i[:w["n_gt"]].cpu().numpy().view(np.uint32)
+        pr_recall = float(formats.recall_at_k(gi_eval, est, k).mean())
+        pr_recall_raw = float(formats.recall_at_k(gi_raw, est, k).mean())
+        pr_err = score_error_f64(q, off, est, out_s[:w["n_gt"]].cpu().numpy(), host, w["n_bit"],
+                                 w["n_gt"])
+        pr = measure(PR)
+        prune_rec = {"qps": pr["qps"], "ms_per_step": pr["total_ms"] / args.steps,
+                     "keep": keep, "shortlist": ptk[PR], "margin": margin,
+                     "fallback_frac": pr["fallback"] / (args.steps * n_query),
+                     "recall@10": pr_recall, "recall@10_vs_raw": pr_recall_raw,
+                     "recall@10_loss_vs_headline": recall.get("fast", 0.0) - pr_recall,
+                     "recall@10_loss_vs_plain": recall.get("plain", 0.0) - pr_recall,
+                     "score_error_vs_f64": pr_err,
+                     "speedup_vs_headline": pr["qps"] / fast["qps"],
+                     "speedup_vs_plain": pr["qps"] / plain["qps"],
+                     "rerank_tok_per_query": pr["n_tok"] / (args.steps * n_query),
+                     "stage_ms_per_step": [float(x / args.steps) for x in pr["stage"]],
+                     "traces": int(len(y)), "train_queries": args.prune_queries,
+                     "trace_s": t_trace, "train_s": t_train, "train_loss": hist,
+                     "heldout_rmse": margin / 3.0,
+                     "features": "per query token the best E4M3 centroid score among the doc's "
+                                 "tokens' centroids, and log(doc length)",
+                     "model": "MLP 33-256-256-1, GELU, BF16 weights, FP32 accumulation; "
+                              "trained by libmvr's kernels (Adam, MSE on exact MaxSim / nq)"}
+        g.set_pruner(None, 0, 0.0)
 
     # end to end: pinned host buffers, copies inside every step
     hq = q.cpu().pin_memory()
@@ -665,36 +842,54 @@ def main():
             "rerank_tflops": 2.0 * nq_avg * D * fast["n_tok"] / 1e12 / (stage[3] / 1e3),
             "rescore_topk_ms_per_step": float(stage[4] / S)}
 
-    cpu = None
+    cpu, parity = None, None
     if streamed:
         cpu = {"value": None, "unit": "queries/s", "cores": 0, "kind": "port",
                "sample": "not run: the streamed index lives on the device only (the CPU port "
                          "is timed on the default workloads)"}
     elif world == 1 and not args.no_cpu_baseline:
-        qps_cpu, n_s, dt_s, _ = cpu_port_qps(host, hq.numpy(), off, w, os.cpu_count(), ptk[PLAIN])
+        qps_cpu, n_s, dt_s, orc = cpu_port_qps(host, hq.numpy(), off, w, os.cpu_count(),
+                                               ptk[PLAIN])
         cpu = {"value": qps_cpu, "unit": "queries/s", "cores": os.cpu_count(), "kind": "port",
                "sample": f"first {n_s} of the {n_query} queries ({dt_s:.1f} s)"}
+        if args.parity_queries > 0:  # the oracle as the checker of the plain GPU path
+            n_chk = min(args.parity_queries, n_query)
+            step(PLAIN)
+            torch.cuda.synchronize()
+            parity = plain_parity(g, orc, hq.numpy(), off, w, ptk[PLAIN], n_chk,
+                                  out_i[:n_chk].cpu().numpy().view(np.uint32),
+                                  out_s[:n_chk].cpu().numpy(), os.cpu_count())
     plaid = None
-    if args.plaid_baseline and not streamed and world == 1:
+    if not args.no_plaid_baseline and not streamed and world == 1:
         plaid = plaid_cpu_baseline(host, hq.numpy(), off, k, os.cpu_count(), gi_eval, gi_raw)
 
     R = args.rescore or 4 * k
+    gt_dt = args.gt_dtype if streamed else "f64"
+    gt_name = ("FP32 (FP64 spot check: gt_f32_spot_check)" if gt_dt == "f32" else "FP64")
     line = {
         "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": S,
         "warmup": args.warmup, "ms_per_step": fast["total_ms"] / S, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp8" if fp8_ran else "bf16",
         "data": "synthetic",
-        "config": dict(workload_config(w, f"{'FP8' if fp8_ran else 'BF16'} tensor-core MaxSim + "
-                                          "FP32 re-score", ptk[FAST]),
-                       **{"rescore": R, "probe_topk": ptk[FAST], "probe_topk_plain": ptk[PLAIN],
+        "config": dict(workload_config(w, ptk[FAST]),
+                       **{"path": f"{'FP8' if fp8_ran else 'BF16'} tensor-core MaxSim + FP32 "
+                                  "re-score", "rescore": R, "probe_topk": ptk[FAST], "probe_topk_plain": ptk[PLAIN],
                           "recall@10": recall.get("fast"), "recall@10_plain": recall.get("plain"),
                           "recall@10_vs_raw": recall.get("fast_raw"),
                           "recall@10_plain_vs_raw": recall.get("plain_raw"),
-                          "recall_ground_truth": "exhaustive FP64 MaxSim over the index's decoded "
-                          "vectors (recall@10); over the raw synthetic tokens (..._vs_raw)",
+                          "recall_ground_truth": f"exhaustive {gt_name} MaxSim over the index's "
+                          "decoded vectors (recall@10); over the raw synthetic tokens (..._vs_raw)",
                           "recall_queries": w["n_gt"], "tuning": tuning,
-                          "ground_truth_dtype": args.gt_dtype if streamed else "f64",
+                          "ground_truth_dtype": gt_dt,
                           "gt_f32_spot_check": recall.get("gt_f32_spot_check"),
+                          ("recall@10_bf16" if other & PREC_BF16 else "recall@10_fp8"):
+                              recall.get("other"),
+                          "score_error_vs_f64": {
+                              "what": "returned FP32 scores vs FP64 MaxSim of the same docs over "
+                                      "the decoded index vectors, over the recall queries' "
+                                      "top-k",
+                              "headline": score_err.get("fast"), "plain": score_err.get("plain"),
+                              ("bf16" if other & PREC_BF16 else "fp8"): score_err.get("other")},
                           "plain_fp32_qps": plain["qps"],
                           ("bf16_qps" if other & PREC_BF16 else "fp8_qps"): alt["qps"],
                           "candidate_scores": "imputed (MVR_CAND_IMPUTE)" if args.impute
@@ -717,6 +912,8 @@ def main():
         "roofline": roof,
         "cpu_baseline": cpu,
         **({"cpu_baseline_plaid": plaid} if plaid is not None else {}),
+        **({"parity": parity} if parity is not None else {}),
+        **({"pruner": prune_rec} if prune_rec is not None else {}),
         "clocks": clk.summary(),
         "gpu_launches": int(fast["launches"]),
         "p99_ms": p99,
