@@ -48,8 +48,8 @@ typedef enum {
                             per-token power-of-two scales, centroid rows and
                             bucket weights as E4M3, FP32 accumulation; the
                             best R docs are re-scored exactly in FP32.
-                            2-bit indexes; other code widths run the BF16
-                            kernel.  May be combined with MVR_SEM_BASIC. */
+                            2- and 4-bit indexes; other code widths run the
+                            BF16 kernel.  May be combined with MVR_SEM_BASIC. */
 
 #define MVR_CAND_IMPUTE 8u /* candidate filter: a query token that visits no
                             probed list holding the doc adds its lowest probed
@@ -58,6 +58,19 @@ typedef enum {
                             closer to the exact MaxSim; not a reference
                             option, so candidate scores then differ from the
                             reference's. */
+
+#define MVR_PRUNE 16u /* learned candidate pruner (no counterpart in the
+                          reference; needs MVR_PREC_FP8, a 2- or 4-bit
+                          index, queries of up to 32 tokens and weights set
+                          by mvr_index_set_pruner): after the shortlist, the
+                          pruner's MLP predicts each shortlisted doc's
+                          MaxSim from its features, and the FP8 MaxSim
+                          scores only the `keep` docs with the best
+                          predictions -- unless the query's R-th best
+                          prediction leads its keep-th best by less than
+                          `margin` (low confidence), when it scores the whole
+                          shortlist.  The exact FP32 re-score stays the judge
+                          of the final top-k. */
 
 typedef struct mvr_index mvr_index;
 
@@ -83,6 +96,8 @@ typedef struct {
                              copy, scoring + probe, filter, rerank (FP32 or
                              BF16 tensor-core), FP32 re-score + top-k,
                              result copy */
+  uint64_t n_prune_fallback; /* MVR_PRUNE: queries whose whole shortlist was
+                                scored (low-confidence predictions) */
 } mvr_stats;
 
 /* Per-query stage trace (parity tests).  Caller-owned host buffers. */
@@ -99,6 +114,10 @@ typedef struct {
   float *short_exact;    /* [probe_topk] exact MaxSim */
   float *topk_score;     /* [topk] final result */
   uint32_t *topk_id;     /* [topk] */
+  float *short_feat;     /* nullable [probe_topk][33]: learned-pruner features
+                            of short_id[i] (FP8 index, <= 32 query tokens) */
+  float *short_pred;     /* nullable [probe_topk]: the pruner's prediction
+                            for short_id[i] (a pruner must be set) */
 } mvr_trace;
 
 /* Error text of the last failing call on this thread ("" if none). */
@@ -222,6 +241,56 @@ int mvr_search_device(mvr_index *h, const float *d_query_l,
 int mvr_search_trace(mvr_index *h, const float *query, uint32_t nq,
                      uint32_t topk, uint32_t nprobe, uint32_t probe_topk,
                      uint32_t flags, mvr_trace *trace);
+
+/* ---- learned candidate pruner (no counterpart in the reference) ----
+ * An MLP 33 -> 256 -> 256 -> 1 with GELU (tanh form) over per-candidate
+ * features -- per query token (up to 32) the best centroid score among the
+ * doc's tokens' centroids, then log(doc length) -- predicting each
+ * shortlisted doc's exact MaxSim.  Parameters: one float vector of
+ * MVR_MLP_NUM_PARAMS values, W1 [256][33], b1 [256], W2 [256][256],
+ * b2 [256], w3 [256], b3; weights are applied rounded to BF16 with FP32
+ * accumulation. */
+#define MVR_MLP_NUM_PARAMS 74753u
+#define MVR_MLP_FEAT 33u
+
+/* Training workspace, in floats, for minibatches of n rows. */
+size_t mvr_mlp_work_floats(uint32_t n);
+
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8, learning rate lr; step counts
+ * from 1) on the loss 0.5 * mean((mlp(x) - y)^2) of a minibatch, with the
+ * library's hand-written kernels.  Device buffers: d_x [n][33], d_y [n],
+ * d_params / d_adam_m / d_adam_v [MVR_MLP_NUM_PARAMS] (updated in place),
+ * d_work [mvr_mlp_work_floats(n)], d_loss (nullable, one float: the
+ * minibatch loss before the step).  Synchronises cuda_stream. */
+int mvr_mlp_train_step(const float *d_x, const float *d_y, uint32_t n,
+                       float *d_params, float *d_adam_m, float *d_adam_v,
+                       float *d_work, float lr, uint32_t step, float *d_loss,
+                       void *cuda_stream);
+
+/* The MLP's forward pass on CUDA cores (the training kernels' arithmetic):
+ * d_out [n] from d_x [n][33]; d_work as for training. */
+int mvr_mlp_forward(const float *d_x, uint32_t n, const float *d_params,
+                    float *d_work, float *d_out, void *cuda_stream);
+
+/* Sets the learned pruner of a handle (MVR_PRUNE): params = host float
+ * [MVR_MLP_NUM_PARAMS] (NULL removes it), keep = docs scored per query when
+ * the predictions are confident (1..probe_topk of the searches), margin =
+ * the confidence threshold (prediction units). */
+int mvr_index_set_pruner(mvr_index *h, const float *params, uint32_t keep,
+                         float margin);
+
+/* Tile shape of the FP8 MaxSim kernel (MVR_PREC_FP8): shortlisted docs per
+ * CTA, 32, 64 or 128 (0: the default, 64); chosen by the library's tuner
+ * (mvr.tune.tune_tile).  No counterpart in the reference. */
+int mvr_index_set_rerank_tile(mvr_index *h, uint32_t docs_per_cta);
+
+/* Failure detection (test hook; no counterpart in the reference, whose
+ * kernels have no bounded waits): the time bound of every pipeline wait of
+ * the FP8 MaxSim kernel, in ns (0 restores the default, 1 s).  A wait that
+ * runs out stops the kernel, which still lets its own copies and MMAs finish
+ * and frees its tensor memory; the search then fails with MVR_ERR_CUDA and
+ * the handle stays usable.  Tests set a tiny bound to make a wait run out. */
+int mvr_index_set_wait_limit(mvr_index *h, uint64_t wait_ns);
 
 /* Candidate filter for ONE query with no device allocation in the call: the
  * probe lists -> candidate set -> approximate scores -> top-probe_topk

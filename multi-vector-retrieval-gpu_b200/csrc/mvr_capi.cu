@@ -19,6 +19,7 @@
 #include "mvr_io.hpp"
 #include "mvr_kernels.cuh"
 #include "mvr_tc.cuh"
+#include "mvr_prune.cuh"
 
 using namespace mvr;
 
@@ -107,7 +108,8 @@ struct Workspace {
   uint32_t *stamp = nullptr;    // rank-table fallback: [fb_slots][n_item]
   uint8_t *rank = nullptr;      //   [fb_slots][n_item][rank_stride]
   uint64_t *key = nullptr;      //   [fb_slots][n_item]
-  uint64_t *hkey = nullptr;     // hash filter: [slots][kHashKeys] candidate keys
+  uint64_t *hkey = nullptr;     // hash filter: [slots][key_stride] candidate keys
+  uint32_t key_stride = 0;      //   keys per slot: kHashFill * the largest range count
   uint32_t *qcnt = nullptr, *ovf = nullptr;  // [slots] hash-filter counters / overflow flags
   // per batch
   uint32_t batch_slots = 0, tok_cap = 0, np_cap = 0, short_cap = 0, topk_cap = 0;
@@ -131,6 +133,14 @@ struct Workspace {
   uint64_t *h_off = nullptr;    // pinned mirror
   uint32_t *qstat = nullptr;    // device [n_query][3]
   uint32_t *h_qstat = nullptr;  // pinned mirror
+  // learned pruner (MVR_PRUNE), per batch
+  uint32_t pr_slots = 0, pr_short = 0, pr_keep = 0;
+  float *feat = nullptr;        // [slots][short][33] features
+  float *pred = nullptr;        // [slots][short] predictions
+  float *kept_s = nullptr;      // [slots][keep] best predictions
+  uint32_t *kept_id = nullptr;  // [slots][keep]
+  uint32_t *fin_id = nullptr;   // [slots][short] docs the rerank takes
+  uint32_t *n_fin = nullptr;    // [slots]
 };
 
 struct mvr_index {
@@ -156,6 +166,17 @@ struct mvr_index {
   uint32_t *d_epoch = nullptr;   // stamp-epoch counter of the rank-table fallback (device)
   uint64_t epoch_used = 0;       // epochs consumed since the stamps were last cleared
   uint64_t ws_gen = 0;           // bumped whenever a workspace buffer is reallocated
+  // hash filter sizing: candidates per probed list, the largest over the
+  // queries of the previous search call (0: none yet)
+  double cand_per_probe = 0.0;
+  uint64_t wait_ns = 1000000000ull;  // bound of the FP8 rerank's pipeline waits
+  uint32_t ws_docs = 64;             // shortlisted docs per CTA of the FP8 rerank
+  // learned pruner (mvr_index_set_pruner): BF16 weight tiles, b1/b2/w3/b3
+  uint8_t *prune_wts = nullptr;
+  float *prune_vecs = nullptr;
+  uint32_t prune_keep = 0;
+  float prune_margin = 0.f;
+  unsigned long long *d_fallback = nullptr;  // queries of a call that scored their whole shortlist
   // CUDA-graph replay of repeated device-buffer searches (mvr_index_set_graphs)
   bool graphs = false;
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;  // stream handoff (no timing)
@@ -167,6 +188,7 @@ struct mvr_index {
     uint32_t *out_id = nullptr;
     uint32_t n_query = 0, topk = 0, nprobe = 0, probe_topk = 0, flags = 0, R = 0, B = 0;
     uint64_t gen = 0;
+    double cand_per_probe = 0.0;  // the hash filter's layout was sized by this
     std::vector<uint64_t> off;
     int launches = 0;
   } graph;
@@ -188,6 +210,10 @@ struct mvr_index {
       if (e) cudaEventDestroy(e);
     free_scratch();
     free_batch();
+    free_prune();
+    dfree(prune_wts);
+    dfree(prune_vecs);
+    dfree(d_fallback);
     dfree(ws.q_off);
     dfree(ws.qstat);
     if (ws.h_off) cudaFreeHost(ws.h_off);
@@ -200,6 +226,14 @@ struct mvr_index {
     ws.stamp = nullptr; ws.rank = nullptr; ws.key = nullptr; ws.hkey = nullptr;
     ws.qcnt = nullptr; ws.ovf = nullptr;
     ws.slots = 0;
+  }
+  void free_prune() {
+    for (void *p : {(void *)ws.feat, (void *)ws.pred, (void *)ws.kept_s, (void *)ws.kept_id,
+                    (void *)ws.fin_id, (void *)ws.n_fin})
+      dfree(p);
+    ws.feat = ws.pred = ws.kept_s = nullptr;
+    ws.kept_id = ws.fin_id = ws.n_fin = nullptr;
+    ws.pr_slots = ws.pr_short = ws.pr_keep = 0;
   }
   void free_batch() {
     for (void *p : {(void *)ws.q, (void *)ws.probe_id, (void *)ws.part_id, (void *)ws.probe_s,
@@ -225,7 +259,8 @@ namespace {
 
 // Queries per device batch: 8 per SM (1,184 on B200) -- large batches fill
 // the tensor-core probe's token tiles and the re-score's CTAs; the hash
-// filter's key space is kHashKeys * 8 B = 917 KB per query.
+// filter's key space is kHashFill * 8 B = 57 KB per query per doc range
+// (8 to 64 ranges).
 uint32_t default_batch(const mvr_index *h) { return 8u * (uint32_t)h->n_sm; }
 
 // Slots of the rank-table fallback (n_item * (4 + 32|64 + 8) bytes each,
@@ -238,16 +273,18 @@ uint32_t fallback_slots(const mvr_index *h, uint32_t slots, uint32_t rank_stride
   return std::max(1u, f);
 }
 
-int ensure_scratch(mvr_index *h, uint32_t slots, uint32_t rank_stride) {
+int ensure_scratch(mvr_index *h, uint32_t slots, uint32_t rank_stride, uint32_t key_stride) {
   Workspace &w = h->ws;
-  if (w.slots >= slots && w.rank_stride >= rank_stride) return MVR_OK;
+  if (w.slots >= slots && w.rank_stride >= rank_stride && w.key_stride >= key_stride)
+    return MVR_OK;
+  key_stride = std::max(key_stride, w.key_stride);
   h->free_scratch();
   const size_t n = (size_t)h->dix.n_item;
   const uint32_t fb = fallback_slots(h, slots, rank_stride);
   MVR_TRY(dalloc(&w.stamp, fb * n));
   MVR_TRY(dalloc(&w.rank, fb * n * rank_stride));
   MVR_TRY(dalloc(&w.key, fb * n));
-  MVR_TRY(dalloc(&w.hkey, (size_t)slots * kHashKeys));
+  MVR_TRY(dalloc(&w.hkey, (size_t)slots * key_stride));
   MVR_TRY(dalloc(&w.qcnt, slots));
   MVR_TRY(dalloc(&w.ovf, slots));
   CUDA_TRY(cudaMemsetAsync(w.qcnt, 0, slots * sizeof(uint32_t), h->stream));
@@ -259,8 +296,29 @@ int ensure_scratch(mvr_index *h, uint32_t slots, uint32_t rank_stride) {
   w.slots = slots;
   w.fb_slots = fb;
   w.rank_stride = rank_stride;
+  w.key_stride = key_stride;
   h->epoch_used = 0;
   h->ws_gen++;
+  return MVR_OK;
+}
+
+int ensure_prune(mvr_index *h, uint32_t slots, uint32_t short_cap, uint32_t keep) {
+  Workspace &w = h->ws;
+  if (w.pr_slots >= slots && w.pr_short >= short_cap && w.pr_keep >= keep) return MVR_OK;
+  slots = std::max(slots, w.pr_slots);
+  short_cap = std::max(short_cap, w.pr_short);
+  keep = std::max(keep, w.pr_keep);
+  h->free_prune();
+  h->ws_gen++;
+  MVR_TRY(dalloc(&w.feat, (size_t)slots * short_cap * 33));
+  MVR_TRY(dalloc(&w.pred, (size_t)slots * short_cap));
+  MVR_TRY(dalloc(&w.kept_s, (size_t)slots * keep));
+  MVR_TRY(dalloc(&w.kept_id, (size_t)slots * keep));
+  MVR_TRY(dalloc(&w.fin_id, (size_t)slots * short_cap));
+  MVR_TRY(dalloc(&w.n_fin, (size_t)slots));
+  w.pr_slots = slots;
+  w.pr_short = short_cap;
+  w.pr_keep = keep;
   return MVR_OK;
 }
 
@@ -405,7 +463,7 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
     return MVR_OK;
   }
   if (!query || !out_s || !out_id) return set_err(MVR_ERR_INVALID_ARG, "null query/result buffer");
-  if (flags & ~(MVR_SEM_BASIC | MVR_PREC_BF16 | MVR_PREC_FP8 | MVR_CAND_IMPUTE))
+  if (flags & ~(MVR_SEM_BASIC | MVR_PREC_BF16 | MVR_PREC_FP8 | MVR_CAND_IMPUTE | MVR_PRUNE))
     return set_err(MVR_ERR_INVALID_ARG, "unknown flags %u", flags);
   const int sem = (flags & MVR_SEM_BASIC) ? 1 : 0;
   const bool fp8 = (flags & MVR_PREC_FP8) != 0 && h->cen8 != nullptr;
@@ -415,6 +473,14 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
   std::vector<uint64_t> off;
   uint32_t nq_max = 0;
   MVR_TRY(build_offsets(tok_off_in, n_query, query_n_vec, off, &nq_max));
+  const bool prune = (flags & MVR_PRUNE) != 0;
+  if (prune) {
+    if (!fp8 || !(flags & MVR_PREC_FP8))
+      return set_err(MVR_ERR_UNSUPPORTED, "MVR_PRUNE needs MVR_PREC_FP8 on a 2- or 4-bit index");
+    if (!h->prune_wts) return set_err(MVR_ERR_INVALID_ARG, "MVR_PRUNE: no pruner set");
+    if (nq_max > 32) return set_err(MVR_ERR_UNSUPPORTED, "MVR_PRUNE: queries of up to 32 tokens");
+  }
+  const uint32_t keep = prune ? std::min(h->prune_keep, probe_topk) : 0u;
   DeviceGuard g(h->device);
 
   const uint32_t B = h->batch_cap ? h->batch_cap : default_batch(h);
@@ -433,11 +499,18 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
       cand_need = std::max(cand_need, (size_t)T * probe_tc_cand_per_token(T, h->dix.n_centroid, h->n_sm, &tsp));
   }
   const uint32_t rank_stride = nq_max <= 32 ? 32u : 64u;
-  MVR_TRY(ensure_scratch(h, std::min(B, n_query), rank_stride));
+  // before the first search: about a third of a mean-length list's docs are
+  // new candidates (measured on the synthetic corpora)
+  const double cpe = h->cand_per_probe > 0.0
+                         ? h->cand_per_probe
+                         : 0.35 * (double)h->dix.n_ele_ivf / std::max(1u, h->dix.n_centroid);
+  const uint32_t parts_max = hash_parts(nq_max, nprobe, cpe);
+  MVR_TRY(ensure_scratch(h, std::min(B, n_query), rank_stride, parts_max * kHashFill));
   MVR_TRY(ensure_batch(h, std::min(B, n_query), tok_cap, nprobe, probe_topk, topk, part_need, R,
                        cand_need));
   MVR_TRY(ensure_call(h, 2 * ((size_t)n_query + n_batch), (size_t)n_query * 3,
                       (size_t)kStages * n_batch + 1));
+  if (prune) MVR_TRY(ensure_prune(h, std::min(B, n_query), probe_topk, keep));
   Workspace &w = h->ws;
 
   // stamp epochs this call takes (one per fallback chunk of every batch);
@@ -467,18 +540,20 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
     for (uint32_t i = s; i <= e; i++, pos++) {
       w.h_off[pos] = off[i] - off[s];
       w.h_off[n_off + pos] = cta;
-      if (i < e) cta += hash_parts((uint32_t)(off[i + 1] - off[i]), nprobe);
+      if (i < e) cta += hash_parts((uint32_t)(off[i + 1] - off[i]), nprobe, cpe);
     }
     n_cta[bt] = (uint32_t)cta;
   }
 
-  FilterScratch scr{w.stamp, w.rank, w.key, h->dix.n_item, w.rank_stride, w.qcnt, w.ovf, w.hkey};
+  FilterScratch scr{w.stamp, w.rank,   w.key,  h->dix.n_item, w.rank_stride,
+                    w.qcnt,  w.ovf,    w.hkey, w.key_stride};
   int launches = 0;
   uint64_t h2d = 2 * n_off * sizeof(uint64_t), d2h = 0;
   auto ev = [&](uint32_t bt, int k) { return h->events[(size_t)bt * kStages + k]; };
   // every device operation of the call, in stream order on `rs`
   // (events recorded while capturing become external event-record nodes)
   auto enqueue = [&](cudaStream_t rs, bool capturing) -> int {
+    if (prune) CUDA_TRY(cudaMemsetAsync(h->d_fallback, 0, sizeof(unsigned long long), rs));
     auto rec = [&](cudaEvent_t e) {
       return capturing ? cudaEventRecordWithFlags(e, rs, cudaEventRecordExternal)
                        : cudaEventRecord(e, rs);
@@ -521,23 +596,39 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
       float *os = host_io ? w.out_s : out_s + (size_t)s * topk;
       uint32_t *oi = host_io ? w.out_id : out_id + (size_t)s * topk;
       if (bf16) {
-        // tensor-core MaxSim (FP8 or BF16) over the whole shortlist, then the
-        // exact FP32 kernel re-scores its best R docs
+        // tensor-core MaxSim (FP8 or BF16) over the shortlist -- with
+        // MVR_PRUNE over the docs the pruner keeps -- then the exact FP32
+        // kernel re-scores its best R docs
+        const uint32_t *sid = w.short_id, *nsh = w.n_short;
+        if (prune) {
+          CUDA_TRY(launch_prune_features(h->dix, h->cen8, qp, qo, nb, w.short_id, w.n_short,
+                                         probe_topk, h->x_bound, w.feat, h->d_err, rs,
+                                         &launches, h->wait_ns));
+          CUDA_TRY(launch_prune_mlp(w.feat, w.n_short, nb, probe_topk, h->prune_wts,
+                                    h->prune_vecs, w.pred, h->d_err, h->n_sm, rs, &launches));
+          CUDA_TRY(launch_topk(w.short_id, w.pred, w.n_short, nb, probe_topk, keep, w.kept_s,
+                               w.kept_id, nullptr, rs, &launches));
+          CUDA_TRY(launch_prune_choose(h->dix, w.short_id, w.n_short, w.kept_id, w.kept_s, nb,
+                                       probe_topk, keep, R, h->prune_margin, w.fin_id, w.n_fin,
+                                       w.qstat + (size_t)s * 3, h->d_fallback, rs, &launches));
+          sid = w.fin_id;
+          nsh = w.n_fin;
+        }
         if (fp8)
-          CUDA_TRY(launch_rerank_tmem(h->dix, h->cen8, h->tw_fp8, qp, qo, nb, w.short_id,
-                                      w.n_short, probe_topk, sem, nq_max, h->x_bound, w.exact,
-                                      h->d_err, rs, &launches, true));
+          CUDA_TRY(launch_rerank_ws(h->dix, h->cen8, h->tw_fp8, qp, qo, nb, sid, nsh,
+                                    probe_topk, sem, nq_max, h->x_bound, w.exact, h->d_err, rs,
+                                    &launches, h->wait_ns, h->ws_docs));
         else if (h->cen_perm)
-          CUDA_TRY(launch_rerank_tmem(h->dix, h->cen_perm, h->tw_bf16, qp, qo, nb, w.short_id,
-                                      w.n_short, probe_topk, sem, nq_max, h->x_bound, w.exact,
+          CUDA_TRY(launch_rerank_tmem(h->dix, h->cen_perm, h->tw_bf16, qp, qo, nb, sid, nsh,
+                                      probe_topk, sem, nq_max, h->x_bound, w.exact,
                                       h->d_err, rs, &launches, false));
         else
           CUDA_TRY(launch_rerank_tc(h->dix, h->cen_bf16, h->lut_bf16, qp, qo, nb, w.short_id,
                                     w.n_short, probe_topk, sem, nq_max, w.exact, h->d_err, rs,
                                     &launches));
         CUDA_TRY(rec(ev(bt, 4)));
-        CUDA_TRY(launch_topk(w.short_id, w.exact, w.n_short, nb, probe_topk, R, w.r_score,
-                             w.r_id, w.n_r, rs, &launches));
+        CUDA_TRY(launch_topk(sid, w.exact, nsh, nb, probe_topk, R, w.r_score, w.r_id, w.n_r, rs,
+                             &launches));
         CUDA_TRY(launch_rerank(h->dix, qp, qo, nb, w.r_id, w.n_r, R, sem, w.r_exact, rs,
                                &launches));
         CUDA_TRY(launch_topk(w.r_id, w.r_exact, w.n_r, nb, R, topk, os, oi, nullptr, rs,
@@ -574,7 +665,7 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
     const bool same = G.exec && G.query == query && G.out_s == out_s && G.out_id == out_id &&
                       G.n_query == n_query && G.topk == topk && G.nprobe == nprobe &&
                       G.probe_topk == probe_topk && G.flags == flags && G.R == R && G.B == B &&
-                      G.gen == h->ws_gen && G.off == off;
+                      G.gen == h->ws_gen && G.off == off && G.cand_per_probe == cpe;
     CUDA_TRY(cudaEventRecord(h->ev_in, st));
     CUDA_TRY(cudaStreamWaitEvent(h->stream, h->ev_in, 0));
     if (!same) {
@@ -596,7 +687,7 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
       }
       G.query = query; G.out_s = out_s; G.out_id = out_id; G.n_query = n_query; G.topk = topk;
       G.nprobe = nprobe; G.probe_topk = probe_topk; G.flags = flags; G.R = R; G.B = B;
-      G.gen = h->ws_gen; G.off = off; G.launches = launches;
+      G.gen = h->ws_gen; G.off = off; G.launches = launches; G.cand_per_probe = cpe;
     }
     launches = G.launches;
     CUDA_TRY(cudaEventRecord(h->ev_g0, h->stream));
@@ -608,13 +699,26 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
   CUDA_TRY(cudaMemcpyAsync(w.h_qstat, w.qstat, (size_t)n_query * 3 * sizeof(uint32_t),
                            cudaMemcpyDeviceToHost, st));
   unsigned herr = 0;
+  unsigned long long n_fallback = 0;
   if (bf16) CUDA_TRY(cudaMemcpyAsync(&herr, h->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+  if (prune)
+    CUDA_TRY(cudaMemcpyAsync(&n_fallback, h->d_fallback, sizeof(n_fallback), cudaMemcpyDeviceToHost,
+                             st));
   CUDA_TRY(cudaStreamSynchronize(st));
   CUDA_TRY(cudaGetLastError());
   if (herr) {
     CUDA_TRY(cudaMemset(h->d_err, 0, sizeof(unsigned)));
     return set_err(MVR_ERR_CUDA, "tensor-core %s: a completion wait timed out",
-                   (herr & 2u) ? "centroid scoring" : "rerank");
+                   (herr & 2u) ? "centroid scoring" : (herr & 8u) ? "pruner MLP" : "rerank");
+  }
+
+  {  // candidates per probed list, sizing the next call's hash filter
+    double r = 0.0;
+    for (uint32_t i = 0; i < n_query; i++) {
+      const uint64_t probes = (off[i + 1] - off[i]) * (uint64_t)nprobe;
+      if (probes) r = std::max(r, (double)w.h_qstat[i * 3 + 0] / (double)probes);
+    }
+    if (r > 0.0) h->cand_per_probe = r;
   }
 
   float total_ms = 0.f, max_ms = 0.f;
@@ -661,6 +765,7 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
       stats->n_rerank_tok += w.h_qstat[i * 3 + 2];
     }
     for (int k = 0; k < kStages; k++) stats->stage_ms[k] = stage_tot[k];
+    stats->n_prune_fallback = n_fallback;
     stats->wall_s =
         std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
   }
@@ -709,7 +814,9 @@ int finish_index(mvr_index *h, const uint32_t *item_n_vec_host, const uint32_t *
   }
   if (fp8_rerank_supported(d.n_bit)) {
     uint8_t *c8;
-    MVR_TRY(dalloc(&c8, (size_t)d.n_centroid * kDim, &h->bufs));
+    // one zero row past the last centroid: the FP8 rerank's padding rows
+    MVR_TRY(dalloc(&c8, (size_t)(d.n_centroid + 1) * kDim, &h->bufs));
+    CUDA_TRY(cudaMemsetAsync(c8 + (size_t)d.n_centroid * kDim, 0, kDim, h->stream));
     CUDA_TRY(make_centroid_fp8(d.centroid, d.n_centroid, d.n_bit, c8, h->stream));
     h->cen8 = c8;
     h->tw_fp8 = make_tm_weights(d.n_bit, weight, true);
@@ -782,9 +889,11 @@ int new_handle(int device, std::unique_ptr<mvr_index> &h) {
 }
 
 template <class T>
-int upload(const T *src, size_t n, T **dst, std::vector<void *> &owner, cudaMemcpyKind kind) {
-  MVR_TRY(dalloc(dst, n, &owner));
+int upload(const T *src, size_t n, T **dst, std::vector<void *> &owner, cudaMemcpyKind kind,
+           size_t pad = 0) {
+  MVR_TRY(dalloc(dst, n + pad, &owner));
   if (n) CUDA_TRY(cudaMemcpy(*dst, src, n * sizeof(T), kind));
+  if (pad) CUDA_TRY(cudaMemset(*dst + n, 0, pad * sizeof(T)));
   return MVR_OK;
 }
 
@@ -835,7 +944,9 @@ int from_arrays_impl(const uint32_t *item_n_vec_l, uint32_t n_item, const float 
   uint8_t *res;
   uint64_t *doff, *dioff;
   MVR_TRY(upload(centroid_l, (size_t)n_centroid * kDim, &cen, h->bufs, kind));
-  MVR_TRY(upload(vq_code_l, (size_t)n_vec, &code, h->bufs, kind));
+  // 16 zero bytes past the codes: the FP8 rerank copies each doc group's
+  // codes in 16-byte-aligned bulk copies that may round up past the last one
+  MVR_TRY(upload(vq_code_l, (size_t)n_vec, &code, h->bufs, kind, 4));
   MVR_TRY(upload(residual_code_l, (size_t)n_vec * d.bytes_per_vec, &res, h->bufs, kind));
   MVR_TRY(upload(inv.data(), n_item, &dinv, h->bufs, cudaMemcpyHostToDevice));
   MVR_TRY(upload(item_off.data(), n_item, &doff, h->bufs, cudaMemcpyHostToDevice));
@@ -1013,6 +1124,56 @@ int mvr_index_set_graphs(mvr_index *h, int enable) {
   return MVR_OK;
 }
 
+int mvr_index_set_pruner(mvr_index *h, const float *params, uint32_t keep, float margin) {
+  if (!h) return set_err(MVR_ERR_INVALID_ARG, "null index handle");
+  DeviceGuard g(h->device);
+  h->drop_graph();
+  if (!params) {
+    dfree(h->prune_wts);
+    dfree(h->prune_vecs);
+    h->prune_wts = nullptr;
+    h->prune_vecs = nullptr;
+    return MVR_OK;
+  }
+  if (keep == 0) return set_err(MVR_ERR_INVALID_ARG, "keep must be >= 1");
+  if (!fp8_rerank_supported(h->dix.n_bit))
+    return set_err(MVR_ERR_UNSUPPORTED, "the pruner's features need a 2- or 4-bit index");
+  if (!h->prune_wts) {
+    MVR_TRY(dalloc(&h->prune_wts, prune_weight_bytes()));
+    MVR_TRY(dalloc(&h->prune_vecs, 769));
+  }
+  if (!h->d_fallback) MVR_TRY(dalloc(&h->d_fallback, 1));
+  float *tmp = nullptr;
+  MVR_TRY(dalloc(&tmp, kNumParams));
+  cudaError_t e = cudaMemcpy(tmp, params, kNumParams * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = prune_prepare(tmp, h->prune_wts, h->prune_vecs, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  dfree(tmp);
+  CUDA_TRY(e);
+  h->prune_keep = keep;
+  h->prune_margin = margin;
+  return MVR_OK;
+}
+
+int mvr_index_set_rerank_tile(mvr_index *h, uint32_t docs_per_cta) {
+  if (!h) return set_err(MVR_ERR_INVALID_ARG, "null index handle");
+  if (docs_per_cta == 0) docs_per_cta = 64;
+  if (!ws_docs_supported(docs_per_cta))
+    return set_err(MVR_ERR_INVALID_ARG, "docs per CTA %u: 32, 64 or 128", docs_per_cta);
+  DeviceGuard g(h->device);
+  h->ws_docs = docs_per_cta;
+  h->drop_graph();
+  return MVR_OK;
+}
+
+int mvr_index_set_wait_limit(mvr_index *h, uint64_t wait_ns) {
+  if (!h) return set_err(MVR_ERR_INVALID_ARG, "null index handle");
+  DeviceGuard g(h->device);
+  h->wait_ns = wait_ns ? wait_ns : 1000000000ull;
+  h->drop_graph();  // recorded launches carry the old bound
+  return MVR_OK;
+}
+
 int mvr_index_set_rescore(mvr_index *h, uint32_t n_rescore) {
   if (!h) return set_err(MVR_ERR_INVALID_ARG, "null index handle");
   h->rescore = n_rescore;
@@ -1053,6 +1214,11 @@ int mvr_search_trace(mvr_index *h, const float *query, uint32_t nq, uint32_t top
                      uint32_t nprobe, uint32_t probe_topk, uint32_t flags, mvr_trace *tr) {
   if (!h || !query || !tr) return set_err(MVR_ERR_INVALID_ARG, "null argument");
   if (!tr->topk_score || !tr->topk_id) return set_err(MVR_ERR_INVALID_ARG, "null trace result buffer");
+  if (flags & MVR_PRUNE)
+    return set_err(MVR_ERR_UNSUPPORTED, "trace the pruner through short_pred, not MVR_PRUNE");
+  if ((tr->short_feat || tr->short_pred) && (!h->cen8 || nq > 32))
+    return set_err(MVR_ERR_UNSUPPORTED, "pruner features: a 2- or 4-bit index, <= 32 tokens");
+  if (tr->short_pred && !h->prune_wts) return set_err(MVR_ERR_INVALID_ARG, "no pruner set");
   MVR_TRY(search_impl(h, query, nullptr, 1, nq, topk, nprobe, probe_topk, flags, tr->topk_score,
                       tr->topk_id, nullptr, nullptr, nullptr, h->stream, true));
   DeviceGuard g(h->device);
@@ -1096,6 +1262,38 @@ int mvr_search_trace(mvr_index *h, const float *query, uint32_t nq, uint32_t top
     if (tr->short_id) tr->short_id[i] = sid[ord[i]];
     if (tr->short_approx) tr->short_approx[i] = sa[ord[i]];
     if (tr->short_exact) tr->short_exact[i] = se[ord[i]];
+  }
+  if ((tr->short_feat || tr->short_pred) && n_short) {
+    // the shortlist's pruner features (and predictions), as the search
+    // computes them
+    float *d_feat = nullptr, *d_pred = nullptr;
+    int l = 0;
+    MVR_TRY(dalloc(&d_feat, (size_t)probe_topk * 33));
+    MVR_TRY(dalloc(&d_pred, probe_topk));
+    std::vector<float> f((size_t)n_short * 33), p(n_short);
+    cudaError_t e = launch_prune_features(h->dix, h->cen8, w.q, w.q_off, 1, w.short_id, w.n_short,
+                                          probe_topk, h->x_bound, d_feat, h->d_err, h->stream, &l,
+                                          h->wait_ns);
+    if (e == cudaSuccess && tr->short_pred)
+      e = launch_prune_mlp(d_feat, w.n_short, 1, probe_topk, h->prune_wts, h->prune_vecs, d_pred,
+                           h->d_err, h->n_sm, h->stream, &l);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e == cudaSuccess) e = cudaMemcpy(f.data(), d_feat, f.size() * 4, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(p.data(), d_pred, p.size() * 4, cudaMemcpyDeviceToHost);
+    unsigned herr = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(&herr, h->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost);
+    dfree(d_feat);
+    dfree(d_pred);
+    CUDA_TRY(e);
+    if (herr) {
+      CUDA_TRY(cudaMemset(h->d_err, 0, sizeof(unsigned)));
+      return set_err(MVR_ERR_CUDA, "pruner features: a completion wait timed out");
+    }
+    for (uint32_t i = 0; i < n_short; i++) {
+      if (tr->short_feat)
+        std::memcpy(tr->short_feat + (size_t)i * 33, f.data() + (size_t)ord[i] * 33, 33 * 4);
+      if (tr->short_pred) tr->short_pred[i] = p[ord[i]];
+    }
   }
   return MVR_OK;
 }
@@ -1254,6 +1452,30 @@ int mvr_kmeans_accumulate_device(const float *d_vec, uint64_t n_vec, uint32_t di
   if (!d_vec || !d_code || !d_sum || !d_count) return set_err(MVR_ERR_INVALID_ARG, "null argument");
   cudaStream_t st = (cudaStream_t)cuda_stream;
   CUDA_TRY(launch_kmeans_accumulate(d_vec, n_vec, d_code, d_sum, d_count, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  return MVR_OK;
+}
+
+size_t mvr_mlp_work_floats(uint32_t n) { return mlp_work_floats(n); }
+
+int mvr_mlp_train_step(const float *d_x, const float *d_y, uint32_t n, float *d_params,
+                       float *d_adam_m, float *d_adam_v, float *d_work, float lr, uint32_t step,
+                       float *d_loss, void *cuda_stream) {
+  if (!d_x || !d_y || !d_params || !d_adam_m || !d_adam_v || !d_work)
+    return set_err(MVR_ERR_INVALID_ARG, "null argument");
+  if (n == 0 || step == 0) return set_err(MVR_ERR_INVALID_ARG, "empty minibatch or step 0");
+  cudaStream_t st = (cudaStream_t)cuda_stream;
+  CUDA_TRY(mlp_train_step(d_x, d_y, n, d_params, d_adam_m, d_adam_v, d_work, lr, step, d_loss, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  return MVR_OK;
+}
+
+int mvr_mlp_forward(const float *d_x, uint32_t n, const float *d_params, float *d_work,
+                    float *d_out, void *cuda_stream) {
+  if (!d_x || !d_params || !d_work || !d_out) return set_err(MVR_ERR_INVALID_ARG, "null argument");
+  if (n == 0) return MVR_OK;
+  cudaStream_t st = (cudaStream_t)cuda_stream;
+  CUDA_TRY(mlp_forward_ref(d_x, n, d_params, d_work, d_out, st));
   CUDA_TRY(cudaStreamSynchronize(st));
   return MVR_OK;
 }

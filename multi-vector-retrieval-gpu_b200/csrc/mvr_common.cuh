@@ -12,7 +12,7 @@ constexpr int kMaxQueryTok = 64;   // query tokens per query
 constexpr int kMaxProbe = 32;      // nprobe upper bound
 constexpr int kMaxShort = 8192;    // probe_topk upper bound
 constexpr int kMaxTopk = 1024;
-constexpr int kHashParts = 16;     // doc ranges of the hash filter's partition table (max CTAs per query)
+constexpr int kHashParts = 64;     // doc ranges of the hash filter's partition table (max CTAs per query)
 
 // Index arrays resident in HBM (one copy per loaded index).
 struct DevIndex {

@@ -551,7 +551,7 @@ filter_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
 }
 
 // ---------------------------------------------------------------------
-// Hash-table filter (main search path).  P = hash_parts(nq, nprobe) CTAs
+// Hash-table filter (main search path).  P = hash_parts(...) CTAs
 // share a query; CTA p owns the docs [p * n_item / P, (p + 1) * n_item / P) and keeps one
 // shared-memory hash-table slot per candidate doc of its range: doc id, the
 // mask of query tokens that have visited it and the exact fixed-point sum of
@@ -677,7 +677,7 @@ filter_hash_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
   __syncthreads();
 
   // emit this CTA's candidates as (score, id) keys (at most kHashFill per CTA)
-  uint64_t *key = scr.hkey + (size_t)b * kHashKeys;
+  uint64_t *key = scr.hkey + (size_t)b * scr.key_stride;
   for (uint32_t s0 = 0; s0 < kHashCap; s0 += blockDim.x) {
     const uint32_t sl = s0 + tid;
     const uint32_t k = sl < kHashCap ? tkey[sl] : kEmpty;
@@ -739,7 +739,7 @@ filter_select_kernel(DevIndex ix, uint32_t probe_topk, FilterScratch scr,
   if (threadIdx.x == 0) { s_sel = 0; s_stok = 0; }
   __syncthreads();
   SelectSmem sm{hist, &s_digit, &s_need, &s_done};
-  select_emit<1>(ix, scr.hkey + (size_t)b * kHashKeys, n_cand, probe_topk, b, 0, sm, &s_sel,
+  select_emit<1>(ix, scr.hkey + (size_t)b * scr.key_stride, n_cand, probe_topk, b, 0, sm, &s_sel,
                  &s_stok, short_id, short_approx);
   __syncthreads();
   if (threadIdx.x == 0) {

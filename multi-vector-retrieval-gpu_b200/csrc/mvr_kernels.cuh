@@ -15,20 +15,28 @@ struct FilterScratch {
   uint32_t rank_stride;  // 32 or 64 (>= query tokens, multiple of 16)
   uint32_t *qcnt;        // [slots] candidate keys emitted by the hash filter (0 between batches)
   uint32_t *ovf;         // [slots] 1: the hash filter overflowed
-  uint64_t *hkey;        // [slots][kHashKeys] hash-filter candidate keys
+  uint64_t *hkey;        // [slots][key_stride] hash-filter candidate keys
+  uint32_t key_stride;   // keys per query slot: kHashFill * the largest range count in use
 };
 
 // Candidate keys one query can hold in the hash filter: every doc range
 // stops inserting at kHashFill candidates, beyond which the query overflows.
 constexpr uint32_t kHashFill = 7168u;
-constexpr uint32_t kHashKeys = (uint32_t)kHashParts * kHashFill;
 
-// Doc ranges (CTAs) of one query in the hash filter: 8, or 16 when the
-// query probes more than 256 lists (nq * nprobe), whose candidate sets
-// outgrow 8 * kHashFill.  Each range is a union of kHashParts / P
-// consecutive ranges of the partition table.
-inline uint32_t hash_parts(uint32_t nq, uint32_t nprobe) {
-  return (uint64_t)nq * nprobe > 256u ? 16u : 8u;
+// Doc ranges (CTAs) of one query in the hash filter, a power of two in
+// [8, kHashParts]: enough that the expected candidate count, nq * nprobe *
+// cand_per_probe, fills each range's hash table to at most 85 % of
+// kHashFill (candidates spread evenly over the doc ranges, up to a few
+// percent).  cand_per_probe: the largest candidates per probed list seen in
+// the handle's previous search (docs listed under several probes count
+// once), or an estimate from the index's mean list length before the first.
+// Each range is a union of kHashParts / P consecutive ranges of the
+// partition table.
+inline uint32_t hash_parts(uint32_t nq, uint32_t nprobe, double cand_per_probe) {
+  const double cand = (double)nq * nprobe * cand_per_probe;
+  uint32_t p = 8;
+  while (p < (uint32_t)kHashParts && cand > 0.85 * kHashFill * p) p *= 2;
+  return p;
 }
 
 cudaError_t configure_kernels();

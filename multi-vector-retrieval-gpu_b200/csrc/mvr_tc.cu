@@ -64,7 +64,8 @@ __device__ __forceinline__ uint64_t global_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
   return t;
 }
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity,
+                                          uint64_t limit_ns = kWaitNs) {
   const uint32_t a = smem_u32(bar);
   uint64_t t0 = 0;
   for (uint32_t i = 0;; i++) {
@@ -77,7 +78,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
         : "memory");
     if (done) return true;
     if (i == 0) t0 = global_ns();
-    else if (global_ns() - t0 > kWaitNs) return false;
+    else if (global_ns() - t0 > limit_ns) return false;
   }
 }
 
@@ -1248,6 +1249,755 @@ cudaError_t launch_probe_tc(const float *q, uint32_t n_tok, const void *cen_sw, 
 }
 
 // BF16 tables: centroid rows and the byte -> per-value weight table.
+// ---------------------------------------------------------------------
+// rerank_ws_kernel<NBIT, NMAX, FEAT, DOCS>: the FP8 (E4M3) MaxSim of the
+// mixed-precision path for 2- and 4-bit codes, warp-specialised over a
+// shared-memory ring.
+//
+// The rows of the MMA tiles are doc-aligned groups: doc d of the CTA's chunk
+// of the shortlist (DOCS docs) takes ceil(L_d / 32) groups of 32 rows (its
+// tokens 32j .. 32j + 31; the rows past its last token are padding), groups
+// are numbered doc after doc, tile i holds groups 4i .. 4i + 3, and group
+// 4i + q sits in TMEM lane quadrant q.  Roles of the 320 threads:
+//  warp 0     producer: per tile, two 1-D bulk copies per group
+//             (cp.async.bulk, completion by mbarrier transaction count): the
+//             group's residual bytes and its vq codes (the latter rounded out
+//             to 16-byte boundaries) into stage i % kWsStages of the ring;
+//  warps 2-5  decoders, one thread per row: the row's code from the ring,
+//             its E4M3 centroid row from L2 (loaded one tile ahead), a
+//             tcgen05.st of that row (A_c), the residual bytes from the ring
+//             expanded by PRMT into E4M3 bucket weights (as
+//             rerank_tmem_kernel's FP8 decode), a tcgen05.st of those (A_r);
+//             padding rows store zeros;
+//  warp 1     MMA: one thread issues 4 K-steps x 2 tcgen05.mma (kind::f8f6f4,
+//             M = 128, N = NMAX, K = 32) per tile, A_c and A_r from TMEM and
+//             the query tile B from shared memory, accumulating both into the
+//             tile's D stage; commits release the A stage and hand D to the
+//             epilogue;
+//  warps 6-9  epilogue, one warp per group: tcgen05.ld of its 32 rows,
+//             re-arms the D stage for the tile kWsDStages later, and takes the
+//             max over the group's rows of each query-token column with one
+//             full-warp REDUX.MAX, folded into the per-(doc, query token)
+//             maxima by shared-memory atomicMax.
+// A D stage starts at OFF (a power of two above |q.x| for every pair of the
+// CTA, as in rerank_tmem_kernel) in real rows and at 0 in padding rows (whose
+// A rows are zero), so every D value is a non-negative float ordered like its
+// bit pattern, and padding never wins a max.  With FEAT the kernel computes
+// the learned pruner's features instead: the centroid part only (no residual
+// copies, decode or MMA), and per doc the maxima themselves (per query token
+// the best centroid score over the doc's tokens) plus log(doc length).
+// Every pipeline mbarrier wait is bounded (wait_ns, 1 s by default); on a
+// timeout the CTA records the error and every role stops; the producer then
+// waits (1 s bound) for its bulk copies still in flight and the MMA thread
+// for its MMAs before TMEM is freed.
+// ---------------------------------------------------------------------
+constexpr int kWsDocs = 64;          // shortlisted docs per CTA (default; 32, 64 or 128)
+constexpr int kWsStages = 4;         // shared-memory ring stages (one tile each)
+constexpr int kWsDStages = 4;        // D stages in TMEM
+constexpr int kWsThreads = 320;
+constexpr uint32_t kWsCodeSlot = 160;  // ring bytes per group for codes: 32 x 4 + alignment slack
+
+__host__ __device__ constexpr int ws_astages(int nmax) { return nmax <= 32 ? 2 : 4; }
+__host__ __device__ constexpr uint32_t ws_cols(int nmax) { return nmax <= 32 ? 256u : 512u; }
+__host__ __device__ constexpr uint32_t ws_stage_bytes(int nbit) {
+  return 128u * (128u * nbit / 8u) + 4u * kWsCodeSlot;
+}
+// dynamic shared memory: 1 KB alignment slack + query tile + ring; the wide
+// (NMAX = 64) variant asks for more than half an SM's shared memory so that
+// one CTA holds the SM's 512 TMEM columns alone
+__host__ __device__ constexpr size_t ws_smem_bytes(int nbit, int nmax) {
+  return nmax <= 32 ? 1024 + (size_t)nmax * 128 + kWsStages * (size_t)ws_stage_bytes(nbit)
+                    : 120 * 1024;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+// 1-D bulk copy global -> shared (16-byte aligned addresses, size a multiple
+// of 16), completing on the mbarrier's transaction count
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes,
+                                         uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+          dst),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+      "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};\n" ::"r"(taddr),
+      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]),
+      "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]),
+      "r"(r[15]), "r"(r[16]), "r"(r[17]), "r"(r[18]), "r"(r[19]), "r"(r[20]), "r"(r[21]),
+      "r"(r[22]), "r"(r[23]), "r"(r[24]), "r"(r[25]), "r"(r[26]), "r"(r[27]), "r"(r[28]),
+      "r"(r[29]), "r"(r[30]), "r"(r[31])
+      : "memory");
+}
+__device__ __forceinline__ void tmem_fill32(uint32_t taddr, uint32_t x) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,"
+      "%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};\n" ::"r"(taddr),
+      "r"(x)
+      : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() {
+  asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory");
+}
+
+// Position in the CTA's group sequence: doc d (of the chunk), its group j.
+struct WsCursor {
+  uint32_t d, j;
+};
+__device__ __forceinline__ void ws_advance(WsCursor &c, uint32_t k, const uint16_t *ng,
+                                           uint32_t nd) {
+  c.j += k;
+  while (c.d < nd && c.j >= ng[c.d]) {
+    c.j -= ng[c.d];
+    c.d++;
+  }
+}
+// rows of the group at c (0 past the last group)
+__device__ __forceinline__ uint32_t ws_rows(const WsCursor &c, const uint32_t *len, uint32_t nd) {
+  return c.d < nd ? min(32u, len[c.d] - 32u * c.j) : 0u;
+}
+
+template <int NBIT, int NMAX, bool FEAT = false, int DOCS = kWsDocs>
+__global__ void __launch_bounds__(kWsThreads, NMAX <= 32 ? 2 : 1)
+rerank_ws_kernel(DevIndex ix, const uint8_t *__restrict__ cen8, TmWeights tw,
+                 const float *__restrict__ q, const uint64_t *__restrict__ q_off,
+                 const uint32_t *__restrict__ short_id, const uint32_t *__restrict__ n_short,
+                 uint32_t probe_topk, int semantics, float x_bound, float *__restrict__ approx,
+                 unsigned *__restrict__ err, uint64_t wait_ns) {
+  static_assert(NBIT == 2 || NBIT == 4, "FP8 decode of 2- and 4-bit codes");
+  static_assert(NMAX == 32 || NMAX == 64, "query tiles of 32 or 64 rows");
+  static_assert(!FEAT || NMAX == 32, "pruner features: queries of up to 32 tokens");
+  static_assert(DOCS == 32 || DOCS == 64 || DOCS == 128, "docs per CTA");
+  constexpr int S = kWsStages, SA = ws_astages(NMAX), SD = kWsDStages;
+  constexpr uint32_t BPV = 128u * NBIT / 8u;       // residual bytes per token
+  constexpr uint32_t RES_STAGE = 128u * BPV;
+  constexpr uint32_t STAGE = ws_stage_bytes(NBIT);
+  constexpr uint32_t COLS = ws_cols(NMAX);
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint8_t *Bq = smem;                   // [NMAX rows][128 B] E4M3, SW128, K-major
+  uint8_t *ring = smem + NMAX * 128;    // [S][STAGE]: residual rows, then 4 code slots
+  __shared__ uint32_t best[DOCS * NMAX];  // [doc][query token]: bits of OFF + max
+  __shared__ uint32_t s_qss, s_groups, tmem_base_s;
+  __shared__ float s_qinv[NMAX];
+  __shared__ uint64_t full[S], sfree[S], afull[SA], afree[SA], dfull[SD], dempty[SD], mdone;
+  __shared__ uint32_t d_len[DOCS];
+  __shared__ uint16_t d_ng[DOCS];
+  __shared__ uint64_t d_off[DOCS];
+  __shared__ volatile int s_abort;
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t b = blockIdx.y;
+  const uint32_t ns = n_short[b];
+  const uint32_t d0 = blockIdx.x * DOCS;
+  const uint64_t tok0 = q_off[b];
+  const uint32_t nq = (uint32_t)(q_off[b + 1] - tok0);
+  // uniform exits before any TMEM or barrier use: no docs here, or the query
+  // belongs to the other width's launch
+  if (d0 >= ns || (nq > 32) != (NMAX > 32)) return;
+  const uint32_t nd = min((uint32_t)DOCS, ns - d0);
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     smem_u32(&tmem_base_s)),
+                 "r"(COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  if (tid == 0) {
+    for (int s = 0; s < S; s++) { mbar_init(&full[s], 1); mbar_init(&sfree[s], 4); }
+    for (int s = 0; s < SA; s++) { mbar_init(&afull[s], 4); mbar_init(&afree[s], 1); }
+    for (int s = 0; s < SD; s++) { mbar_init(&dfull[s], 1); mbar_init(&dempty[s], 4); }
+    mbar_init(&mdone, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    s_abort = 0;
+    s_qss = 0;
+    s_groups = 0;
+  }
+  if (tid < (int)nd) {
+    const uint32_t it = short_id[(size_t)b * probe_topk + d0 + tid];
+    const uint32_t L = ix.item_n_vec[it];
+    d_len[tid] = L;
+    d_off[tid] = ix.item_off[it];
+    d_ng[tid] = (uint16_t)((L + 31u) / 32u);
+  }
+  for (int i = tid; i < DOCS * NMAX; i += kWsThreads) best[i] = 0u;
+  __syncthreads();
+  if (tid < (int)nd) atomicAdd(&s_groups, (uint32_t)d_ng[tid]);
+  // query tokens -> B (E4M3, per-token power-of-two scales, FP8 K order,
+  // swizzled, rows >= nq zero): 8 lanes per row, 16 positions each
+  for (int i = tid; i < NMAX * 8; i += kWsThreads) {
+    const int row = i >> 3, ch = i & 7;
+    float x[16];
+    float amax = 0.0f, ss = 0.0f;
+#pragma unroll
+    for (int u = 0; u < 16; u++) {
+      x[u] = (uint32_t)row < nq ? __ldg(q + (tok0 + row) * kDim + fp8_dim_of<NBIT>(16 * ch + u))
+                                : 0.0f;
+      amax = fmaxf(amax, fabsf(x[u]));
+      ss = fmaf(x[u], x[u], ss);
+    }
+#pragma unroll
+    for (int o = 4; o > 0; o >>= 1) {
+      amax = fmaxf(amax, __shfl_xor_sync(kFull, amax, o));
+      ss += __shfl_xor_sync(kFull, ss, o);
+    }
+    const float sc = amax > 0.0f ? exp2f(floorf(log2f(224.0f / amax))) : 1.0f;
+    uint32_t v[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const __nv_fp8x2_storage_t lo = __nv_cvt_float2_to_fp8x2(
+          make_float2(x[4 * u] * sc, x[4 * u + 1] * sc), __NV_SATFINITE, __NV_E4M3);
+      const __nv_fp8x2_storage_t hi = __nv_cvt_float2_to_fp8x2(
+          make_float2(x[4 * u + 2] * sc, x[4 * u + 3] * sc), __NV_SATFINITE, __NV_E4M3);
+      v[u] = (uint32_t)lo | ((uint32_t)hi << 16);
+    }
+    *reinterpret_cast<uint4 *>(Bq + sw128_off(row, ch)) = make_uint4(v[0], v[1], v[2], v[3]);
+    if ((lane & 7) == 0) {
+      atomicMax(&s_qss, __float_as_uint(ss * sc * sc));
+      s_qinv[row] = 1.0f / sc;
+    }
+  }
+  __syncthreads();
+  const uint32_t tmem = tmem_base_s;
+  const uint32_t n_tiles = (s_groups + 3u) / 4u;
+  const float off = fmaxf(1.0f, exp2f(ceilf(log2f(sqrtf(__uint_as_float(s_qss)) * x_bound * 1.15f +
+                                                  1e-30f))));
+  const uint32_t off_bits = __float_as_uint(off);
+  const uint32_t qd = warp & 3;  // TMEM lane quadrant of this warp
+  const uint32_t lane_off = (32u * qd) << 16;
+  const uint32_t dbase = tmem + 64u * SA;  // D stages after the A stages
+
+  if (warp >= 6) {  // epilogue warps arm the D stages of tiles 0 .. SD-1
+    WsCursor c{0, 0};
+    ws_advance(c, qd, d_ng, nd);
+    for (int sd = 0; sd < SD; sd++) {
+      const uint32_t x = (uint32_t)lane < ws_rows(c, d_len, nd) ? off_bits : 0u;
+#pragma unroll
+      for (int h = 0; h < NMAX / 32; h++) tmem_fill32(dbase + lane_off + NMAX * sd + 32 * h, x);
+      ws_advance(c, 4, d_ng, nd);
+    }
+    tmem_wait_st();
+  }
+  fence_async_smem();  // B tile (generic stores) before the MMAs read it
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+
+  if (warp == 0) {
+    // ---------------- producer ----------------
+    WsCursor c{0, 0};
+    ws_advance(c, (uint32_t)min(lane, 3), d_ng, nd);  // lane g < 4: group 4i + g
+    const uint32_t ring_u32 = smem_u32(ring);
+    uint32_t issued = 0;
+    bool ok = true;
+    for (uint32_t i = 0; i < n_tiles; i++) {
+      const uint32_t s = i % S;
+      if (i >= (uint32_t)S &&
+          !__all_sync(kFull, mbar_wait(&sfree[s], ((i / S) + 1) & 1, wait_ns))) {
+        ok = false;
+        break;
+      }
+      uint32_t rb = 0, cb = 0;
+      const uint8_t *rsrc = nullptr, *csrc = nullptr;
+      if (lane < 4 && c.d < nd) {
+        const uint32_t cnt = min(32u, d_len[c.d] - 32u * c.j);
+        const uint64_t v = d_off[c.d] + 32ull * c.j;
+        rb = FEAT ? 0u : cnt * BPV;
+        rsrc = ix.residual + v * BPV;
+        const uintptr_t a = (uintptr_t)(ix.vq_code + v);
+        const uintptr_t a0 = a & ~(uintptr_t)15, a1 = (a + 4u * cnt + 15u) & ~(uintptr_t)15;
+        cb = (uint32_t)(a1 - a0);
+        csrc = reinterpret_cast<const uint8_t *>(a0);
+      }
+      uint32_t tot = rb + cb;
+      tot += __shfl_xor_sync(kFull, tot, 1);
+      tot += __shfl_xor_sync(kFull, tot, 2);
+      if (lane == 0) mbar_expect_tx(&full[s], tot);
+      __syncwarp();
+      if (cb) {
+        if (rb) bulk_g2s(ring_u32 + s * STAGE + lane * 32u * BPV, rsrc, rb, &full[s]);
+        bulk_g2s(ring_u32 + s * STAGE + RES_STAGE + lane * kWsCodeSlot, csrc, cb, &full[s]);
+      }
+      ws_advance(c, 4, d_ng, nd);
+      issued = i + 1;
+      if (s_abort) {
+        ok = false;
+        break;
+      }
+    }
+    if (!ok) {
+      if (lane == 0) {
+        atomicOr(err, 4u);
+        s_abort = 1;
+      }
+      // the copies still in flight land before the CTA may exit
+      for (uint32_t i = issued > (uint32_t)S ? issued - S : 0; i < issued; i++)
+        mbar_wait(&full[i % S], (i / S) & 1);
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issue ----------------
+    if (lane == 0) {
+      const uint32_t idesc = idesc_e4m3(128, NMAX);
+      const uint32_t b_base = smem_u32(Bq);
+      uint32_t i = 0;
+      for (; i < n_tiles; i++) {
+        const uint32_t sa = i % SA, sd = i % SD;
+        if (!mbar_wait(&afull[sa], (i / SA) & 1, wait_ns)) break;
+        if (i >= (uint32_t)SD && !mbar_wait(&dempty[sd], ((i / SD) + 1) & 1, wait_ns)) break;
+        tc_fence_after();
+        const uint32_t dcol = dbase + NMAX * sd;
+#pragma unroll
+        for (int kk = 0; kk < 4; kk++) {  // K = 32 per MMA: centroid part, residual part
+          const uint64_t bd = sw128_desc(b_base + kk * 32);
+          mma_e4m3_ta(dcol, tmem + 64u * sa + 8u * kk, bd, idesc);
+          if constexpr (!FEAT) mma_e4m3_ta(dcol, tmem + 64u * sa + 32u + 8u * kk, bd, idesc);
+        }
+        mma_commit(&dfull[sd]);
+        mma_commit(&afree[sa]);
+        if (s_abort) {
+          i++;
+          break;
+        }
+      }
+      if (i < n_tiles || s_abort) {
+        atomicOr(err, 4u);
+        s_abort = 1;
+      }
+      mma_commit(&mdone);  // every MMA of this CTA has completed once this phase does
+      mbar_wait(&mdone, 0);
+    }
+    __syncwarp();
+  } else if (warp < 6) {
+    // ---------------- decoders ----------------
+    WsCursor c{0, 0};
+    ws_advance(c, qd, d_ng, nd);
+    uint32_t cen[32];
+    // the code of this row in tile i (cursor cc) and its centroid row: the
+    // zero row (index n_centroid) for padding rows
+    auto fetch = [&](uint32_t i, const WsCursor &cc) -> bool {
+      const uint32_t s = i % S;
+      if (!mbar_wait(&full[s], (i / S) & 1, wait_ns)) return false;
+      uint32_t code = ix.n_centroid;
+      if ((uint32_t)lane < ws_rows(cc, d_len, nd)) {
+        const uint64_t v = d_off[cc.d] + 32ull * cc.j;
+        const uint32_t shift = (uint32_t)((uintptr_t)(ix.vq_code + v) & 15u);
+        code = *reinterpret_cast<const uint32_t *>(ring + s * STAGE + RES_STAGE + qd * kWsCodeSlot +
+                                                   shift + 4u * lane);
+      }
+      const uint4 *cp = reinterpret_cast<const uint4 *>(cen8 + (size_t)code * kDim);
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const uint4 t = __ldg(cp + u);
+        cen[4 * u] = t.x;
+        cen[4 * u + 1] = t.y;
+        cen[4 * u + 2] = t.z;
+        cen[4 * u + 3] = t.w;
+      }
+      return true;
+    };
+    bool ok = n_tiles == 0 || fetch(0, c);
+    for (uint32_t i = 0; ok && i < n_tiles; i++) {
+      const uint32_t s = i % S, sa = i % SA;
+      const bool valid = (uint32_t)lane < ws_rows(c, d_len, nd);
+      (void)valid;
+      if (i >= (uint32_t)SA && !mbar_wait(&afree[sa], ((i / SA) + 1) & 1, wait_ns)) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t acol = tmem + lane_off + 64u * sa;
+      tmem_st32(acol, cen);  // A_c: the centroid row as loaded
+      tmem_wait_st();
+      // this row's residual words (tile i), then the next tile's centroid row
+      uint32_t res[BPV / 4];
+      if constexpr (!FEAT) {
+        const uint4 *rp = reinterpret_cast<const uint4 *>(ring + s * STAGE + qd * 32u * BPV +
+                                                          (uint32_t)lane * BPV);
+#pragma unroll
+        for (int u = 0; u < (int)(BPV / 16); u++) {
+          const uint4 t = rp[u];
+          res[4 * u] = t.x;
+          res[4 * u + 1] = t.y;
+          res[4 * u + 2] = t.z;
+          res[4 * u + 3] = t.w;
+        }
+      }
+      WsCursor cn = c;
+      ws_advance(cn, 4, d_ng, nd);
+      if (i + 1 < n_tiles && !fetch(i + 1, cn)) ok = false;
+      // A_r: the E4M3 bucket weights (zero weights for padding rows)
+      if constexpr (!FEAT) {
+        uint32_t out[16];
+        if constexpr (NBIT == 4) {
+          TmWeights t = tw;
+#pragma unroll
+          for (int k = 0; k < 6; k++) t.w[k] = valid ? tw.w[k] : 0u;
+          fp8_decode16_b4(res, t, out);
+          tmem_st16(acol + 32u, out);
+          fp8_decode16_b4(res + 8, t, out);
+          tmem_st16(acol + 48u, out);
+        } else {
+          const uint32_t wt = valid ? tw.w[0] : 0u;
+          fp8_decode16(res, wt, out);
+          tmem_st16(acol + 32u, out);
+          fp8_decode16(res + 4, wt, out);
+          tmem_st16(acol + 48u, out);
+        }
+        tmem_wait_st();
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) {
+        mbar_arrive(&afull[sa]);
+        mbar_arrive(&sfree[s]);
+      }
+      c = cn;
+      if (s_abort) ok = false;
+    }
+    if (!__all_sync(kFull, ok) && lane == 0) {
+      atomicOr(err, 4u);
+      s_abort = 1;
+    }
+  } else {
+    // ---------------- epilogue ----------------
+    WsCursor c{0, 0}, ca{0, 0};
+    ws_advance(c, qd, d_ng, nd);
+    ws_advance(ca, qd + 4u * SD, d_ng, nd);  // the group this warp re-arms for
+    bool ok = true;
+    for (uint32_t i = 0; i < n_tiles; i++) {
+      const uint32_t sd = i % SD;
+      if (!__all_sync(kFull, mbar_wait(&dfull[sd], (i / SD) & 1, wait_ns))) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t dcol = dbase + lane_off + NMAX * sd;
+      uint32_t v0[32];
+      tmem_ld32(dcol, v0);
+      uint32_t v1[NMAX > 32 ? 32 : 1];
+      if constexpr (NMAX > 32) tmem_ld32(dcol + 32u, v1);
+      // re-arm the stage for tile i + SD, then hand it back to the MMA
+      const uint32_t x = (uint32_t)lane < ws_rows(ca, d_len, nd) ? off_bits : 0u;
+#pragma unroll
+      for (int h = 0; h < NMAX / 32; h++) tmem_fill32(dcol + 32u * h, x);
+      tmem_wait_st();
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&dempty[sd]);
+      ws_advance(ca, 4, d_ng, nd);
+      if (c.d < nd) {  // uniform: this warp's group of tile i holds tokens of doc c.d
+        uint32_t m0 = 0u;
+#pragma unroll
+        for (int j = 0; j < 32; j++) {
+          const uint32_t m = __reduce_max_sync(kFull, v0[j]);
+          m0 = lane == j ? m : m0;
+        }
+        if ((uint32_t)lane < nq) atomicMax(&best[c.d * NMAX + lane], m0);
+        if constexpr (NMAX > 32) {
+          uint32_t m1 = 0u;
+#pragma unroll
+          for (int j = 0; j < 32; j++) {
+            const uint32_t m = __reduce_max_sync(kFull, v1[j]);
+            m1 = lane == j ? m : m1;
+          }
+          if ((uint32_t)lane + 32u < nq) atomicMax(&best[c.d * NMAX + 32 + lane], m1);
+        }
+      }
+      ws_advance(c, 4, d_ng, nd);
+      if (s_abort) {
+        ok = false;
+        break;
+      }
+    }
+    if (!ok && lane == 0) {
+      atomicOr(err, 4u);
+      s_abort = 1;
+    }
+  }
+  __syncthreads();
+
+  if constexpr (FEAT) {
+    // pruner features: approx is [queries][probe_topk][33]: per query token
+    // the doc's best centroid score (0 past the query's last token), then
+    // log(doc length)
+    for (int i = tid; i < (int)nd * 33 && !s_abort; i += kWsThreads) {
+      const int d = i / 33, t = i % 33;
+      float f = 0.0f;
+      if (t == 32) f = logf((float)d_len[d]);
+      else if ((uint32_t)t < nq) f = (__uint_as_float(best[d * NMAX + t]) - off) * s_qinv[t];
+      approx[((size_t)b * probe_topk + d0 + d) * 33 + t] = f;
+    }
+  } else if (tid < (int)nd && !s_abort) {
+    const bool clamp = semantics == 1 && d_len[tid] < ix.max_item_n_vec;
+    float s = 0.0f;
+    for (uint32_t t = 0; t < nq; t++) {
+      float m = (__uint_as_float(best[tid * NMAX + t]) - off) * s_qinv[t];
+      if (clamp) m = fmaxf(m, 0.0f);
+      s += m;
+    }
+    approx[(size_t)b * probe_topk + d0 + tid] = s;
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(COLS));
+  }
+}
+
+// ---------------------------------------------------------------------
+// prune_mlp_kernel: the learned pruner's MLP (33 -> 256 -> 256 -> 1, GELU)
+// on the tensor cores, over the features of every shortlisted doc of a
+// batch.  Persistent: each CTA loads the BF16 weights once (pre-swizzled
+// K-major tiles, 1-D bulk copies: W1 [256 x 64] 32 KB, W2 [256 x 256]
+// 128 KB) and loops over tiles of 128 (query, doc) rows.  Per tile: the
+// threads write the rows' features as BF16 into a swizzled A tile (K = 33,
+// zero-padded to 64); one thread issues 4 tcgen05.mma (kind::f16, M = 128,
+// N = 256, K = 16) into a 256-column TMEM accumulator; the 8 warps read it
+// back (warp w: lane quadrant w & 3, columns 128 (w >> 2) ..), add b1, apply
+// GELU and write H1 as BF16 into a second swizzled A tile [128 x 256]
+// (aliasing the feature tile); 16 more MMAs compute H1 W2^T into the same
+// columns; the epilogue adds b2, applies GELU, multiplies by w3 and sums
+// each row (the two column halves combined through shared memory).  GELU is
+// the tanh form with the hardware tanh approximation.
+// ---------------------------------------------------------------------
+constexpr int kMlpThreads = 256;
+constexpr uint32_t kMlpW1Bytes = 256u * 128u, kMlpW2Bytes = 4u * 256u * 128u;
+constexpr uint32_t kMlpHBytes = 4u * 128u * 128u;
+constexpr size_t kMlpSmem = 1024 + kMlpW1Bytes + kMlpW2Bytes + kMlpHBytes;  // 225 KB
+
+__device__ __forceinline__ float gelu_fast(float x) {
+  float t;
+  asm("tanh.approx.f32 %0, %1;\n" : "=f"(t) : "f"(0.7978845608f * fmaf(0.044715f * x * x, x, x)));
+  return 0.5f * x * (1.0f + t);
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
+  __nv_bfloat162 p = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<uint32_t *>(&p);
+}
+
+__global__ void __launch_bounds__(kMlpThreads, 1)
+prune_mlp_kernel(const float *__restrict__ feat, const uint32_t *__restrict__ n_short,
+                 uint32_t n_query, uint32_t probe_topk, const uint8_t *__restrict__ wts,
+                 const float *__restrict__ vecs, float *__restrict__ pred,
+                 unsigned *__restrict__ err) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint8_t *W1s = smem, *W2s = smem + kMlpW1Bytes, *H = W2s + kMlpW2Bytes;
+  __shared__ uint64_t bar_load, bar_mma;
+  __shared__ uint32_t tmem_base_s;
+  __shared__ float red[128];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t n_rows = n_query * probe_topk;
+  const uint32_t n_tiles = (n_rows + 127u) / 128u;
+  if (blockIdx.x >= n_tiles) return;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     smem_u32(&tmem_base_s)),
+                 "r"(256u));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  if (tid == 0) {
+    mbar_init(&bar_load, 1);
+    mbar_init(&bar_mma, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  if (tid == 0) {
+    mbar_expect_tx(&bar_load, kMlpW1Bytes + kMlpW2Bytes);
+    for (uint32_t o = 0; o < kMlpW1Bytes + kMlpW2Bytes; o += 16384u)
+      bulk_g2s(smem_u32(W1s) + o, wts + o, 16384u, &bar_load);
+  }
+  bool ok = mbar_wait(&bar_load, 0);
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_s;
+  const uint32_t qd = warp & 3, hh = warp >> 2;
+  const uint32_t lane_off = (32u * qd) << 16;
+  const uint32_t row = 32u * qd + lane;  // this thread's row of the tile (epilogues)
+  const float *b1 = vecs, *b2 = vecs + 256, *w3 = vecs + 512;
+  const float b3 = vecs[768];
+  const uint32_t idesc = idesc_bf16(128, 256);
+  uint32_t phase = 0;
+  for (uint32_t t = blockIdx.x; ok && t < n_tiles; t += gridDim.x) {
+    // features -> BF16 A tile (two threads per row, 4 of the 8 chunks each)
+    {
+      const uint32_t r = tid >> 1, half = tid & 1;
+      const uint32_t gr = t * 128u + r;
+      const uint32_t bq = gr / probe_topk, d = gr % probe_topk;
+      const bool valid = gr < n_rows && d < n_short[bq];
+      const float *f = feat + (size_t)gr * 33;
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        const uint32_t ch = half * 4 + c;
+        uint32_t v[4];
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          const uint32_t k = ch * 8 + 2 * e;
+          const float a = valid && k < 33 ? __ldg(f + k) : 0.0f;
+          const float bb = valid && k + 1 < 33 ? __ldg(f + k + 1) : 0.0f;
+          v[e] = pack_bf16(a, bb);
+        }
+        *reinterpret_cast<uint4 *>(H + sw128_off(r, ch)) = make_uint4(v[0], v[1], v[2], v[3]);
+      }
+    }
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (tid == 0) {
+#pragma unroll
+      for (int ks = 0; ks < 4; ks++)
+        mma_bf16(tmem, sw128_desc(smem_u32(H) + 32 * ks), sw128_desc(smem_u32(W1s) + 32 * ks),
+                 idesc, ks > 0 ? 1u : 0u);
+      mma_commit(&bar_mma);
+    }
+    if (!__syncthreads_and(mbar_wait(&bar_mma, phase & 1))) { ok = false; break; }
+    phase++;
+    tc_fence_after();
+    // H1 = GELU(X W1^T + b1) -> BF16 A tile of layer 2 (over the feature tile)
+    for (uint32_t c0 = 0; c0 < 128; c0 += 32) {
+      const uint32_t col0 = 128u * hh + c0;
+      uint32_t v[32];
+      tmem_ld32(tmem + lane_off + col0, v);
+#pragma unroll
+      for (int g = 0; g < 4; g++) {  // 4 chunks of 8 columns
+        uint32_t w[4];
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          const uint32_t c = col0 + 8 * g + 2 * e;
+          const float a = gelu_fast(__uint_as_float(v[8 * g + 2 * e]) + __ldg(b1 + c));
+          const float bb = gelu_fast(__uint_as_float(v[8 * g + 2 * e + 1]) + __ldg(b1 + c + 1));
+          w[e] = pack_bf16(a, bb);
+        }
+        const uint32_t col = col0 + 8 * g;
+        *reinterpret_cast<uint4 *>(H + (col >> 6) * 16384u + sw128_off(row, (col & 63) >> 3)) =
+            make_uint4(w[0], w[1], w[2], w[3]);
+      }
+    }
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (tid == 0) {
+#pragma unroll
+      for (int kb = 0; kb < 4; kb++)
+#pragma unroll
+        for (int ks = 0; ks < 4; ks++)
+          mma_bf16(tmem, sw128_desc(smem_u32(H) + kb * 16384u + 32 * ks),
+                   sw128_desc(smem_u32(W2s) + kb * 32768u + 32 * ks), idesc,
+                   (kb | ks) ? 1u : 0u);
+      mma_commit(&bar_mma);
+    }
+    if (!__syncthreads_and(mbar_wait(&bar_mma, phase & 1))) { ok = false; break; }
+    phase++;
+    tc_fence_after();
+    // y = GELU(H1 W2^T + b2) . w3 + b3
+    float part = 0.0f;
+    for (uint32_t c0 = 0; c0 < 128; c0 += 32) {
+      const uint32_t col0 = 128u * hh + c0;
+      uint32_t v[32];
+      tmem_ld32(tmem + lane_off + col0, v);
+#pragma unroll
+      for (int j = 0; j < 32; j++)
+        part = fmaf(gelu_fast(__uint_as_float(v[j]) + __ldg(b2 + col0 + j)), __ldg(w3 + col0 + j),
+                    part);
+    }
+    if (hh == 1) red[row] = part;
+    tc_fence_before();
+    __syncthreads();
+    if (hh == 0) {
+      const uint32_t gr = t * 128u + row;
+      if (gr < n_rows) pred[gr] = part + red[row] + b3;
+    }
+  }
+  if (!ok && tid == 0) atomicOr(err, 8u);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(256u));
+  }
+}
+
+// BF16 weight tiles of the MLP kernel from the float parameter vector
+// (layout of mvr_prune.cuh): W1 [256 rows][K 64] (K >= 33 zero), then W2 as
+// 4 K-blocks of [256 rows][64], all K-major with the 128-byte swizzle; vecs:
+// b1, b2, w3 (256 each), b3.
+__global__ void prune_prep_kernel(const float *__restrict__ p, uint8_t *__restrict__ wts,
+                                  float *__restrict__ vecs) {
+  const uint32_t n1 = 256u * 64u, n2 = 4u * 256u * 64u;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n1 + n2 + 769u;
+       i += gridDim.x * blockDim.x) {
+    if (i < n1) {
+      const uint32_t r = i / 64, k = i % 64;
+      const float w = k < 33 ? p[r * 33 + k] : 0.0f;
+      *reinterpret_cast<__nv_bfloat16 *>(wts + sw128_off(r, k >> 3) + 2 * (k & 7)) =
+          __float2bfloat16_rn(w);
+    } else if (i < n1 + n2) {
+      const uint32_t j = i - n1, kb = j / (256u * 64u), r = (j / 64) % 256u, k = j % 64;
+      const float w = p[256u * 33u + 256u + r * 256u + kb * 64u + k];
+      *reinterpret_cast<__nv_bfloat16 *>(wts + kMlpW1Bytes + kb * 32768u + sw128_off(r, k >> 3) +
+                                         2 * (k & 7)) = __float2bfloat16_rn(w);
+    } else {
+      const uint32_t j = i - n1 - n2;  // b1 (256), b2 (256), w3 (256), b3
+      const uint32_t src = j < 256 ? 256u * 33u + j
+                         : j < 512 ? 256u * 33u + 256u + 65536u + (j - 256u)
+                         : j < 768 ? 256u * 33u + 256u + 65536u + 256u + (j - 512u)
+                                   : 256u * 33u + 256u + 65536u + 512u;
+      vecs[j] = j >= 512 && j < 768 ? __bfloat162float(__float2bfloat16_rn(p[src])) : p[src];
+    }
+  }
+}
+
+// Per query (one warp): the docs the rerank takes after the pruner -- the
+// `keep` best predictions (kept_id, sorted best first, stride keep) when the
+// shortlist is longer than keep and the prediction of its R-th best doc
+// leads the keep-th best by at least margin; otherwise the whole shortlist
+// (a fallback, counted in *n_fallback).  fin_id / n_fin: stride probe_topk.
+// qstat[b * 3 + 2] becomes the chosen docs' token count.
+__global__ void prune_choose_kernel(const DevIndex ix, const uint32_t *__restrict__ short_id,
+                                    const uint32_t *__restrict__ n_short,
+                                    const uint32_t *__restrict__ kept_id,
+                                    const float *__restrict__ kept_s, uint32_t n_query,
+                                    uint32_t probe_topk, uint32_t keep, uint32_t R, float margin,
+                                    uint32_t *__restrict__ fin_id, uint32_t *__restrict__ n_fin,
+                                    uint32_t *__restrict__ qstat,
+                                    unsigned long long *__restrict__ n_fallback) {
+  const uint32_t b = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (b >= n_query) return;
+  const uint32_t ns = n_short[b];
+  bool prune = ns > keep;
+  if (prune) {
+    const float *ks = kept_s + (size_t)b * keep;
+    prune = ks[min(R, keep) - 1] - ks[keep - 1] >= margin;
+    if (!prune && lane == 0) atomicAdd(n_fallback, 1ull);
+  }
+  const uint32_t n = prune ? keep : ns;
+  const uint32_t *src = prune ? kept_id + (size_t)b * keep : short_id + (size_t)b * probe_topk;
+  uint32_t tok = 0;
+  for (uint32_t i = lane; i < n; i += 32) {
+    const uint32_t d = src[i];
+    fin_id[(size_t)b * probe_topk + i] = d;
+    tok += ix.item_n_vec[d];
+  }
+  tok = __reduce_add_sync(kFull, tok);
+  if (lane == 0) {
+    n_fin[b] = n;
+    qstat[b * 3 + 2] = tok;
+  }
+}
+
 __global__ void to_bf16_kernel(const float *__restrict__ in, size_t n, __nv_bfloat16 *__restrict__ out) {
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     out[i] = __float2bfloat16_rn(in[i]);
@@ -1275,6 +2025,18 @@ cudaError_t configure_tc_kernels() {
   e = cudaFuncSetAttribute(rerank_tmem_kernel<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tm_smem_bytes(64));
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(rerank_tmem_kernel<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tm_smem_bytes(64));
+  if (e != cudaSuccess) return e;
+#define MVR_WS_ATTR(NB, NM, F, D)                                                                \
+  e = cudaFuncSetAttribute(rerank_ws_kernel<NB, NM, F, D>,                                       \
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ws_smem_bytes(NB, NM)); \
+  if (e != cudaSuccess) return e;
+  MVR_WS_ATTR(2, 32, false, 32) MVR_WS_ATTR(2, 32, false, 64) MVR_WS_ATTR(2, 32, false, 128)
+  MVR_WS_ATTR(2, 64, false, 32) MVR_WS_ATTR(2, 64, false, 64) MVR_WS_ATTR(2, 64, false, 128)
+  MVR_WS_ATTR(4, 32, false, 32) MVR_WS_ATTR(4, 32, false, 64) MVR_WS_ATTR(4, 32, false, 128)
+  MVR_WS_ATTR(4, 64, false, 32) MVR_WS_ATTR(4, 64, false, 64) MVR_WS_ATTR(4, 64, false, 128)
+  MVR_WS_ATTR(2, 32, true, 64) MVR_WS_ATTR(4, 32, true, 64)
+#undef MVR_WS_ATTR
+  e = cudaFuncSetAttribute(prune_mlp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMlpSmem);
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(rerank_tc_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem_bytes(8, 64));
 }
@@ -1406,6 +2168,118 @@ cudaError_t launch_rerank_tmem(const DevIndex &ix, const void *cen_perm, const T
   else if (ix.n_bit == 2) MVR_TM_LAUNCH(2, false);
   else MVR_TM_LAUNCH(1, false);
 #undef MVR_TM_LAUNCH
+  *n_launch += 1;
+  return cudaGetLastError();
+}
+
+bool ws_docs_supported(uint32_t docs) { return docs == 32 || docs == 64 || docs == 128; }
+
+template <int NB, int NM, int DOCS>
+static void ws_launch(const DevIndex &ix, const uint8_t *c, const TmWeights &tw, const float *q,
+                      const uint64_t *q_off, uint32_t n_query, const uint32_t *short_id,
+                      const uint32_t *n_short, uint32_t probe_topk, int semantics, float x_bound,
+                      float *approx, unsigned *err, cudaStream_t st, uint64_t wait_ns) {
+  const dim3 grid((probe_topk + DOCS - 1) / DOCS, n_query);
+  rerank_ws_kernel<NB, NM, false, DOCS><<<grid, kWsThreads, ws_smem_bytes(NB, NM), st>>>(
+      ix, c, tw, q, q_off, short_id, n_short, probe_topk, semantics, x_bound, approx, err,
+      wait_ns);
+}
+
+template <int NB, int NM>
+static void ws_launch_docs(uint32_t docs, const DevIndex &ix, const uint8_t *c,
+                           const TmWeights &tw, const float *q, const uint64_t *q_off,
+                           uint32_t n_query, const uint32_t *short_id, const uint32_t *n_short,
+                           uint32_t probe_topk, int semantics, float x_bound, float *approx,
+                           unsigned *err, cudaStream_t st, uint64_t wait_ns) {
+  if (docs == 32)
+    ws_launch<NB, NM, 32>(ix, c, tw, q, q_off, n_query, short_id, n_short, probe_topk, semantics,
+                          x_bound, approx, err, st, wait_ns);
+  else if (docs == 128)
+    ws_launch<NB, NM, 128>(ix, c, tw, q, q_off, n_query, short_id, n_short, probe_topk, semantics,
+                           x_bound, approx, err, st, wait_ns);
+  else
+    ws_launch<NB, NM, 64>(ix, c, tw, q, q_off, n_query, short_id, n_short, probe_topk, semantics,
+                          x_bound, approx, err, st, wait_ns);
+}
+
+cudaError_t launch_rerank_ws(const DevIndex &ix, const void *cen8, const TmWeights &tw,
+                             const float *q, const uint64_t *q_off, uint32_t n_query,
+                             const uint32_t *short_id, const uint32_t *n_short,
+                             uint32_t probe_topk, int semantics, uint32_t nq_max, float x_bound,
+                             float *approx, unsigned *err, cudaStream_t st, int *n_launch,
+                             uint64_t wait_ns, uint32_t docs) {
+  if (!fp8_rerank_supported(ix.n_bit) || !ws_docs_supported(docs)) return cudaErrorInvalidValue;
+  const uint8_t *c = reinterpret_cast<const uint8_t *>(cen8);
+  // queries of up to 32 tokens run in the 32-column variant (two CTAs per
+  // SM), longer ones in the 64-column variant (one CTA per SM); each launch
+  // skips the other's queries
+  if (ix.n_bit == 4)
+    ws_launch_docs<4, 32>(docs, ix, c, tw, q, q_off, n_query, short_id, n_short, probe_topk,
+                          semantics, x_bound, approx, err, st, wait_ns);
+  else
+    ws_launch_docs<2, 32>(docs, ix, c, tw, q, q_off, n_query, short_id, n_short, probe_topk,
+                          semantics, x_bound, approx, err, st, wait_ns);
+  *n_launch += 1;
+  if (nq_max > 32) {
+    if (ix.n_bit == 4)
+      ws_launch_docs<4, 64>(docs, ix, c, tw, q, q_off, n_query, short_id, n_short, probe_topk,
+                            semantics, x_bound, approx, err, st, wait_ns);
+    else
+      ws_launch_docs<2, 64>(docs, ix, c, tw, q, q_off, n_query, short_id, n_short, probe_topk,
+                            semantics, x_bound, approx, err, st, wait_ns);
+    *n_launch += 1;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_prune_features(const DevIndex &ix, const void *cen8, const float *q,
+                                  const uint64_t *q_off, uint32_t n_query,
+                                  const uint32_t *short_id, const uint32_t *n_short,
+                                  uint32_t probe_topk, float x_bound, float *feat, unsigned *err,
+                                  cudaStream_t st, int *n_launch, uint64_t wait_ns) {
+  if (!fp8_rerank_supported(ix.n_bit)) return cudaErrorInvalidValue;
+  const dim3 grid((probe_topk + kWsDocs - 1) / kWsDocs, n_query);
+  const uint8_t *c = reinterpret_cast<const uint8_t *>(cen8);
+  const TmWeights none{};
+  if (ix.n_bit == 4)
+    rerank_ws_kernel<4, 32, true><<<grid, kWsThreads, ws_smem_bytes(4, 32), st>>>(
+        ix, c, none, q, q_off, short_id, n_short, probe_topk, 0, x_bound, feat, err, wait_ns);
+  else
+    rerank_ws_kernel<2, 32, true><<<grid, kWsThreads, ws_smem_bytes(2, 32), st>>>(
+        ix, c, none, q, q_off, short_id, n_short, probe_topk, 0, x_bound, feat, err, wait_ns);
+  *n_launch += 1;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_prune_choose(const DevIndex &ix, const uint32_t *short_id,
+                                const uint32_t *n_short, const uint32_t *kept_id,
+                                const float *kept_s, uint32_t n_query, uint32_t probe_topk,
+                                uint32_t keep, uint32_t R, float margin, uint32_t *fin_id,
+                                uint32_t *n_fin, uint32_t *qstat,
+                                unsigned long long *n_fallback, cudaStream_t st, int *n_launch) {
+  prune_choose_kernel<<<(n_query + 7) / 8, 256, 0, st>>>(ix, short_id, n_short, kept_id, kept_s,
+                                                         n_query, probe_topk, keep, R, margin,
+                                                         fin_id, n_fin, qstat, n_fallback);
+  *n_launch += 1;
+  return cudaGetLastError();
+}
+
+size_t prune_weight_bytes() { return kMlpW1Bytes + kMlpW2Bytes; }
+
+cudaError_t prune_prepare(const float *params, uint8_t *wts, float *vecs, cudaStream_t st) {
+  prune_prep_kernel<<<592, 256, 0, st>>>(params, wts, vecs);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_prune_mlp(const float *feat, const uint32_t *n_short, uint32_t n_query,
+                             uint32_t probe_topk, const uint8_t *wts, const float *vecs,
+                             float *pred, unsigned *err, int n_sm, cudaStream_t st,
+                             int *n_launch) {
+  const uint32_t tiles = (n_query * probe_topk + 127u) / 128u;
+  const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)n_sm);
+  if (grid == 0) return cudaSuccess;
+  prune_mlp_kernel<<<grid, kMlpThreads, kMlpSmem, st>>>(feat, n_short, n_query, probe_topk, wts,
+                                                         vecs, pred, err);
   *n_launch += 1;
   return cudaGetLastError();
 }

@@ -46,6 +46,46 @@ bool fp8_rerank_supported(uint32_t n_bit);
 cudaError_t make_centroid_fp8(const float *cen, uint32_t n_cent, uint32_t n_bit, void *out,
                               cudaStream_t st);
 
+// The same FP8 MaxSim, warp-specialised (producer / decoders / MMA / epilogue
+// over a shared-memory ring fed by bulk copies): cen8 as above with one zero
+// row appended (row n_centroid); the vq code array must be readable 16 bytes
+// past its last code.  wait_ns bounds every pipeline wait of the kernel (on
+// expiry it stops and sets bit 4 of *err); docs: shortlisted docs per CTA.
+cudaError_t launch_rerank_ws(const DevIndex &ix, const void *cen8, const TmWeights &tw,
+                             const float *q, const uint64_t *q_off, uint32_t n_query,
+                             const uint32_t *short_id, const uint32_t *n_short,
+                             uint32_t probe_topk, int semantics, uint32_t nq_max, float x_bound,
+                             float *approx, unsigned *err, cudaStream_t st, int *n_launch,
+                             uint64_t wait_ns, uint32_t docs);
+// shortlisted docs per CTA the FP8 kernel is built for (32, 64, 128)
+bool ws_docs_supported(uint32_t docs);
+
+// Learned-pruner features of every shortlisted doc with the FP8 kernel's
+// centroid part only: feat [n_query][probe_topk][33] = per query token the
+// best E4M3 centroid score q.c over the doc's tokens, then log(doc length).
+// Queries of up to 32 tokens.
+cudaError_t launch_prune_features(const DevIndex &ix, const void *cen8, const float *q,
+                                  const uint64_t *q_off, uint32_t n_query,
+                                  const uint32_t *short_id, const uint32_t *n_short,
+                                  uint32_t probe_topk, float x_bound, float *feat, unsigned *err,
+                                  cudaStream_t st, int *n_launch, uint64_t wait_ns);
+// The docs the rerank takes after the pruner (see mvr_tc.cu).
+cudaError_t launch_prune_choose(const DevIndex &ix, const uint32_t *short_id,
+                                const uint32_t *n_short, const uint32_t *kept_id,
+                                const float *kept_s, uint32_t n_query, uint32_t probe_topk,
+                                uint32_t keep, uint32_t R, float margin, uint32_t *fin_id,
+                                uint32_t *n_fin, uint32_t *qstat,
+                                unsigned long long *n_fallback, cudaStream_t st, int *n_launch);
+// The learned pruner's MLP on the tensor cores: pred [n_query][probe_topk]
+// from the features of the rows d < n_short[query]; wts / vecs: the weights
+// prepared by prune_prepare (prune_weight_bytes() bytes / 769 floats).
+size_t prune_weight_bytes();
+cudaError_t prune_prepare(const float *params, uint8_t *wts, float *vecs, cudaStream_t st);
+cudaError_t launch_prune_mlp(const float *feat, const uint32_t *n_short, uint32_t n_query,
+                             uint32_t probe_topk, const uint8_t *wts, const float *vecs,
+                             float *pred, unsigned *err, int n_sm, cudaStream_t st,
+                             int *n_launch);
+
 // tensor-core centroid scoring: candidates per token = splits * 16; the
 // centroid tiles hold 64 centroids each (n_tiles = C_pad / 64)
 uint32_t probe_tc_cand_per_token(uint32_t n_tok, uint32_t n_cent, int n_sm, uint32_t *splits);

@@ -21,6 +21,7 @@ MVR_SEM_BASIC = 1
 MVR_PREC_BF16 = 2
 MVR_PREC_FP8 = 4
 MVR_CAND_IMPUTE = 8
+MVR_PRUNE = 16
 
 # every symbol include/mvr.h declares
 EXPORTS = (
@@ -31,7 +32,9 @@ EXPORTS = (
     "mvr_search_device", "mvr_search_trace", "mvr_decompress", "mvr_unpack_buckets",
     "mvr_assign_device", "mvr_assign_tc_device", "mvr_pack_residual_device",
     "mvr_kmeans_accumulate_device",
-    "mvr_filter_noalloc",
+    "mvr_filter_noalloc", "mvr_index_set_wait_limit",
+    "mvr_mlp_work_floats", "mvr_mlp_train_step", "mvr_mlp_forward", "mvr_index_set_pruner",
+    "mvr_index_set_rerank_tile",
 )
 
 
@@ -53,7 +56,8 @@ class Stats(C.Structure):
                 ("n_batch", C.c_uint32), ("gpu_launches", C.c_uint32),
                 ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64),
                 ("n_cand_total", C.c_uint64), ("n_rerank_tok", C.c_uint64),
-                ("n_list_ent", C.c_uint64), ("stage_ms", C.c_double * 6)]
+                ("n_list_ent", C.c_uint64), ("stage_ms", C.c_double * 6),
+                ("n_prune_fallback", C.c_uint64)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_}
@@ -67,7 +71,8 @@ class Trace(C.Structure):
                 ("cand_id", C.c_void_p), ("cand_score", C.c_void_p),
                 ("n_short", C.c_uint32), ("short_id", C.c_void_p),
                 ("short_approx", C.c_void_p), ("short_exact", C.c_void_p),
-                ("topk_score", C.c_void_p), ("topk_id", C.c_void_p)]
+                ("topk_score", C.c_void_p), ("topk_id", C.c_void_p),
+                ("short_feat", C.c_void_p), ("short_pred", C.c_void_p)]
 
 
 _lib = None
@@ -109,11 +114,18 @@ def lib():
         "mvr_pack_residual_device": [vp, u64, vp, u32, vp, vp, u32, vp, vp],
         "mvr_kmeans_accumulate_device": [vp, u64, u32, vp, vp, vp, vp],
         "mvr_filter_noalloc": [vp, vp, vp, u32, u32, u32, vp, vp, vp, vp],
+        "mvr_index_set_wait_limit": [vp, u64],
+        "mvr_mlp_train_step": [vp, vp, u32, vp, vp, vp, vp, C.c_float, u32, vp, vp],
+        "mvr_mlp_forward": [vp, u32, vp, vp, vp, vp],
+        "mvr_index_set_pruner": [vp, vp, u32, C.c_float],
+        "mvr_index_set_rerank_tile": [vp, u32],
     }
     for name, args in sig.items():
         f = getattr(L, name)
         f.argtypes = args
         f.restype = i32
+    L.mvr_mlp_work_floats.argtypes = [u32]
+    L.mvr_mlp_work_floats.restype = C.c_size_t
     _lib = L
     return L
 

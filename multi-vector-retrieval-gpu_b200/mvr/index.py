@@ -17,6 +17,7 @@ SEM_BASIC = _lib.MVR_SEM_BASIC
 PREC_BF16 = _lib.MVR_PREC_BF16
 PREC_FP8 = _lib.MVR_PREC_FP8
 CAND_IMPUTE = _lib.MVR_CAND_IMPUTE
+PRUNE = _lib.MVR_PRUNE
 
 
 def _ptr(a):
@@ -129,6 +130,25 @@ class Index:
     def set_rescore(self, n_rescore):
         check(lib().mvr_index_set_rescore(self._h, n_rescore))
 
+    def set_pruner(self, params, keep, margin):
+        """Learned pruner of MVR_PRUNE searches: params float32 [74753]
+        (None removes it), keep docs per query, confidence margin."""
+        if params is None:
+            check(lib().mvr_index_set_pruner(self._h, None, 0, 0.0))
+            return
+        p = _c(params, np.float32)
+        check(lib().mvr_index_set_pruner(self._h, _ptr(p), int(keep), float(margin)))
+
+    def set_rerank_tile(self, docs_per_cta=0):
+        """Shortlisted docs per CTA of the FP8 MaxSim kernel: 32, 64 or 128
+        (0: the default)."""
+        check(lib().mvr_index_set_rerank_tile(self._h, int(docs_per_cta)))
+
+    def set_wait_limit(self, wait_ns=0):
+        """Time bound (ns) of the FP8 MaxSim kernel's pipeline waits; 0 restores
+        the default (1 s).  A failure-detection test hook."""
+        check(lib().mvr_index_set_wait_limit(self._h, int(wait_ns)))
+
     def set_graphs(self, enable=True):
         """Replay repeated search_device calls as one recorded CUDA graph."""
         check(lib().mvr_index_set_graphs(self._h, 1 if enable else 0))
@@ -180,29 +200,44 @@ class Index:
                                       C.byref(st)))
         return st
 
-    def trace(self, query, k, nprobe, probe_topk, semantics=SEM_PP):
+    def trace(self, query, k, nprobe, probe_topk, semantics=SEM_PP, features=False, pred=False,
+              cand=True):
+        """One query through every stage; with features / pred also the
+        learned pruner's features [n_short, 33] / predictions of the
+        shortlist (short_feat / short_pred); cand=False skips the candidate
+        set (n_item-sized buffers)."""
         q = _c(query, np.float32)
         nq = q.shape[0]
-        inf = self.info()
+        n_item = self.info()["n_item"] if cand else 0
         arrs = dict(
             probe_id=np.zeros(nq * nprobe, np.uint32), probe_score=np.zeros(nq * nprobe, np.float32),
-            cand_id=np.zeros(inf["n_item"], np.uint32), cand_score=np.zeros(inf["n_item"], np.float32),
             short_id=np.zeros(probe_topk, np.uint32), short_approx=np.zeros(probe_topk, np.float32),
             short_exact=np.zeros(probe_topk, np.float32), topk_score=np.zeros(k, np.float32),
             topk_id=np.zeros(k, np.uint32))
+        if features:
+            arrs["short_feat"] = np.zeros(probe_topk * 33, np.float32)
+        if pred:
+            arrs["short_pred"] = np.zeros(probe_topk, np.float32)
+        if cand:
+            arrs["cand_id"] = np.zeros(n_item, np.uint32)
+            arrs["cand_score"] = np.zeros(n_item, np.float32)
         tr = _lib.Trace()
-        tr.cand_cap = inf["n_item"]
+        tr.cand_cap = n_item
         for name, a in arrs.items():
             setattr(tr, name, a.ctypes.data)
         check(lib().mvr_search_trace(self._h, _ptr(q), nq, k, nprobe, probe_topk, semantics,
                                      C.byref(tr)))
         nc, ns = tr.n_cand, tr.n_short
         return dict(probe_id=arrs["probe_id"].reshape(nq, nprobe),
-                    probe_score=arrs["probe_score"].reshape(nq, nprobe),
-                    cand_id=arrs["cand_id"][:nc], cand_score=arrs["cand_score"][:nc],
+                    probe_score=arrs["probe_score"].reshape(nq, nprobe), n_cand=nc,
+                    **({"cand_id": arrs["cand_id"][:nc], "cand_score": arrs["cand_score"][:nc]}
+                       if cand else {}),
                     short_id=arrs["short_id"][:ns], short_approx=arrs["short_approx"][:ns],
                     short_exact=arrs["short_exact"][:ns], score=arrs["topk_score"],
-                    id=arrs["topk_id"])
+                    id=arrs["topk_id"],
+                    **({"short_feat": arrs["short_feat"][:ns * 33].reshape(ns, 33)}
+                       if features else {}),
+                    **({"short_pred": arrs["short_pred"][:ns]} if pred else {}))
 
     def decompress(self, vec_ids):
         ids = _c(vec_ids, np.uint64)

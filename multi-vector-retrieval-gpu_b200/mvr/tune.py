@@ -77,3 +77,30 @@ def tune_batch(index, queries, k, nprobe, probe_topk, semantics,
     index.set_batch(0)
     pick = min(table, key=lambda t: (t["ms"], t["batch"]))
     return dict(pick, table=table)
+
+
+def tune_tile(index, queries, k, nprobe, probe_topk, semantics, tiles=(32, 64, 128), repeats=3,
+              tok_off=None, stage=3):
+    """Tile shape of the FP8 MaxSim kernel (shortlisted docs per CTA): every
+    candidate is set on the index (set_rerank_tile) and the same search timed
+    (best of `repeats` of the rerank stage's device time, stage_ms[stage]);
+    returns dict(docs, ms, table) for the fastest and leaves it set.  Results
+    do not depend on the tile shape, only the time does (more docs per CTA
+    amortise its set-up, fewer spread a short shortlist over more SMs)."""
+    table = []
+    for d in tiles:
+        index.set_rerank_tile(d)
+        best = None
+        for _ in range(repeats):
+            if tok_off is None:
+                st = index.search(queries, k, nprobe, probe_topk, semantics=semantics,
+                                  with_stats=True)[2]
+            else:
+                st = index.search(queries, k, nprobe, probe_topk, tok_off=tok_off,
+                                  semantics=semantics, with_stats=True)[2]
+            ms = st["stage_ms"][stage] or st["device_ms"]
+            best = ms if best is None else min(best, ms)
+        table.append(dict(docs=d, ms=best))
+    pick = min(table, key=lambda t: (t["ms"], t["docs"]))
+    index.set_rerank_tile(pick["docs"])
+    return dict(pick, table=table)
