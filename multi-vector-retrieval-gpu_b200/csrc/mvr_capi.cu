@@ -708,6 +708,9 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
   CUDA_TRY(cudaGetLastError());
   if (herr) {
     CUDA_TRY(cudaMemset(h->d_err, 0, sizeof(unsigned)));
+    if (herr & 16u)
+      return set_err(MVR_ERR_CUDA, "FP8 rerank: query and doc token norms beyond the "
+                                   "positive-offset range (2^21)");
     return set_err(MVR_ERR_CUDA, "tensor-core %s: a completion wait timed out",
                    (herr & 2u) ? "centroid scoring" : (herr & 8u) ? "pruner MLP" : "rerank");
   }

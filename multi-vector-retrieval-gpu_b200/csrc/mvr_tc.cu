@@ -1251,62 +1251,57 @@ cudaError_t launch_probe_tc(const float *q, uint32_t n_tok, const void *cen_sw, 
 // BF16 tables: centroid rows and the byte -> per-value weight table.
 // ---------------------------------------------------------------------
 // rerank_ws_kernel<NBIT, NMAX, FEAT, DOCS>: the FP8 (E4M3) MaxSim of the
-// mixed-precision path for 2- and 4-bit codes, warp-specialised over a
-// shared-memory ring.
+// mixed-precision path for 2- and 4-bit codes, warp-specialised.
 //
-// The rows of the MMA tiles are doc-aligned groups: doc d of the CTA's chunk
-// of the shortlist (DOCS docs) takes ceil(L_d / 32) groups of 32 rows (its
-// tokens 32j .. 32j + 31; the rows past its last token are padding), groups
-// are numbered doc after doc, tile i holds groups 4i .. 4i + 3, and group
-// 4i + q sits in TMEM lane quadrant q.  Roles of the 320 threads:
-//  warp 0     producer: per tile, two 1-D bulk copies per group
-//             (cp.async.bulk, completion by mbarrier transaction count): the
-//             group's residual bytes and its vq codes (the latter rounded out
-//             to 16-byte boundaries) into stage i % kWsStages of the ring;
-//  warps 2-5  decoders, one thread per row: the row's code from the ring,
-//             its E4M3 centroid row from L2 (loaded one tile ahead), a
-//             tcgen05.st of that row (A_c), the residual bytes from the ring
-//             expanded by PRMT into E4M3 bucket weights (as
-//             rerank_tmem_kernel's FP8 decode), a tcgen05.st of those (A_r);
-//             padding rows store zeros;
-//  warp 1     MMA: one thread issues 4 K-steps x 2 tcgen05.mma (kind::f8f6f4,
-//             M = 128, N = NMAX, K = 32) per tile, A_c and A_r from TMEM and
-//             the query tile B from shared memory, accumulating both into the
-//             tile's D stage; commits release the A stage and hand D to the
-//             epilogue;
-//  warps 6-9  epilogue, one warp per group: tcgen05.ld of its 32 rows,
-//             re-arms the D stage for the tile kWsDStages later, and takes the
-//             max over the group's rows of each query-token column with one
-//             full-warp REDUX.MAX, folded into the per-(doc, query token)
-//             maxima by shared-memory atomicMax.
-// A D stage starts at OFF (a power of two above |q.x| for every pair of the
-// CTA, as in rerank_tmem_kernel) in real rows and at 0 in padding rows (whose
-// A rows are zero), so every D value is a non-negative float ordered like its
-// bit pattern, and padding never wins a max.  With FEAT the kernel computes
-// the learned pruner's features instead: the centroid part only (no residual
-// copies, decode or MMA), and per doc the maxima themselves (per query token
-// the best centroid score over the doc's tokens) plus log(doc length).
-// Every pipeline mbarrier wait is bounded (wait_ns, 1 s by default); on a
-// timeout the CTA records the error and every role stops; the producer then
-// waits (1 s bound) for its bulk copies still in flight and the MMA thread
-// for its MMAs before TMEM is freed.
+// The CTA takes DOCS docs of a query's shortlist; their tokens, doc after
+// doc, are the rows of its MMA tiles (128 rows per tile; rows past the last
+// token are zero).  Roles of the 320 threads:
+//  warp 0     producer: per tile, one 1-D bulk copy (cp.async.bulk, completion
+//             by mbarrier transaction count) of the residual bytes of every
+//             doc segment the tile covers, into stage i % kWsStages of a
+//             shared-memory ring;
+//  warps 2-5  decoders, one thread per row: the row's vq code (loaded from
+//             HBM three tiles ahead), its E4M3 centroid row from L2 (one tile
+//             ahead), a tcgen05.st of that row (A_c), the residual bytes from
+//             the ring (read in a bank-conflict-free order) expanded by PRMT
+//             into E4M3 bucket weights (as rerank_tmem_kernel's FP8 decode),
+//             a tcgen05.st of those (A_r);
+//  warp 1     MMA: one thread issues per tile a bias MMA that writes OFF into
+//             every element of the tile's D stage (a constant A_e of 16.0 in
+//             TMEM times a B_e tile of OFF / 512, 32 products summed exactly),
+//             then 4 K-steps x 2 tcgen05.mma (kind::f8f6f4, M = 128,
+//             N = NMAX, K = 32): A_c and A_r from TMEM, the query tile B from
+//             shared memory; commits release the A stage and hand D over;
+//  warps 6-9  epilogue, one warp per 32 rows: tcgen05.ld of its rows, the D
+//             stage released at once, then for each doc its rows belong to
+//             one full-warp REDUX.MAX per query-token column (rows of other
+//             docs masked to 0), folded into the per-(doc, query token) maxima
+//             by shared-memory atomicMax.
+// D starts at OFF, a power of two above |q.x| for every pair of the CTA
+// (Cauchy-Schwarz with the query-token norms and the index's bound on |x|),
+// so every D value is a positive float ordered like its bit pattern.  With
+// FEAT the kernel computes the learned pruner's features instead: the
+// centroid part only (no producer, residual decode or residual MMA), and
+// per doc the maxima themselves (per query token the best centroid score
+// over the doc's tokens) plus log(doc length).  Every pipeline mbarrier wait
+// is bounded (wait_ns, 1 s by default); on a timeout the CTA records the
+// error and every role stops; the producer then waits (1 s bound) for its
+// bulk copies still in flight and the MMA thread for its MMAs before TMEM
+// is freed.
 // ---------------------------------------------------------------------
 constexpr int kWsDocs = 64;          // shortlisted docs per CTA (default; 32, 64 or 128)
-constexpr int kWsStages = 4;         // shared-memory ring stages (one tile each)
-constexpr int kWsDStages = 4;        // D stages in TMEM
+constexpr int kWsStages = 4;         // shared-memory ring stages (residual bytes of one tile)
+constexpr int kWsDStages = 3;        // D stages in TMEM
 constexpr int kWsThreads = 320;
-constexpr uint32_t kWsCodeSlot = 160;  // ring bytes per group for codes: 32 x 4 + alignment slack
 
 __host__ __device__ constexpr int ws_astages(int nmax) { return nmax <= 32 ? 2 : 4; }
 __host__ __device__ constexpr uint32_t ws_cols(int nmax) { return nmax <= 32 ? 256u : 512u; }
-__host__ __device__ constexpr uint32_t ws_stage_bytes(int nbit) {
-  return 128u * (128u * nbit / 8u) + 4u * kWsCodeSlot;
-}
-// dynamic shared memory: 1 KB alignment slack + query tile + ring; the wide
-// (NMAX = 64) variant asks for more than half an SM's shared memory so that
-// one CTA holds the SM's 512 TMEM columns alone
+__host__ __device__ constexpr uint32_t ws_stage_bytes(int nbit) { return 128u * (128u * nbit / 8u); }
+// dynamic shared memory: 1 KB alignment slack + query tile + bias tile + ring;
+// the wide (NMAX = 64) variant asks for more than half an SM's shared memory
+// so that one CTA holds the SM's 512 TMEM columns alone
 __host__ __device__ constexpr size_t ws_smem_bytes(int nbit, int nmax) {
-  return nmax <= 32 ? 1024 + (size_t)nmax * 128 + kWsStages * (size_t)ws_stage_bytes(nbit)
+  return nmax <= 32 ? 1024 + 2 * (size_t)nmax * 128 + kWsStages * (size_t)ws_stage_bytes(nbit)
                     : 120 * 1024;
 }
 
@@ -1339,32 +1334,23 @@ __device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&r)[32
       "r"(r[29]), "r"(r[30]), "r"(r[31])
       : "memory");
 }
-__device__ __forceinline__ void tmem_fill32(uint32_t taddr, uint32_t x) {
-  asm volatile(
-      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,"
-      "%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};\n" ::"r"(taddr),
-      "r"(x)
-      : "memory");
+// the same word into 8 consecutive TMEM columns of the warp's 32 lanes
+__device__ __forceinline__ void tmem_fill8(uint32_t taddr, uint32_t x) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1};\n" ::"r"(
+                   taddr),
+               "r"(x)
+               : "memory");
 }
 __device__ __forceinline__ void tmem_wait_st() {
   asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory");
 }
-
-// Position in the CTA's group sequence: doc d (of the chunk), its group j.
-struct WsCursor {
-  uint32_t d, j;
-};
-__device__ __forceinline__ void ws_advance(WsCursor &c, uint32_t k, const uint16_t *ng,
-                                           uint32_t nd) {
-  c.j += k;
-  while (c.d < nd && c.j >= ng[c.d]) {
-    c.j -= ng[c.d];
-    c.d++;
-  }
-}
-// rows of the group at c (0 past the last group)
-__device__ __forceinline__ uint32_t ws_rows(const WsCursor &c, const uint32_t *len, uint32_t nd) {
-  return c.d < nd ? min(32u, len[c.d] - 32u * c.j) : 0u;
+__device__ __forceinline__ void mma_e4m3_acc(uint32_t tmem_d, uint32_t tmem_a, uint64_t b,
+                                             uint32_t idesc, uint32_t accum) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], [%1], %2, %3, p;\n}\n" ::"r"(tmem_d),
+      "r"(tmem_a), "l"(b), "r"(idesc), "r"(accum)
+      : "memory");
 }
 
 template <int NBIT, int NMAX, bool FEAT = false, int DOCS = kWsDocs>
@@ -1380,19 +1366,21 @@ rerank_ws_kernel(DevIndex ix, const uint8_t *__restrict__ cen8, TmWeights tw,
   static_assert(DOCS == 32 || DOCS == 64 || DOCS == 128, "docs per CTA");
   constexpr int S = kWsStages, SA = ws_astages(NMAX), SD = kWsDStages;
   constexpr uint32_t BPV = 128u * NBIT / 8u;       // residual bytes per token
-  constexpr uint32_t RES_STAGE = 128u * BPV;
   constexpr uint32_t STAGE = ws_stage_bytes(NBIT);
   constexpr uint32_t COLS = ws_cols(NMAX);
+  constexpr uint32_t DCOL0 = 64u * SA;              // D stages after the A stages
+  constexpr uint32_t ECOL = DCOL0 + NMAX * SD;      // bias operand A_e (8 columns)
+  static_assert(ECOL + 8 <= COLS, "TMEM columns");
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  uint8_t *Bq = smem;                   // [NMAX rows][128 B] E4M3, SW128, K-major
-  uint8_t *ring = smem + NMAX * 128;    // [S][STAGE]: residual rows, then 4 code slots
+  uint8_t *Bq = smem;                     // [NMAX rows][128 B] E4M3, SW128, K-major
+  uint8_t *Be = smem + NMAX * 128;        // bias B operand, same layout
+  uint8_t *ring = smem + 2 * NMAX * 128;  // [S][128 rows][BPV] residual bytes
   __shared__ uint32_t best[DOCS * NMAX];  // [doc][query token]: bits of OFF + max
-  __shared__ uint32_t s_qss, s_groups, tmem_base_s;
+  __shared__ uint32_t s_qss, tmem_base_s;
   __shared__ float s_qinv[NMAX];
   __shared__ uint64_t full[S], sfree[S], afull[SA], afree[SA], dfull[SD], dempty[SD], mdone;
-  __shared__ uint32_t d_len[DOCS];
-  __shared__ uint16_t d_ng[DOCS];
+  __shared__ uint32_t d_len[DOCS], d_pref[DOCS + 1];
   __shared__ uint64_t d_off[DOCS];
   __shared__ volatile int s_abort;
 
@@ -1421,18 +1409,28 @@ rerank_ws_kernel(DevIndex ix, const uint8_t *__restrict__ cen8, TmWeights tw,
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     s_abort = 0;
     s_qss = 0;
-    s_groups = 0;
   }
   if (tid < (int)nd) {
     const uint32_t it = short_id[(size_t)b * probe_topk + d0 + tid];
-    const uint32_t L = ix.item_n_vec[it];
-    d_len[tid] = L;
+    d_len[tid] = ix.item_n_vec[it];
     d_off[tid] = ix.item_off[it];
-    d_ng[tid] = (uint16_t)((L + 31u) / 32u);
   }
   for (int i = tid; i < DOCS * NMAX; i += kWsThreads) best[i] = 0u;
   __syncthreads();
-  if (tid < (int)nd) atomicAdd(&s_groups, (uint32_t)d_ng[tid]);
+  if (warp == 0) {  // token offsets of the docs within the CTA (warp scan)
+    uint32_t carry = 0;
+    if (lane == 0) d_pref[0] = 0;
+    for (uint32_t base = 0; base < nd; base += 32) {
+      uint32_t v = base + lane < nd ? d_len[base + lane] : 0u;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(kFull, v, o);
+        if (lane >= o) v += t;
+      }
+      if (base + lane < nd) d_pref[base + lane + 1] = carry + v;
+      carry += __shfl_sync(kFull, v, 31);
+    }
+  }
   // query tokens -> B (E4M3, per-token power-of-two scales, FP8 K order,
   // swizzled, rows >= nq zero): 8 lanes per row, 16 positions each
   for (int i = tid; i < NMAX * 8; i += kWsThreads) {
@@ -1469,78 +1467,74 @@ rerank_ws_kernel(DevIndex ix, const uint8_t *__restrict__ cen8, TmWeights tw,
   }
   __syncthreads();
   const uint32_t tmem = tmem_base_s;
-  const uint32_t n_tiles = (s_groups + 3u) / 4u;
+  const uint32_t T = d_pref[nd];                 // rows (tokens) of the CTA
+  const uint32_t n_tiles = (T + 127u) / 128u;
   const float off = fmaxf(1.0f, exp2f(ceilf(log2f(sqrtf(__uint_as_float(s_qss)) * x_bound * 1.15f +
                                                   1e-30f))));
-  const uint32_t off_bits = __float_as_uint(off);
+  // bias operands: OFF = 2^e = 32 * A_e * B_e with A_e = 2^a (a in [4, 8],
+  // every row and K position of A_e) and B_e = 2^(e - 5 - a) >= 2^-9 in K
+  // positions 0..31 of every row of the bias tile (the rest 0): both exact in
+  // E4M3, the 32 products sum to OFF exactly, for OFF up to 2^21
+  const int e_off = (int)log2f(off);
+  const int a_exp = min(8, e_off + 4);
+  if (e_off > 21) {  // norms beyond the bias's range: report, do not guess
+    if (tid == 0) atomicOr(err, 16u);
+  }
+  for (int i = tid; i < NMAX * 8; i += kWsThreads) {
+    const int row = i >> 3, ch = i & 7;
+    const uint32_t e = ch < 2 ? (uint32_t)__nv_cvt_float_to_fp8(exp2f((float)(e_off - 5 - a_exp)),
+                                                                __NV_SATFINITE, __NV_E4M3) *
+                                    0x01010101u
+                              : 0u;
+    *reinterpret_cast<uint4 *>(Be + sw128_off(row, ch)) = make_uint4(e, e, e, e);
+  }
   const uint32_t qd = warp & 3;  // TMEM lane quadrant of this warp
   const uint32_t lane_off = (32u * qd) << 16;
-  const uint32_t dbase = tmem + 64u * SA;  // D stages after the A stages
-
-  if (warp >= 6) {  // epilogue warps arm the D stages of tiles 0 .. SD-1
-    WsCursor c{0, 0};
-    ws_advance(c, qd, d_ng, nd);
-    for (int sd = 0; sd < SD; sd++) {
-      const uint32_t x = (uint32_t)lane < ws_rows(c, d_len, nd) ? off_bits : 0u;
-#pragma unroll
-      for (int h = 0; h < NMAX / 32; h++) tmem_fill32(dbase + lane_off + NMAX * sd + 32 * h, x);
-      ws_advance(c, 4, d_ng, nd);
-    }
+  if (warp >= 2 && warp < 6) {  // A_e = 2^a: E4M3 exponent field a + 7, mantissa 0
+    tmem_fill8(tmem + lane_off + ECOL, (uint32_t)((a_exp + 7) << 3) * 0x01010101u);
     tmem_wait_st();
   }
-  fence_async_smem();  // B tile (generic stores) before the MMAs read it
+  fence_async_smem();  // B and bias tiles (generic stores) before the MMAs read them
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
 
   if (warp == 0) {
-    // ---------------- producer ----------------
-    WsCursor c{0, 0};
-    ws_advance(c, (uint32_t)min(lane, 3), d_ng, nd);  // lane g < 4: group 4i + g
-    const uint32_t ring_u32 = smem_u32(ring);
-    uint32_t issued = 0;
-    bool ok = true;
-    for (uint32_t i = 0; i < n_tiles; i++) {
-      const uint32_t s = i % S;
-      if (i >= (uint32_t)S &&
-          !__all_sync(kFull, mbar_wait(&sfree[s], ((i / S) + 1) & 1, wait_ns))) {
-        ok = false;
-        break;
+    // ---------------- producer: residual bytes of each tile's doc segments ----------------
+    if constexpr (!FEAT) {
+      const uint32_t ring_u32 = smem_u32(ring);
+      uint32_t dfirst = 0, issued = 0;
+      bool ok = true;
+      for (uint32_t i = 0; i < n_tiles; i++) {
+        const uint32_t s = i % S;
+        if (i >= (uint32_t)S &&
+            !__all_sync(kFull, mbar_wait(&sfree[s], ((i / S) + 1) & 1, wait_ns))) {
+          ok = false;
+          break;
+        }
+        const uint32_t R0 = 128u * i, R1 = min(R0 + 128u, T);
+        if (lane == 0) mbar_expect_tx(&full[s], (R1 - R0) * BPV);
+        __syncwarp();
+        for (uint32_t d = dfirst + lane; d < nd && d_pref[d] < R1; d += 32) {
+          const uint32_t rs = max(d_pref[d], R0), re = min(d_pref[d + 1], R1);
+          if (re > rs)
+            bulk_g2s(ring_u32 + s * STAGE + (rs - R0) * BPV,
+                     ix.residual + (d_off[d] + (rs - d_pref[d])) * BPV, (re - rs) * BPV, &full[s]);
+        }
+        while (dfirst < nd && d_pref[dfirst + 1] <= R1) dfirst++;
+        issued = i + 1;
+        if (__any_sync(kFull, s_abort != 0)) {
+          ok = false;
+          break;
+        }
       }
-      uint32_t rb = 0, cb = 0;
-      const uint8_t *rsrc = nullptr, *csrc = nullptr;
-      if (lane < 4 && c.d < nd) {
-        const uint32_t cnt = min(32u, d_len[c.d] - 32u * c.j);
-        const uint64_t v = d_off[c.d] + 32ull * c.j;
-        rb = FEAT ? 0u : cnt * BPV;
-        rsrc = ix.residual + v * BPV;
-        const uintptr_t a = (uintptr_t)(ix.vq_code + v);
-        const uintptr_t a0 = a & ~(uintptr_t)15, a1 = (a + 4u * cnt + 15u) & ~(uintptr_t)15;
-        cb = (uint32_t)(a1 - a0);
-        csrc = reinterpret_cast<const uint8_t *>(a0);
-      }
-      uint32_t tot = rb + cb;
-      tot += __shfl_xor_sync(kFull, tot, 1);
-      tot += __shfl_xor_sync(kFull, tot, 2);
-      if (lane == 0) mbar_expect_tx(&full[s], tot);
-      __syncwarp();
-      if (cb) {
-        if (rb) bulk_g2s(ring_u32 + s * STAGE + lane * 32u * BPV, rsrc, rb, &full[s]);
-        bulk_g2s(ring_u32 + s * STAGE + RES_STAGE + lane * kWsCodeSlot, csrc, cb, &full[s]);
-      }
-      ws_advance(c, 4, d_ng, nd);
-      issued = i + 1;
-      if (s_abort) {
-        ok = false;
-        break;
-      }
-    }
-    if (!ok) {
-      if (lane == 0) {
+      if (!ok && lane == 0) {
         atomicOr(err, 4u);
         s_abort = 1;
       }
-      // the copies still in flight land before the CTA may exit
+      // the copies still in flight land before the CTA may exit (after a
+      // normal run the decoders have seen every one of them land; after an
+      // abort of another role some may still be on their way)
       for (uint32_t i = issued > (uint32_t)S ? issued - S : 0; i < issued; i++)
         mbar_wait(&full[i % S], (i / S) & 1);
     }
@@ -1549,18 +1543,20 @@ rerank_ws_kernel(DevIndex ix, const uint8_t *__restrict__ cen8, TmWeights tw,
     if (lane == 0) {
       const uint32_t idesc = idesc_e4m3(128, NMAX);
       const uint32_t b_base = smem_u32(Bq);
+      const uint64_t be_desc = sw128_desc(smem_u32(Be));
       uint32_t i = 0;
       for (; i < n_tiles; i++) {
         const uint32_t sa = i % SA, sd = i % SD;
         if (!mbar_wait(&afull[sa], (i / SA) & 1, wait_ns)) break;
         if (i >= (uint32_t)SD && !mbar_wait(&dempty[sd], ((i / SD) + 1) & 1, wait_ns)) break;
         tc_fence_after();
-        const uint32_t dcol = dbase + NMAX * sd;
+        const uint32_t dcol = tmem + DCOL0 + NMAX * sd;
+        mma_e4m3_acc(dcol, tmem + ECOL, be_desc, idesc, 0u);  // D = OFF
 #pragma unroll
         for (int kk = 0; kk < 4; kk++) {  // K = 32 per MMA: centroid part, residual part
           const uint64_t bd = sw128_desc(b_base + kk * 32);
-          mma_e4m3_ta(dcol, tmem + 64u * sa + 8u * kk, bd, idesc);
-          if constexpr (!FEAT) mma_e4m3_ta(dcol, tmem + 64u * sa + 32u + 8u * kk, bd, idesc);
+          mma_e4m3_acc(dcol, tmem + 64u * sa + 8u * kk, bd, idesc, 1u);
+          if constexpr (!FEAT) mma_e4m3_acc(dcol, tmem + 64u * sa + 32u + 8u * kk, bd, idesc, 1u);
         }
         mma_commit(&dfull[sd]);
         mma_commit(&afree[sa]);
@@ -1578,22 +1574,17 @@ rerank_ws_kernel(DevIndex ix, const uint8_t *__restrict__ cen8, TmWeights tw,
     }
     __syncwarp();
   } else if (warp < 6) {
-    // ---------------- decoders ----------------
-    WsCursor c{0, 0};
-    ws_advance(c, qd, d_ng, nd);
+    // ---------------- decoders: one thread per row ----------------
+    const uint32_t r = 32u * qd + lane;  // row of each tile
+    uint32_t dcur = 0;                    // doc of the row whose code is loaded next (monotone)
+    auto code_of = [&](uint32_t tile) -> uint32_t {
+      const uint32_t g = 128u * tile + r;
+      if (tile >= n_tiles || g >= T) return ix.n_centroid;  // the zero row
+      while (d_pref[dcur + 1] <= g) dcur++;
+      return __ldg(ix.vq_code + d_off[dcur] + (g - d_pref[dcur]));
+    };
     uint32_t cen[32];
-    // the code of this row in tile i (cursor cc) and its centroid row: the
-    // zero row (index n_centroid) for padding rows
-    auto fetch = [&](uint32_t i, const WsCursor &cc) -> bool {
-      const uint32_t s = i % S;
-      if (!mbar_wait(&full[s], (i / S) & 1, wait_ns)) return false;
-      uint32_t code = ix.n_centroid;
-      if ((uint32_t)lane < ws_rows(cc, d_len, nd)) {
-        const uint64_t v = d_off[cc.d] + 32ull * cc.j;
-        const uint32_t shift = (uint32_t)((uintptr_t)(ix.vq_code + v) & 15u);
-        code = *reinterpret_cast<const uint32_t *>(ring + s * STAGE + RES_STAGE + qd * kWsCodeSlot +
-                                                   shift + 4u * lane);
-      }
+    auto load_cen = [&](uint32_t code) {
       const uint4 *cp = reinterpret_cast<const uint4 *>(cen8 + (size_t)code * kDim);
 #pragma unroll
       for (int u = 0; u < 8; u++) {
@@ -1603,14 +1594,19 @@ rerank_ws_kernel(DevIndex ix, const uint8_t *__restrict__ cen8, TmWeights tw,
         cen[4 * u + 2] = t.z;
         cen[4 * u + 3] = t.w;
       }
-      return true;
     };
-    bool ok = n_tiles == 0 || fetch(0, c);
+    // codes three tiles ahead, centroid rows one tile ahead
+    const uint32_t c0 = code_of(0);
+    uint32_t c1 = code_of(1), c2 = code_of(2);
+    load_cen(c0);
+    // chunk rotation of the residual reads: rows are BPV bytes apart, so a
+    // wavefront's 8 lanes (rows) start in 4 (2-bit) or 2 (4-bit) bank groups
+    const uint32_t rot = NBIT == 2 ? ((uint32_t)lane >> 2) & 1u : ((uint32_t)lane >> 1) & 3u;
+    bool ok = true;
     for (uint32_t i = 0; ok && i < n_tiles; i++) {
       const uint32_t s = i % S, sa = i % SA;
-      const bool valid = (uint32_t)lane < ws_rows(c, d_len, nd);
-      (void)valid;
-      if (i >= (uint32_t)SA && !mbar_wait(&afree[sa], ((i / SA) + 1) & 1, wait_ns)) {
+      if (i >= (uint32_t)SA &&
+          !__all_sync(kFull, mbar_wait(&afree[sa], ((i / SA) + 1) & 1, wait_ns))) {
         ok = false;
         break;
       }
@@ -1618,61 +1614,73 @@ rerank_ws_kernel(DevIndex ix, const uint8_t *__restrict__ cen8, TmWeights tw,
       const uint32_t acol = tmem + lane_off + 64u * sa;
       tmem_st32(acol, cen);  // A_c: the centroid row as loaded
       tmem_wait_st();
-      // this row's residual words (tile i), then the next tile's centroid row
-      uint32_t res[BPV / 4];
+      if (i + 1 < n_tiles) load_cen(c1);
+      c1 = c2;
+      c2 = code_of(i + 3);
       if constexpr (!FEAT) {
-        const uint4 *rp = reinterpret_cast<const uint4 *>(ring + s * STAGE + qd * 32u * BPV +
-                                                          (uint32_t)lane * BPV);
+        if (!__all_sync(kFull, mbar_wait(&full[s], (i / S) & 1, wait_ns))) ok = false;
+        // A_r: this row's residual words decoded into E4M3 bucket weights
+        // (rows past the last token decode stale ring bytes; the epilogue
+        // skips them).  The 16-byte chunks of a row are read in an order that
+        // depends on the lane, so that the 8 lanes of each shared-memory
+        // wavefront hit 8 different groups of 4 banks
+        uint32_t res[BPV / 4];
+        const uint4 *rp = reinterpret_cast<const uint4 *>(ring + s * STAGE + r * BPV);
+        uint4 t[BPV / 16];
+#pragma unroll
+        for (int u = 0; u < (int)(BPV / 16); u++) t[u] = rp[u ^ rot];
+        // undo the rotation: chunk u sits in t[u ^ rot], one swap stage per bit of rot
+#pragma unroll
+        for (int bit = 1; bit < (int)(BPV / 16); bit <<= 1) {
+          if (rot & bit) {
+#pragma unroll
+            for (int u = 0; u < (int)(BPV / 16); u++)
+              if (!(u & bit)) {
+                const uint4 x = t[u];
+                t[u] = t[u | bit];
+                t[u | bit] = x;
+              }
+          }
+        }
 #pragma unroll
         for (int u = 0; u < (int)(BPV / 16); u++) {
-          const uint4 t = rp[u];
-          res[4 * u] = t.x;
-          res[4 * u + 1] = t.y;
-          res[4 * u + 2] = t.z;
-          res[4 * u + 3] = t.w;
+          res[4 * u] = t[u].x;
+          res[4 * u + 1] = t[u].y;
+          res[4 * u + 2] = t[u].z;
+          res[4 * u + 3] = t[u].w;
         }
-      }
-      WsCursor cn = c;
-      ws_advance(cn, 4, d_ng, nd);
-      if (i + 1 < n_tiles && !fetch(i + 1, cn)) ok = false;
-      // A_r: the E4M3 bucket weights (zero weights for padding rows)
-      if constexpr (!FEAT) {
         uint32_t out[16];
         if constexpr (NBIT == 4) {
-          TmWeights t = tw;
-#pragma unroll
-          for (int k = 0; k < 6; k++) t.w[k] = valid ? tw.w[k] : 0u;
-          fp8_decode16_b4(res, t, out);
+          fp8_decode16_b4(res, tw, out);
           tmem_st16(acol + 32u, out);
-          fp8_decode16_b4(res + 8, t, out);
+          fp8_decode16_b4(res + 8, tw, out);
           tmem_st16(acol + 48u, out);
         } else {
-          const uint32_t wt = valid ? tw.w[0] : 0u;
-          fp8_decode16(res, wt, out);
+          fp8_decode16(res, tw.w[0], out);
           tmem_st16(acol + 32u, out);
-          fp8_decode16(res + 4, wt, out);
+          fp8_decode16(res + 4, tw.w[0], out);
           tmem_st16(acol + 48u, out);
         }
         tmem_wait_st();
+      } else {
+        (void)rot;
       }
       tc_fence_before();
       __syncwarp();
       if (lane == 0) {
         mbar_arrive(&afull[sa]);
-        mbar_arrive(&sfree[s]);
+        if constexpr (!FEAT) mbar_arrive(&sfree[s]);
       }
-      c = cn;
-      if (s_abort) ok = false;
+      if (__any_sync(kFull, s_abort != 0)) ok = false;
     }
     if (!__all_sync(kFull, ok) && lane == 0) {
       atomicOr(err, 4u);
       s_abort = 1;
     }
   } else {
-    // ---------------- epilogue ----------------
-    WsCursor c{0, 0}, ca{0, 0};
-    ws_advance(c, qd, d_ng, nd);
-    ws_advance(ca, qd + 4u * SD, d_ng, nd);  // the group this warp re-arms for
+    // ---------------- epilogue: one warp per 32 rows ----------------
+    const uint32_t r = 32u * qd + lane;
+    uint32_t dcur = 0;
     bool ok = true;
     for (uint32_t i = 0; i < n_tiles; i++) {
       const uint32_t sd = i % SD;
@@ -1681,40 +1689,61 @@ rerank_ws_kernel(DevIndex ix, const uint8_t *__restrict__ cen8, TmWeights tw,
         break;
       }
       tc_fence_after();
-      const uint32_t dcol = dbase + lane_off + NMAX * sd;
+      const uint32_t dcol = tmem + lane_off + DCOL0 + NMAX * sd;
       uint32_t v0[32];
       tmem_ld32(dcol, v0);
       uint32_t v1[NMAX > 32 ? 32 : 1];
       if constexpr (NMAX > 32) tmem_ld32(dcol + 32u, v1);
-      // re-arm the stage for tile i + SD, then hand it back to the MMA
-      const uint32_t x = (uint32_t)lane < ws_rows(ca, d_len, nd) ? off_bits : 0u;
-#pragma unroll
-      for (int h = 0; h < NMAX / 32; h++) tmem_fill32(dcol + 32u * h, x);
-      tmem_wait_st();
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&dempty[sd]);
-      ws_advance(ca, 4, d_ng, nd);
-      if (c.d < nd) {  // uniform: this warp's group of tile i holds tokens of doc c.d
+      const uint32_t g = 128u * i + r;
+      int doc = -1;
+      if (g < T) {
+        while (d_pref[dcur + 1] <= g) dcur++;
+        doc = (int)dcur;
+      }
+      // per doc of these rows: REDUX over its rows of every column
+      unsigned rem = __ballot_sync(kFull, doc >= 0);
+      while (rem) {
+        const int gd = __shfl_sync(kFull, doc, __ffs(rem) - 1);
+        const bool in = doc == gd;
+        const unsigned mem = __ballot_sync(kFull, in);
+        rem &= ~mem;
         uint32_t m0 = 0u;
-#pragma unroll
-        for (int j = 0; j < 32; j++) {
-          const uint32_t m = __reduce_max_sync(kFull, v0[j]);
-          m0 = lane == j ? m : m0;
-        }
-        if ((uint32_t)lane < nq) atomicMax(&best[c.d * NMAX + lane], m0);
-        if constexpr (NMAX > 32) {
-          uint32_t m1 = 0u;
+        if (mem == kFull) {
 #pragma unroll
           for (int j = 0; j < 32; j++) {
-            const uint32_t m = __reduce_max_sync(kFull, v1[j]);
-            m1 = lane == j ? m : m1;
+            const uint32_t m = __reduce_max_sync(kFull, v0[j]);
+            m0 = lane == j ? m : m0;
           }
-          if ((uint32_t)lane + 32u < nq) atomicMax(&best[c.d * NMAX + 32 + lane], m1);
+        } else {
+#pragma unroll
+          for (int j = 0; j < 32; j++) {
+            const uint32_t m = __reduce_max_sync(kFull, in ? v0[j] : 0u);
+            m0 = lane == j ? m : m0;
+          }
+        }
+        if ((uint32_t)lane < nq) atomicMax(&best[gd * NMAX + lane], m0);
+        if constexpr (NMAX > 32) {
+          uint32_t m1 = 0u;
+          if (mem == kFull) {
+#pragma unroll
+            for (int j = 0; j < 32; j++) {
+              const uint32_t m = __reduce_max_sync(kFull, v1[j]);
+              m1 = lane == j ? m : m1;
+            }
+          } else {
+#pragma unroll
+            for (int j = 0; j < 32; j++) {
+              const uint32_t m = __reduce_max_sync(kFull, in ? v1[j] : 0u);
+              m1 = lane == j ? m : m1;
+            }
+          }
+          if ((uint32_t)lane + 32u < nq) atomicMax(&best[gd * NMAX + 32 + lane], m1);
         }
       }
-      ws_advance(c, 4, d_ng, nd);
-      if (s_abort) {
+      if (__any_sync(kFull, s_abort != 0)) {
         ok = false;
         break;
       }
