@@ -629,13 +629,13 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
         CUDA_TRY(rec(ev(bt, 4)));
         CUDA_TRY(launch_topk(sid, w.exact, nsh, nb, probe_topk, R, w.r_score, w.r_id, w.n_r, rs,
                              &launches));
-        CUDA_TRY(launch_rerank(h->dix, qp, qo, nb, w.r_id, w.n_r, R, sem, w.r_exact, rs,
-                               &launches));
+        CUDA_TRY(launch_rerank(h->dix, qp, qo, nb, w.r_id, w.n_r, R, sem, w.r_exact, h->d_err,
+                               rs, &launches, h->wait_ns));
         CUDA_TRY(launch_topk(w.r_id, w.r_exact, w.n_r, nb, R, topk, os, oi, nullptr, rs,
                              &launches));
       } else {
         CUDA_TRY(launch_rerank(h->dix, qp, qo, nb, w.short_id, w.n_short, probe_topk, sem,
-                               w.exact, rs, &launches));
+                               w.exact, h->d_err, rs, &launches, h->wait_ns));
         CUDA_TRY(rec(ev(bt, 4)));
         CUDA_TRY(launch_topk(w.short_id, w.exact, w.n_short, nb, probe_topk, topk, os, oi,
                              nullptr, rs, &launches));
@@ -700,7 +700,7 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
                            cudaMemcpyDeviceToHost, st));
   unsigned herr = 0;
   unsigned long long n_fallback = 0;
-  if (bf16) CUDA_TRY(cudaMemcpyAsync(&herr, h->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaMemcpyAsync(&herr, h->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
   if (prune)
     CUDA_TRY(cudaMemcpyAsync(&n_fallback, h->d_fallback, sizeof(n_fallback), cudaMemcpyDeviceToHost,
                              st));
@@ -708,6 +708,8 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
   CUDA_TRY(cudaGetLastError());
   if (herr) {
     CUDA_TRY(cudaMemset(h->d_err, 0, sizeof(unsigned)));
+    if (herr & 32u)
+      return set_err(MVR_ERR_CUDA, "FP32 rerank: a pipeline wait timed out");
     if (herr & 16u)
       return set_err(MVR_ERR_CUDA, "FP8 rerank: query and doc token norms beyond the "
                                    "positive-offset range (2^21)");

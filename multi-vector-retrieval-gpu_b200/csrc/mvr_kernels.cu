@@ -18,6 +18,7 @@
 // arithmetic and independent of launch shape.
 #include "mvr_common.cuh"
 #include "mvr_kernels.cuh"
+#include "mvr_mbar.cuh"
 
 #include <cfloat>
 
@@ -751,149 +752,340 @@ filter_select_kernel(DevIndex ix, uint32_t probe_topk, FilterScratch scr,
 }
 
 // ---------------------------------------------------------------------
-// K3: decompress + exact MaxSim for CH shortlisted docs of one query.
-// 256 threads; 128 doc tokens per tile decompressed into Xs[k][128] (FP32);
-// thread (warp w, lane l): query tokens (w&3)*8..+8 of the current 32-token
-// block, doc tokens (w>>2)*64 + 2l, +1.  Per-(token, doc) maxima go through
-// warp match/reduce into shared best[q][doc]; max is order-free and the final
-// sum over query tokens runs in token order.
+// K3: decompress + exact MaxSim of up to kRkDocs shortlisted docs of one query.
+//
+// The docs' tokens, each doc padded to a multiple of 4 tokens, form a stream
+// of 512-token tiles; a tile is consumed in 8 chunks of 16 dimensions.
+//  warps 8-11  decoders: per chunk, each thread decodes 4 tokens (positions
+//              p, p+128, p+256, p+384 of the tile) x 16 dims,
+//              x = centroid + W[bucket] (one rounded FP32 add; W from a table
+//              replicated across the 32 banks, read conflict-free), into
+//              stage i % kRkStages of a shared-memory ring [16 dims][512];
+//  warps 0-7   FMA: thread (warp w, lane l) owns query tokens 16(w&1)..+16 of
+//              the pass and doc tokens 128(w>>1) + 4l..+4 of the tile, so per
+//              dimension it reads 16 query values (4 broadcast LDS.128) and 4
+//              doc values (one LDS.128) for 64 FMAs: FMA-bound, not bound by
+//              shared-memory wavefronts.  After the 8th chunk of a tile: max
+//              over the thread's valid tokens (all of one doc, thanks to the
+//              padding), then per doc a __reduce_max_sync over the lanes
+//              holding it, folded into best[query token][doc] by atomicMax.
+// Queries of more than 32 tokens run in two passes (tokens 0-31, 32-63).
+// Ring handoff: mbarriers full[s] (the 128 decoder threads arrive) and
+// empty[s] (the 256 FMA threads arrive); every wait is bounded (wait_ns) and
+// a timeout sets bit 32 of *err and stops the CTA without writing scores.
+// Every dot product is the sequential __fmaf_rn chain over d = 0..127 from
+// 0.0f, so the scores are bit-identical to the canonical arithmetic.
 // ---------------------------------------------------------------------
-constexpr int kRerankDocs = 16;
-constexpr int kRerankTile = 128;
+constexpr int kRkDocs = 64;       // shortlisted docs per CTA
+constexpr int kRkTile = 512;      // doc tokens per tile
+constexpr int kRkChunk = 16;      // dimensions per ring stage
+constexpr int kRkStages = 4;      // ring stages
+constexpr int kRkQ = 32;          // query tokens per pass
+constexpr int kRkThreads = 512;   // 8 FMA warps + 8 decoder warps
+constexpr int kRkFma = 256;       // FMA threads
+// registers per thread after the split (setmaxnreg): the launch gives every
+// thread 128 (65,536 / 512); the FMA warpgroups give 8 each back and the
+// decoder warpgroups take them, 256 x 120 + 256 x 136 = 512 x 128
+constexpr int kRkRegLaunch = 128;
+constexpr int kRkRegFma = 120;
+constexpr int kRkRegDec = 136;
+static_assert(kRkFma * kRkRegFma + (kRkThreads - kRkFma) * kRkRegDec == kRkThreads * kRkRegLaunch,
+              "register split must equal the launch allocation");
+
+// CTA-local barrier of the FMA warps only (named barrier 1, 256 threads)
+__device__ __forceinline__ void fma_bar_sync() {
+  asm volatile("bar.sync 1, %0;\n" ::"n"(kRkFma) : "memory");
+}
+
+__host__ __device__ constexpr size_t rk_smem_bytes(int n_bit) {
+  return (size_t)kRkStages * kRkChunk * kRkTile * sizeof(float) +  // ring
+         (size_t)kDim * kRkQ * sizeof(float) +                      // query tokens of the pass
+         (size_t)(1 << n_bit) * 32 * sizeof(float) +                // replicated weights
+         (size_t)kMaxQueryTok * kRkDocs * sizeof(int);              // best[q][doc]
+}
 
 template <int NBIT>
-__global__ void __launch_bounds__(256)
-rerank_kernel(DevIndex ix, const float *__restrict__ q,
-              const uint64_t *__restrict__ q_off,
-              const uint32_t *__restrict__ short_id,
-              const uint32_t *__restrict__ n_short, uint32_t probe_topk,
-              int semantics, float *__restrict__ exact) {
-  constexpr int VPB = 8 / NBIT;
-  constexpr int HALF_BYTES = 64 / VPB;  // residual bytes for 64 dims
+__global__ void __launch_bounds__(kRkThreads, 1)
+rerank_kernel(DevIndex ix, const float *__restrict__ q, const uint64_t *__restrict__ q_off,
+              const uint32_t *__restrict__ short_id, const uint32_t *__restrict__ n_short,
+              uint32_t probe_topk, int semantics, float *__restrict__ exact,
+              unsigned *__restrict__ err, uint64_t wait_ns) {
+  constexpr int VPB = 8 / NBIT;             // values per residual byte
+  constexpr int CB = kRkChunk * NBIT / 8;   // residual bytes per token and chunk
+  constexpr int RW = (CB + 3) / 4;          // ... in 32-bit words
+  constexpr uint32_t MASK = (1u << NBIT) - 1u;
+  constexpr int NCH = kDim / kRkChunk;      // chunks per tile
   extern __shared__ __align__(16) float smem[];
-  float *Xs = smem;                            // [128][128]
-  float *Qs = Xs + kDim * kRerankTile;         // [128][64]
-  float *lut = Qs + kDim * kMaxQueryTok;       // [256][VPB]
-  int *best = reinterpret_cast<int *>(lut + 256 * VPB);  // [64][CH]
-  __shared__ uint32_t d_item[kRerankDocs], d_len[kRerankDocs], d_pref[kRerankDocs + 1];
-  __shared__ uint64_t d_off[kRerankDocs];
-  __shared__ int tok_doc[kRerankTile];
+  float *ring = smem;                                       // [S][16][512]
+  float *Qs = ring + kRkStages * kRkChunk * kRkTile;        // [128 dims][32 query tokens]
+  float *wrep = Qs + kDim * kRkQ;                           // [2^NBIT][32]
+  int *best = reinterpret_cast<int *>(wrep + (1 << NBIT) * 32);  // [64 query tokens][kRkDocs]
+  __shared__ uint32_t d_len[kRkDocs], d_pp[kRkDocs + 1];
+  __shared__ uint64_t d_off[kRkDocs];
+  __shared__ uint64_t full[kRkStages], empty[kRkStages];
+  __shared__ volatile int s_abort;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint32_t b = blockIdx.y;
   const uint32_t ns = n_short[b];
-  const uint32_t d0 = blockIdx.x * kRerankDocs;
+  const uint32_t d0 = blockIdx.x * kRkDocs;
   if (d0 >= ns) return;
-  const uint32_t nd = min((uint32_t)kRerankDocs, ns - d0);
+  const uint32_t nd = min((uint32_t)kRkDocs, ns - d0);
   const uint64_t tok0 = q_off[b];
   const uint32_t nq = (uint32_t)(q_off[b + 1] - tok0);
 
   if (tid < (int)nd) {
     const uint32_t it = short_id[(size_t)b * probe_topk + d0 + tid];
-    d_item[tid] = it;
     d_len[tid] = ix.item_n_vec[it];
     d_off[tid] = ix.item_off[it];
   }
-  for (int i = tid; i < 256 * VPB; i += 256) lut[i] = ix.lut[i];
-  for (int i = tid; i < kMaxQueryTok * kRerankDocs; i += 256) best[i] = f2si(-INFINITY);
-  for (int i = tid; i < kMaxQueryTok * (kDim / 4); i += 256) {
-    const int t = i % kMaxQueryTok, k4 = i / kMaxQueryTok;
-    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-    if ((uint32_t)t < nq) v = __ldg(reinterpret_cast<const float4 *>(q + (tok0 + t) * kDim) + k4);
-    Qs[(k4 * 4 + 0) * kMaxQueryTok + t] = v.x;
-    Qs[(k4 * 4 + 1) * kMaxQueryTok + t] = v.y;
-    Qs[(k4 * 4 + 2) * kMaxQueryTok + t] = v.z;
-    Qs[(k4 * 4 + 3) * kMaxQueryTok + t] = v.w;
-  }
-  __syncthreads();
   if (tid == 0) {
-    uint32_t acc = 0;
-    for (uint32_t i = 0; i < nd; i++) { d_pref[i] = acc; acc += d_len[i]; }
-    d_pref[nd] = acc;
+    for (int s = 0; s < kRkStages; s++) {
+      mbar_init(&full[s], kRkThreads - kRkFma);
+      mbar_init(&empty[s], kRkFma);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    s_abort = 0;
+  }
+  for (int i = tid; i < (1 << NBIT) * 32; i += kRkThreads) {
+    // bucket v sits in the top NBIT bits of byte v << (8 - NBIT), position 0
+    const uint32_t v = (uint32_t)i >> 5;
+    wrep[i] = ix.lut[((v << (8 - NBIT)) & 0xffu) * VPB];
+  }
+  for (int i = tid; i < kMaxQueryTok * kRkDocs; i += kRkThreads) best[i] = f2si(-INFINITY);
+  __syncthreads();
+  if (warp == 0) {  // padded token offsets of the docs (warp scan)
+    uint32_t carry = 0;
+    if (lane == 0) d_pp[0] = 0;
+    for (uint32_t base = 0; base < nd; base += 32) {
+      uint32_t v = base + lane < nd ? (d_len[base + lane] + 3u) & ~3u : 0u;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(kFull, v, o);
+        if (lane >= o) v += t;
+      }
+      if (base + lane < nd) d_pp[base + lane + 1] = carry + v;
+      carry += __shfl_sync(kFull, v, 31);
+    }
   }
   __syncthreads();
-  const uint32_t n_tok = d_pref[nd];
+  const uint32_t Tp = d_pp[nd];
+  const uint32_t n_tiles = (Tp + kRkTile - 1) / kRkTile;
+  const uint32_t n_pass = (nq + kRkQ - 1) / kRkQ;
+  const uint32_t total = n_tiles * NCH;  // ring chunks per pass
 
-  for (uint32_t p0 = 0; p0 < n_tok; p0 += kRerankTile) {
-    // -- decompress 128 tokens: thread = (token tid&127, half tid>>7) --
-    {
-      const int t = tid & (kRerankTile - 1), half = tid >> 7;
-      const uint32_t s = p0 + t;
-      float *xcol = Xs + (half * 64) * kRerankTile + t;
-      if (s < n_tok) {
-        const uint32_t di = find_seg(d_pref, (int)nd, s);
-        const uint64_t v = d_off[di] + (s - d_pref[di]);
-        if (half == 0) tok_doc[t] = (int)di;
-        const float4 *cen = reinterpret_cast<const float4 *>(ix.centroid + (size_t)ix.vq_code[v] * kDim + half * 64);
-        const uint8_t *res = ix.residual + v * ix.bytes_per_vec + half * HALF_BYTES;
-        uint8_t rb[HALF_BYTES];
+  if (warp >= kRkFma / 32) {
+    // ---------------- decoders (kRkRegDec registers) ----------------
+    // thread pt decodes tile positions pt and pt + 256 of every chunk; the
+    // loads of chunk i + 1 are in flight while chunk i is decoded, and the
+    // tokens (codes, residual rows) of tile t + 1 are located during tile t
+    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;\n" ::"n"(kRkRegDec));
+    const uint32_t pt = (uint32_t)(tid - kRkFma);
+    uint32_t code[2], code_n[2];
+    uint64_t vix[2], vix_n[2];
+    // tile tl's tokens of this thread; past a doc's last token (padding) or
+    // past the last doc: some valid token, whose values the FMA warps mask
+    auto locate = [&](uint32_t tl, uint32_t (&cd)[2], uint64_t (&vx)[2]) {
 #pragma unroll
-        for (int u = 0; u < HALF_BYTES / 8; u++)
-          *reinterpret_cast<uint2 *>(rb + 8 * u) = __ldg(reinterpret_cast<const uint2 *>(res) + u);
+      for (int j = 0; j < 2; j++) {
+        const uint32_t g = kRkTile * tl + (kRkTile / 2) * j + pt;
+        uint64_t v = d_off[0];
+        if (g < Tp) {
+          const uint32_t d = find_seg(d_pp, (int)nd, g);
+          v = d_off[d] + min(g - d_pp[d], d_len[d] - 1u);
+        }
+        vx[j] = v;
+        cd[j] = __ldg(ix.vq_code + v);
+      }
+    };
+    auto issue = [&](const uint32_t (&cd)[2], const uint64_t (&vx)[2], uint32_t c,
+                     float4 (&cv)[2][4], uint32_t (&rw)[2][RW]) {
 #pragma unroll
-        for (int d4 = 0; d4 < 16; d4++) {
-          const float4 c = __ldg(cen + d4);
-          const float cc[4] = {c.x, c.y, c.z, c.w};
+      for (int j = 0; j < 2; j++) {
+        const float4 *cp = reinterpret_cast<const float4 *>(ix.centroid + (size_t)cd[j] * kDim) + 4 * c;
 #pragma unroll
-          for (int u = 0; u < 4; u++) {
-            const int d = d4 * 4 + u;
-            const float w = lut[(uint32_t)rb[d / VPB] * VPB + (d % VPB)];
-            xcol[d * kRerankTile] = __fadd_rn(cc[u], w);
+        for (int u = 0; u < 4; u++) cv[j][u] = __ldg(cp + u);
+        const uint8_t *rp = ix.residual + vx[j] * ix.bytes_per_vec + (size_t)c * CB;
+        if constexpr (CB == 2) {
+          rw[j][0] = __ldg(reinterpret_cast<const unsigned short *>(rp));
+        } else if constexpr (CB == 4) {
+          rw[j][0] = __ldg(reinterpret_cast<const uint32_t *>(rp));
+        } else if constexpr (CB == 8) {
+          const uint2 t = __ldg(reinterpret_cast<const uint2 *>(rp));
+          rw[j][0] = t.x;
+          rw[j][1] = t.y;
+        } else {
+          const uint4 t = __ldg(reinterpret_cast<const uint4 *>(rp));
+          rw[j][0] = t.x;
+          rw[j][1] = t.y;
+          rw[j][2] = t.z;
+          rw[j][3] = t.w;
+        }
+      }
+    };
+    bool ok = true;
+    uint32_t base = 0;  // ring chunk counter at the start of the pass
+    // decode chunk q of the pass (values in cv / rw) into its ring stage
+    auto put = [&](uint32_t q, const float4 (&cv)[2][4], const uint32_t (&rw)[2][RW]) {
+      const uint32_t gq = base + q;
+      const uint32_t s = gq % kRkStages;
+      if (gq >= (uint32_t)kRkStages &&
+          !__all_sync(kFull, mbar_wait_sleep(&empty[s], ((gq / kRkStages) + 1) & 1, wait_ns))) {
+        ok = false;
+        return;
+      }
+      float *xs = ring + s * (kRkChunk * kRkTile) + pt;
+#pragma unroll
+      for (int j = 0; j < 2; j++) {
+        const float cc[16] = {cv[j][0].x, cv[j][0].y, cv[j][0].z, cv[j][0].w,
+                              cv[j][1].x, cv[j][1].y, cv[j][1].z, cv[j][1].w,
+                              cv[j][2].x, cv[j][2].y, cv[j][2].z, cv[j][2].w,
+                              cv[j][3].x, cv[j][3].y, cv[j][3].z, cv[j][3].w};
+#pragma unroll
+        for (int kk = 0; kk < kRkChunk; kk++) {
+          // dim 16c + kk: byte kk / VPB of the chunk, most significant bits first
+          const int gbit = 8 * (kk / VPB) + 8 - NBIT * (kk % VPB + 1);
+          const uint32_t v = (rw[j][gbit >> 5] >> (gbit & 31)) & MASK;
+          xs[kk * kRkTile + (kRkTile / 2) * j] = __fadd_rn(cc[kk], wrep[v * 32 + lane]);
+        }
+      }
+      mbar_arrive(&full[s]);
+      if (__any_sync(kFull, s_abort != 0)) ok = false;
+    };
+    // the loads of chunk q + 1 (the next tile's first chunk after chunk 7)
+    auto prefetch = [&](uint32_t q, float4 (&cv)[2][4], uint32_t (&rw)[2][RW]) {
+      if (q + 1 >= total) return;
+      if ((q + 1) % NCH != 0) issue(code, vix, (q + 1) % NCH, cv, rw);
+      else issue(code_n, vix_n, 0, cv, rw);
+    };
+    float4 cva[2][4], cvb[2][4];
+    uint32_t rwa[2][RW], rwb[2][RW];
+    for (uint32_t pass = 0; ok && pass < n_pass; pass++, base += total) {
+      locate(0, code, vix);
+      issue(code, vix, 0, cva, rwa);
+      if (n_tiles > 1) locate(1, code_n, vix_n);
+      for (uint32_t q = 0; ok && q < total; q += 2) {
+        // even chunk q: values in a; a tile starts at every multiple of 8
+        if (q % NCH == 0 && q > 0) {
+          const uint32_t tl = q / NCH;
+#pragma unroll
+          for (int j = 0; j < 2; j++) {
+            code[j] = code_n[j];
+            vix[j] = vix_n[j];
           }
+          if (tl + 1 < n_tiles) locate(tl + 1, code_n, vix_n);
         }
-      } else {
-        if (half == 0) tok_doc[t] = -1;
-#pragma unroll 8
-        for (int d = 0; d < 64; d++) xcol[d * kRerankTile] = 0.0f;
+        prefetch(q, cvb, rwb);
+        put(q, cva, rwa);
+        if (!ok || q + 1 >= total) break;
+        // odd chunk q + 1: values in b
+        prefetch(q + 1, cva, rwa);
+        put(q + 1, cvb, rwb);
       }
     }
-    __syncthreads();
-
-    const int tcol = (warp >> 2) * 64 + lane * 2;
-    const int doc0 = tok_doc[tcol], doc1 = tok_doc[tcol + 1];
-    const unsigned g0 = __match_any_sync(kFull, doc0);
-    const unsigned g1 = __match_any_sync(kFull, doc1);
-    for (uint32_t qb = 0; qb < nq; qb += 32) {
-      float acc[8][2];
+    if (!ok && lane == 0) {
+      atomicOr(err, 32u);
+      s_abort = 1;
+    }
+  } else {
+    // ---------------- FMA warps (kRkRegFma registers) ----------------
+    // Every FMA warp executes the same sequence of named barriers (two per
+    // pass and one at the end): a warp's own failure only skips its work.
+    asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" ::"n"(kRkRegFma));
+    const uint32_t qg = (uint32_t)warp & 1u;
+    const uint32_t tb = 128u * ((uint32_t)warp >> 1) + 4u * lane;
+    uint32_t it = 0;  // ring chunk counter (continues across tiles and passes)
+    bool ok = true;
+    for (uint32_t pass = 0; pass < n_pass; pass++) {
+      // query tokens 32 pass .. +32 -> Qs[dim][token] (zero past the last token)
+      for (int i = tid; i < kDim / 4 * kRkQ; i += kRkFma) {
+        const int j = i % kRkQ, k4 = i / kRkQ;
+        const uint32_t t = kRkQ * pass + j;
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (t < nq) v = __ldg(reinterpret_cast<const float4 *>(q + (tok0 + t) * kDim) + k4);
+        Qs[(4 * k4 + 0) * kRkQ + j] = v.x;
+        Qs[(4 * k4 + 1) * kRkQ + j] = v.y;
+        Qs[(4 * k4 + 2) * kRkQ + j] = v.z;
+        Qs[(4 * k4 + 3) * kRkQ + j] = v.w;
+      }
+      fma_bar_sync();
+      for (uint32_t tl = 0; ok && tl < n_tiles; tl++) {
+        const uint32_t g0 = kRkTile * tl + tb;
+        int doc = -1;
+        uint32_t nval = 0;
+        if (g0 < Tp) {
+          doc = (int)find_seg(d_pp, (int)nd, g0);
+          nval = min(4u, d_len[doc] - (g0 - d_pp[doc]));
+        }
+        float acc[16][4];
 #pragma unroll
-      for (int i = 0; i < 8; i++) acc[i][0] = acc[i][1] = 0.0f;
-      const float *qs = Qs + qb + (warp & 3) * 8;
-      const float *xs = Xs + tcol;
-#pragma unroll 4
-      for (int k = 0; k < kDim; k++) {
-        const float4 a0 = *reinterpret_cast<const float4 *>(qs + k * kMaxQueryTok);
-        const float4 a1 = *reinterpret_cast<const float4 *>(qs + k * kMaxQueryTok + 4);
-        const float2 x = *reinterpret_cast<const float2 *>(xs + k * kRerankTile);
-        const float a[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+        for (int i = 0; i < 16; i++)
 #pragma unroll
-        for (int i = 0; i < 8; i++) {
-          acc[i][0] = __fmaf_rn(a[i], x.x, acc[i][0]);
-          acc[i][1] = __fmaf_rn(a[i], x.y, acc[i][1]);
+          for (int j = 0; j < 4; j++) acc[i][j] = 0.0f;
+        for (int c = 0; c < NCH; c++, it++) {
+          const uint32_t s = it % kRkStages;
+          if (!__all_sync(kFull, mbar_wait_sleep(&full[s], (it / kRkStages) & 1, wait_ns)) ||
+              __any_sync(kFull, s_abort != 0)) {
+            ok = false;
+            break;
+          }
+          const float *xs = ring + s * (kRkChunk * kRkTile) + tb;
+          const float *qs = Qs + (kRkChunk * c) * kRkQ + 16 * qg;
+#pragma unroll
+          for (int kk = 0; kk < kRkChunk; kk++) {
+            const float4 x = *reinterpret_cast<const float4 *>(xs + kk * kRkTile);
+            float a[16];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+              const float4 t = *reinterpret_cast<const float4 *>(qs + kk * kRkQ + 4 * u);
+              a[4 * u] = t.x;
+              a[4 * u + 1] = t.y;
+              a[4 * u + 2] = t.z;
+              a[4 * u + 3] = t.w;
+            }
+#pragma unroll
+            for (int i = 0; i < 16; i++) {
+              acc[i][0] = __fmaf_rn(a[i], x.x, acc[i][0]);
+              acc[i][1] = __fmaf_rn(a[i], x.y, acc[i][1]);
+              acc[i][2] = __fmaf_rn(a[i], x.z, acc[i][2]);
+              acc[i][3] = __fmaf_rn(a[i], x.w, acc[i][3]);
+            }
+          }
+          mbar_arrive(&empty[s]);
+        }
+        if (!ok) {
+          if (lane == 0) {
+            atomicOr(err, 32u);
+            s_abort = 1;
+          }
+          break;
+        }
+        // max over the thread's valid tokens (one doc), then over the lanes of that doc
+        const unsigned grp = __match_any_sync(kFull, doc);
+        const bool lead = lane == __ffs(grp) - 1;
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+          int m = f2si(-INFINITY);
+#pragma unroll
+          for (int j = 0; j < 4; j++)
+            if ((uint32_t)j < nval) m = max(m, f2si(acc[i][j]));
+          m = __reduce_max_sync(grp, m);
+          const uint32_t qt = kRkQ * pass + 16u * qg + i;
+          if (doc >= 0 && lead && qt < nq) atomicMax(&best[qt * kRkDocs + doc], m);
         }
       }
-#pragma unroll
-      for (int i = 0; i < 8; i++) {
-        const uint32_t qt = qb + (warp & 3) * 8 + i;
-        const int m0 = __reduce_max_sync(g0, f2si(acc[i][0]));
-        const int m1 = __reduce_max_sync(g1, f2si(acc[i][1]));
-        if (qt < nq) {
-          if (doc0 >= 0 && lane == __ffs(g0) - 1) atomicMax(&best[qt * kRerankDocs + doc0], m0);
-          if (doc1 >= 0 && lane == __ffs(g1) - 1) atomicMax(&best[qt * kRerankDocs + doc1], m1);
-        }
+      fma_bar_sync();  // Qs is reloaded by the next pass; best is complete after the last
+    }
+    if (tid < (int)nd && !s_abort) {  // FMA threads 0 .. nd - 1
+      const bool clamp = semantics == 1 && d_len[tid] < ix.max_item_n_vec;
+      float s = 0.0f;
+      for (uint32_t t = 0; t < nq; t++) {
+        float m = si2f(best[t * kRkDocs + tid]);
+        if (clamp) m = fmaxf(m, 0.0f);
+        s = __fadd_rn(s, m);
       }
+      exact[(size_t)b * probe_topk + d0 + tid] = s;
     }
-    __syncthreads();
-  }
-
-  if (tid < (int)nd) {
-    const bool clamp = semantics == 1 && d_len[tid] < ix.max_item_n_vec;
-    float s = 0.0f;
-    for (uint32_t t = 0; t < nq; t++) {
-      float m = si2f(best[t * kRerankDocs + tid]);
-      if (clamp) m = fmaxf(m, 0.0f);
-      s = __fadd_rn(s, m);
-    }
-    exact[(size_t)b * probe_topk + d0 + tid] = s;
   }
 }
 
@@ -939,22 +1131,38 @@ topk_kernel(const uint32_t *__restrict__ short_id, const float *__restrict__ exa
 // ---------------------------------------------------------------------
 // host-side launchers
 // ---------------------------------------------------------------------
-size_t rerank_smem_bytes(int n_bit) {
-  return (size_t)(kDim * kRerankTile + kDim * kMaxQueryTok + 256 * (8 / n_bit)) * sizeof(float) +
-         (size_t)kMaxQueryTok * kRerankDocs * sizeof(int);
+// The register split of rerank_kernel (setmaxnreg) hands the FMA warps' and
+// decoders' shares out of the allocation the CTA was launched with; it is
+// only valid when that allocation is kRkRegLaunch per thread (a smaller one
+// would leave setmaxnreg.inc waiting), so the library refuses to run a build
+// that compiled to another count.
+template <typename K>
+static cudaError_t check_rk_registers(K kernel) {
+  cudaFuncAttributes a;
+  const cudaError_t e = cudaFuncGetAttributes(&a, kernel);
+  if (e != cudaSuccess) return e;
+  return a.numRegs == kRkRegLaunch ? cudaSuccess : cudaErrorInvalidKernelImage;
 }
 
 cudaError_t configure_kernels() {
   cudaError_t e = cudaFuncSetAttribute(probe_topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)kProbeSmem);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(rerank_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rerank_smem_bytes(1));
+  e = cudaFuncSetAttribute(rerank_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rk_smem_bytes(1));
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(rerank_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rerank_smem_bytes(2));
+  e = check_rk_registers(rerank_kernel<1>);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(rerank_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rerank_smem_bytes(4));
+  e = cudaFuncSetAttribute(rerank_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rk_smem_bytes(2));
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(rerank_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rerank_smem_bytes(8));
+  e = check_rk_registers(rerank_kernel<2>);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(rerank_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rk_smem_bytes(4));
+  if (e != cudaSuccess) return e;
+  e = check_rk_registers(rerank_kernel<4>);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(rerank_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rk_smem_bytes(8));
+  if (e != cudaSuccess) return e;
+  e = check_rk_registers(rerank_kernel<8>);
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(filter_hash_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)hash_smem_bytes(1));
@@ -1079,17 +1287,22 @@ cudaError_t launch_filter_hash(const DevIndex &ix, const uint32_t *probe_id,
 cudaError_t launch_rerank(const DevIndex &ix, const float *q, const uint64_t *q_off,
                           uint32_t n_query, const uint32_t *short_id,
                           const uint32_t *n_short, uint32_t probe_topk,
-                          int semantics, float *exact, cudaStream_t st,
-                          int *n_launch) {
-  dim3 grid((probe_topk + kRerankDocs - 1) / kRerankDocs, n_query);
-  const size_t sm = rerank_smem_bytes((int)ix.n_bit);
+                          int semantics, float *exact, unsigned *err, cudaStream_t st,
+                          int *n_launch, uint64_t wait_ns) {
+  if (n_query == 0 || probe_topk == 0) return cudaSuccess;
+  dim3 grid((probe_topk + kRkDocs - 1) / kRkDocs, n_query);
+  const size_t sm = rk_smem_bytes((int)ix.n_bit);
+#define MVR_RK(NB)                                                                              \
+  rerank_kernel<NB><<<grid, kRkThreads, sm, st>>>(ix, q, q_off, short_id, n_short, probe_topk, \
+                                                  semantics, exact, err, wait_ns)
   switch (ix.n_bit) {
-    case 1: rerank_kernel<1><<<grid, 256, sm, st>>>(ix, q, q_off, short_id, n_short, probe_topk, semantics, exact); break;
-    case 2: rerank_kernel<2><<<grid, 256, sm, st>>>(ix, q, q_off, short_id, n_short, probe_topk, semantics, exact); break;
-    case 4: rerank_kernel<4><<<grid, 256, sm, st>>>(ix, q, q_off, short_id, n_short, probe_topk, semantics, exact); break;
-    case 8: rerank_kernel<8><<<grid, 256, sm, st>>>(ix, q, q_off, short_id, n_short, probe_topk, semantics, exact); break;
+    case 1: MVR_RK(1); break;
+    case 2: MVR_RK(2); break;
+    case 4: MVR_RK(4); break;
+    case 8: MVR_RK(8); break;
     default: return cudaErrorInvalidValue;
   }
+#undef MVR_RK
   *n_launch += 1;
   return cudaGetLastError();
 }

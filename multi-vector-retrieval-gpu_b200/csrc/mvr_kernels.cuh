@@ -86,8 +86,8 @@ cudaError_t launch_filter_hash(const DevIndex &ix, const uint32_t *probe_id,
 cudaError_t launch_rerank(const DevIndex &ix, const float *q, const uint64_t *q_off,
                           uint32_t n_query, const uint32_t *short_id,
                           const uint32_t *n_short, uint32_t probe_topk,
-                          int semantics, float *exact, cudaStream_t st,
-                          int *n_launch);
+                          int semantics, float *exact, unsigned *err, cudaStream_t st,
+                          int *n_launch, uint64_t wait_ns);
 cudaError_t launch_topk(const uint32_t *short_id, const float *exact,
                         const uint32_t *n_short, uint32_t n_query,
                         uint32_t probe_topk, uint32_t topk, float *out_s,

@@ -14,6 +14,7 @@
 // best of them with the exact FP32 kernel.
 #include "mvr_common.cuh"
 #include "mvr_tc.cuh"
+#include "mvr_mbar.cuh"
 
 #include <cuda_bf16.h>
 #include <cuda_fp8.h>
@@ -29,11 +30,6 @@ constexpr unsigned kFull = 0xffffffffu;
 constexpr int kTcTile = 128;      // doc tokens per MMA tile (M)
 constexpr int kTcDocs = 32;       // shortlisted docs per CTA
 constexpr int kTcThreads = 256;
-constexpr uint64_t kWaitNs = 1000000000ull;  // mbarrier wait bound (1 s)
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
 
 // K-major SWIZZLE_128B UMMA shared-memory descriptor: 8-row x 128 B atoms,
 // SBO = 1024 B between 8-row groups, LBO unused (1), version 1 (sm_100).
@@ -50,36 +46,6 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int m, int n) {
 // byte offset of element (row, k) in a [rows][64] BF16 K-block, 128B swizzle
 __device__ __forceinline__ uint32_t sw128_off(uint32_t row, uint32_t chunk16) {
   return (row >> 3) * 1024u + (row & 7u) * 128u + ((chunk16 ^ (row & 7u)) << 4);
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count));
-}
-
-// Bounded wait on an mbarrier phase: try_wait suspends the thread until the
-// phase completes (or a hardware time slice passes); gives up after ~1 s of
-// %globaltimer and returns false.
-__device__ __forceinline__ uint64_t global_ns() {
-  uint64_t t;
-  asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
-  return t;
-}
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity,
-                                          uint64_t limit_ns = kWaitNs) {
-  const uint32_t a = smem_u32(bar);
-  uint64_t t0 = 0;
-  for (uint32_t i = 0;; i++) {
-    uint32_t done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        " selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (done) return true;
-    if (i == 0) t0 = global_ns();
-    else if (global_ns() - t0 > limit_ns) return false;
-  }
 }
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
@@ -1305,9 +1271,6 @@ __host__ __device__ constexpr size_t ws_smem_bytes(int nbit, int nmax) {
                     : 120 * 1024;
 }
 
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
-}
 __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)),
                "r"(bytes)

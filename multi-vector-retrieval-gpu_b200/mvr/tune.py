@@ -18,18 +18,22 @@ from .formats import recall_at_k
 
 
 def tune(index, queries, gnd_ids, k, nprobe, target, semantics,
-         probe_topks=(100, 150, 200, 300, 400, 600, 800, 1000, 1500, 2000),
+         probe_topks=(100, 150, 200, 300, 400, 600, 800, 1000, 1500, 2000, 3000, 4000,
+                     6000, 8000),
          rescores=(0,), repeats=3, tok_off=None):
     """queries: float32 [n_query, n_tok, 128] (host), or [total_tokens, 128]
     with tok_off (uint64 [n_query + 1]) for ragged queries; gnd_ids:
     [n_query, >= k].
     Returns dict(probe_topk, rescore, recall, ms, table, reached) for the
     smallest setting with mean recall@k >= target (the most accurate one if
-    none reaches it); `table` lists every setting measured."""
+    none reaches it); the ascending grid is measured up to the first setting
+    that reaches the target, and `table` lists every setting measured."""
     table = []
     for ptk in probe_topks:
         if ptk < k:
             continue
+        if table and any(t["recall"] >= target for t in table):
+            break  # the grid ascends: the smallest setting reaching the target is known
         for r in rescores:
             if r and (r < k or r > ptk):
                 continue
