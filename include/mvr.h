@@ -60,17 +60,20 @@ typedef enum {
                             reference's. */
 
 #define MVR_PRUNE 16u /* learned candidate pruner (no counterpart in the
-                          reference; needs MVR_PREC_FP8, a 2- or 4-bit
-                          index, queries of up to 32 tokens and weights set
-                          by mvr_index_set_pruner): after the shortlist, the
-                          pruner's MLP predicts each shortlisted doc's
-                          MaxSim from its features, and the FP8 MaxSim
-                          scores only the `keep` docs with the best
-                          predictions -- unless the query's R-th best
-                          prediction leads its keep-th best by less than
-                          `margin` (low confidence), when it scores the whole
-                          shortlist.  The exact FP32 re-score stays the judge
-                          of the final top-k. */
+                          reference; needs a 2- or 4-bit index, queries of
+                          up to 32 tokens and weights set by
+                          mvr_index_set_pruner; alone, or with
+                          MVR_PREC_FP8): after the shortlist, the pruner's
+                          MLP predicts each shortlisted doc's MaxSim from its
+                          features, and only the `keep` docs with the best
+                          predictions are decompressed and scored -- by the
+                          exact FP32 MaxSim (no precision flag) or by the FP8
+                          MaxSim then the exact FP32 re-score (MVR_PREC_FP8)
+                          -- unless the query's R-th best prediction (R = the
+                          re-score count, 4 k by default) leads its keep-th
+                          best by less than `margin` (low confidence), when
+                          the whole shortlist is scored.  Returned scores are
+                          always exact FP32 MaxSim. */
 
 typedef struct mvr_index mvr_index;
 
@@ -280,7 +283,7 @@ int mvr_index_set_pruner(mvr_index *h, const float *params, uint32_t keep,
                          float margin);
 
 /* Tile shape of the FP8 MaxSim kernel (MVR_PREC_FP8): shortlisted docs per
- * CTA, 32, 64 or 128 (0: the default, 64); chosen by the library's tuner
+ * CTA, 32, 64 or 128 (0: the default, 128); chosen by the library's tuner
  * (mvr.tune.tune_tile).  No counterpart in the reference. */
 int mvr_index_set_rerank_tile(mvr_index *h, uint32_t docs_per_cta);
 

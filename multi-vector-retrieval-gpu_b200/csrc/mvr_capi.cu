@@ -170,7 +170,7 @@ struct mvr_index {
   // queries of the previous search call (0: none yet)
   double cand_per_probe = 0.0;
   uint64_t wait_ns = 1000000000ull;  // bound of the FP8 rerank's pipeline waits
-  uint32_t ws_docs = 64;             // shortlisted docs per CTA of the FP8 rerank
+  uint32_t ws_docs = 128;            // shortlisted docs per CTA of the FP8 rerank
   // learned pruner (mvr_index_set_pruner): BF16 weight tiles, b1/b2/w3/b3
   uint8_t *prune_wts = nullptr;
   float *prune_vecs = nullptr;
@@ -475,8 +475,13 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
   MVR_TRY(build_offsets(tok_off_in, n_query, query_n_vec, off, &nq_max));
   const bool prune = (flags & MVR_PRUNE) != 0;
   if (prune) {
-    if (!fp8 || !(flags & MVR_PREC_FP8))
-      return set_err(MVR_ERR_UNSUPPORTED, "MVR_PRUNE needs MVR_PREC_FP8 on a 2- or 4-bit index");
+    // the features come from the FP8 centroid table (2- and 4-bit indexes);
+    // the pruned docs go to the FP8 MaxSim (with MVR_PREC_FP8) or straight
+    // to the exact FP32 rerank (no precision flag)
+    if (!h->cen8)
+      return set_err(MVR_ERR_UNSUPPORTED, "MVR_PRUNE needs a 2- or 4-bit index");
+    if (bf16 && !(flags & MVR_PREC_FP8))
+      return set_err(MVR_ERR_UNSUPPORTED, "MVR_PRUNE: with a precision flag, MVR_PREC_FP8");
     if (!h->prune_wts) return set_err(MVR_ERR_INVALID_ARG, "MVR_PRUNE: no pruner set");
     if (nq_max > 32) return set_err(MVR_ERR_UNSUPPORTED, "MVR_PRUNE: queries of up to 32 tokens");
   }
@@ -634,11 +639,28 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
         CUDA_TRY(launch_topk(w.r_id, w.r_exact, w.n_r, nb, R, topk, os, oi, nullptr, rs,
                              &launches));
       } else {
-        CUDA_TRY(launch_rerank(h->dix, qp, qo, nb, w.short_id, w.n_short, probe_topk, sem,
-                               w.exact, h->d_err, rs, &launches, h->wait_ns));
+        // exact FP32 MaxSim over the shortlist -- with MVR_PRUNE over the docs
+        // the pruner keeps (its fallback: the whole shortlist)
+        const uint32_t *sid = w.short_id, *nsh = w.n_short;
+        if (prune) {
+          CUDA_TRY(launch_prune_features(h->dix, h->cen8, qp, qo, nb, w.short_id, w.n_short,
+                                         probe_topk, h->x_bound, w.feat, h->d_err, rs,
+                                         &launches, h->wait_ns));
+          CUDA_TRY(launch_prune_mlp(w.feat, w.n_short, nb, probe_topk, h->prune_wts,
+                                    h->prune_vecs, w.pred, h->d_err, h->n_sm, rs, &launches));
+          CUDA_TRY(launch_topk(w.short_id, w.pred, w.n_short, nb, probe_topk, keep, w.kept_s,
+                               w.kept_id, nullptr, rs, &launches));
+          CUDA_TRY(launch_prune_choose(h->dix, w.short_id, w.n_short, w.kept_id, w.kept_s, nb,
+                                       probe_topk, keep, R, h->prune_margin, w.fin_id, w.n_fin,
+                                       w.qstat + (size_t)s * 3, h->d_fallback, rs, &launches));
+          sid = w.fin_id;
+          nsh = w.n_fin;
+        }
+        CUDA_TRY(launch_rerank(h->dix, qp, qo, nb, sid, nsh, probe_topk, sem, w.exact, h->d_err,
+                               rs, &launches, h->wait_ns));
         CUDA_TRY(rec(ev(bt, 4)));
-        CUDA_TRY(launch_topk(w.short_id, w.exact, w.n_short, nb, probe_topk, topk, os, oi,
-                             nullptr, rs, &launches));
+        CUDA_TRY(launch_topk(sid, w.exact, nsh, nb, probe_topk, topk, os, oi, nullptr, rs,
+                             &launches));
       }
       CUDA_TRY(rec(ev(bt, 5)));
       if (host_io) {
@@ -1162,7 +1184,7 @@ int mvr_index_set_pruner(mvr_index *h, const float *params, uint32_t keep, float
 
 int mvr_index_set_rerank_tile(mvr_index *h, uint32_t docs_per_cta) {
   if (!h) return set_err(MVR_ERR_INVALID_ARG, "null index handle");
-  if (docs_per_cta == 0) docs_per_cta = 64;
+  if (docs_per_cta == 0) docs_per_cta = 128;
   if (!ws_docs_supported(docs_per_cta))
     return set_err(MVR_ERR_INVALID_ARG, "docs per CTA %u: 32, 64 or 128", docs_per_cta);
   DeviceGuard g(h->device);

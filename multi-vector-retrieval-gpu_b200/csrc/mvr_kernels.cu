@@ -650,27 +650,39 @@ filter_hash_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
       const uint32_t *ids = ix.ivf_ids + lof[t * nprobe + j];
       // first visit: the probe score replaces the token's imputed score
       const unsigned long long add = (unsigned long long)(pfix[t * nprobe + j] - impf[t]);
-      for (uint32_t p = lane; p < sz; p += 32) {
-        const uint32_t it = __ldg(ids + p);
-        // find or insert `it` (linear probing; the fill limit keeps >= 1024
-        // slots empty, so the walk ends)
-        uint32_t h = (it * 2654435769u) >> (32 - kHashLog);
-        uint32_t slot = kEmpty;
-        for (uint32_t step = 0; step < kHashCap; step++) {
-          const uint32_t k = *reinterpret_cast<volatile uint32_t *>(&tkey[h]);
-          if (k == it) { slot = h; break; }
-          if (k == kEmpty) {
-            if (atomicAdd(&s_fill, 1u) >= kHashFill) { s_ovf = 1; break; }
-            const uint32_t old = atomicCAS(&tkey[h], kEmpty, it);
-            if (old == kEmpty) { slot = h; break; }
-            atomicSub(&s_fill, 1u);  // lost the slot to another insert
-            if (old == it) { slot = h; break; }
-          }
-          h = (h + 1) & (kHashCap - 1);
+      // 4 entries per lane in flight (the loads are independent; the
+      // entries of one probe carry the same score, so their order is free)
+      for (uint32_t p0 = 0; p0 < sz; p0 += 128) {
+        uint32_t its[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const uint32_t p = p0 + lane + 32u * u;
+          its[u] = p < sz ? __ldg(ids + p) : kEmpty;
         }
-        if (slot == kEmpty) continue;
-        const uint32_t old = atomicOr(&tmask[slot * MW + word], bit);
-        if (!(old & bit)) atomicAdd(&tacc[slot], add);
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const uint32_t it = its[u];
+          if (it == kEmpty) continue;
+          // find or insert `it` (linear probing; the fill limit keeps >= 1024
+          // slots empty, so the walk ends)
+          uint32_t h = (it * 2654435769u) >> (32 - kHashLog);
+          uint32_t slot = kEmpty;
+          for (uint32_t step = 0; step < kHashCap; step++) {
+            const uint32_t k = *reinterpret_cast<volatile uint32_t *>(&tkey[h]);
+            if (k == it) { slot = h; break; }
+            if (k == kEmpty) {
+              if (atomicAdd(&s_fill, 1u) >= kHashFill) { s_ovf = 1; break; }
+              const uint32_t old = atomicCAS(&tkey[h], kEmpty, it);
+              if (old == kEmpty) { slot = h; break; }
+              atomicSub(&s_fill, 1u);  // lost the slot to another insert
+              if (old == it) { slot = h; break; }
+            }
+            h = (h + 1) & (kHashCap - 1);
+          }
+          if (slot == kEmpty) continue;
+          const uint32_t old = atomicOr(&tmask[slot * MW + word], bit);
+          if (!(old & bit)) atomicAdd(&tacc[slot], add);
+        }
       }
       __syncwarp();  // rank j of token t before rank j + 1
     }
@@ -755,44 +767,50 @@ filter_select_kernel(DevIndex ix, uint32_t probe_topk, FilterScratch scr,
 // K3: decompress + exact MaxSim of up to kRkDocs shortlisted docs of one query.
 //
 // The docs' tokens, each doc padded to a multiple of 4 tokens, form a stream
-// of 512-token tiles; a tile is consumed in 8 chunks of 16 dimensions.
-//  warps 8-11  decoders: per chunk, each thread decodes 4 tokens (positions
-//              p, p+128, p+256, p+384 of the tile) x 16 dims,
+// of 256-token tiles; a tile is consumed in 8 chunks of 16 dimensions.  Two
+// CTAs of 256 threads per SM:
+//  warps 4-7   decoders (one warpgroup): per chunk, each thread decodes 2
+//              tokens (positions p and p + 128 of the tile) x 16 dims,
 //              x = centroid + W[bucket] (one rounded FP32 add; W from a table
 //              replicated across the 32 banks, read conflict-free), into
-//              stage i % kRkStages of a shared-memory ring [16 dims][512];
-//  warps 0-7   FMA: thread (warp w, lane l) owns query tokens 16(w&1)..+16 of
-//              the pass and doc tokens 128(w>>1) + 4l..+4 of the tile, so per
-//              dimension it reads 16 query values (4 broadcast LDS.128) and 4
-//              doc values (one LDS.128) for 64 FMAs: FMA-bound, not bound by
-//              shared-memory wavefronts.  After the 8th chunk of a tile: max
-//              over the thread's valid tokens (all of one doc, thanks to the
-//              padding), then per doc a __reduce_max_sync over the lanes
-//              holding it, folded into best[query token][doc] by atomicMax.
+//              stage i % kRkStages of a shared-memory ring [16 dims][256];
+//              the loads of chunk i + 1 are in flight while chunk i is
+//              decoded, and the next tile's tokens are located a tile ahead;
+//  warps 0-3   FMA (one warpgroup): thread (warp w, lane l) owns query tokens
+//              16(w&1)..+16 of the pass and doc tokens 128(w>>1) + 4l..+4 of
+//              the tile, so per dimension it reads 16 query values (4
+//              broadcast LDS.128) and 4 doc values (one LDS.128) for 64 FMAs.
+//              After the 8th chunk of a tile: max over the thread's valid
+//              tokens (all of one doc, thanks to the padding), then per doc a
+//              __reduce_max_sync over the lanes holding it, folded into
+//              best[query token][doc] by atomicMax.
+// Registers: the launch gives every thread 128; setmaxnreg lowers the FMA
+// warpgroup to 120 and raises the decoders to 136.
 // Queries of more than 32 tokens run in two passes (tokens 0-31, 32-63).
 // Ring handoff: mbarriers full[s] (the 128 decoder threads arrive) and
-// empty[s] (the 256 FMA threads arrive); every wait is bounded (wait_ns) and
+// empty[s] (the 128 FMA threads arrive); every wait is bounded (wait_ns) and
 // a timeout sets bit 32 of *err and stops the CTA without writing scores.
 // Every dot product is the sequential __fmaf_rn chain over d = 0..127 from
 // 0.0f, so the scores are bit-identical to the canonical arithmetic.
 // ---------------------------------------------------------------------
 constexpr int kRkDocs = 64;       // shortlisted docs per CTA
-constexpr int kRkTile = 512;      // doc tokens per tile
+constexpr int kRkTile = 256;      // doc tokens per tile
 constexpr int kRkChunk = 16;      // dimensions per ring stage
 constexpr int kRkStages = 4;      // ring stages
 constexpr int kRkQ = 32;          // query tokens per pass
-constexpr int kRkThreads = 512;   // 8 FMA warps + 8 decoder warps
-constexpr int kRkFma = 256;       // FMA threads
+constexpr int kRkThreads = 256;   // 4 FMA warps + 4 decoder warps (two CTAs per SM)
+constexpr int kRkFma = 128;       // FMA threads
 // registers per thread after the split (setmaxnreg): the launch gives every
-// thread 128 (65,536 / 512); the FMA warpgroups give 8 each back and the
-// decoder warpgroups take them, 256 x 120 + 256 x 136 = 512 x 128
+// thread 128 (65,536 / 512 for the SM's two CTAs); the FMA warpgroup gives 8
+// each back and the decoder warpgroup takes them, 128 x 120 + 128 x 136 =
+// 256 x 128
 constexpr int kRkRegLaunch = 128;
 constexpr int kRkRegFma = 120;
 constexpr int kRkRegDec = 136;
 static_assert(kRkFma * kRkRegFma + (kRkThreads - kRkFma) * kRkRegDec == kRkThreads * kRkRegLaunch,
               "register split must equal the launch allocation");
 
-// CTA-local barrier of the FMA warps only (named barrier 1, 256 threads)
+// CTA-local barrier of the FMA warps only (named barrier 1, kRkFma threads)
 __device__ __forceinline__ void fma_bar_sync() {
   asm volatile("bar.sync 1, %0;\n" ::"n"(kRkFma) : "memory");
 }
@@ -805,7 +823,7 @@ __host__ __device__ constexpr size_t rk_smem_bytes(int n_bit) {
 }
 
 template <int NBIT>
-__global__ void __launch_bounds__(kRkThreads, 1)
+__global__ void __launch_bounds__(kRkThreads, 2)
 rerank_kernel(DevIndex ix, const float *__restrict__ q, const uint64_t *__restrict__ q_off,
               const uint32_t *__restrict__ short_id, const uint32_t *__restrict__ n_short,
               uint32_t probe_topk, int semantics, float *__restrict__ exact,

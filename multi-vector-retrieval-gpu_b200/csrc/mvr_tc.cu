@@ -48,14 +48,6 @@ __device__ __forceinline__ uint32_t sw128_off(uint32_t row, uint32_t chunk16) {
   return (row >> 3) * 1024u + (row & 7u) * 128u + ((chunk16 ^ (row & 7u)) << 4);
 }
 
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(smem)), "l"(gmem));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
 
 __device__ __forceinline__ void tc_fence_before() {
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
@@ -80,6 +72,21 @@ __device__ __forceinline__ void mma_commit(uint64_t *bar) {
   asm volatile(
       "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
           smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+// 1-D bulk copy global -> shared (16-byte aligned addresses, size a multiple
+// of 16), completing on the mbarrier's transaction count
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes,
+                                         uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+          dst),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
       : "memory");
 }
 
@@ -885,25 +892,32 @@ __global__ void perm_centroid_kernel(const float *__restrict__ cen, uint32_t n_c
 // Centroid scoring on tensor cores.
 //
 // probe_tc_kernel: CTA = 128 query tokens (operand A, M = 128, BF16
-// swizzled in smem) x a range of 64-centroid tiles (operand B, N = 64).
-// Centroid tiles are stored pre-swizzled in HBM (cen_sw, 16 KB per tile) and
-// streamed by all threads with cp.async into a double buffer; one thread
+// swizzled in smem) x a range of 64-centroid tiles (operand B, N = 64),
+// warp-specialised.  Centroid tiles are stored pre-swizzled in HBM (cen_sw,
+// 16 KB per tile, contiguous); one thread of warp 4 streams them by 1-D bulk
+// copies (cp.async.bulk, mbarrier transaction count) into a 3-stage ring and
 // issues 8 tcgen05.mma per tile into a double-buffered TMEM accumulator
-// (2 x 64 columns) whose completion an mbarrier tracks, so the epilogue of
-// tile j-1 overlaps the MMA of tile j.  Epilogue: thread = token row reads its
-// 64 scores with tcgen05.ld (two 32-column chunks) and keeps the token's best
-// kCand of the split sorted in registers.  A chunk whose max beats the list's
+// (2 x 64 columns); commits hand D to the epilogue and free the ring stage,
+// and the epilogue releases D as soon as it has loaded it, so the MMAs of
+// tile j + 1 run while tile j is scanned.  Epilogue (warps 0-3): thread =
+// token row reads its 64 scores with tcgen05.ld (two 32-column chunks) and
+// keeps the token's best kCand of the split sorted in registers.  Every
+// mbarrier wait is bounded; a timeout sets bit 2 of *err and stops the CTA
+// after its MMAs and copies have completed.  A chunk whose max beats the list's
 // last score is staged in the thread's shared-memory row and only its
 // qualifying columns are inserted (branch-free 16-slot insertion).  Candidate
 // ids per token per split go to `cand`; probe_rescore_kernel recomputes their
 // scores exactly (canonical FP32 fma chain) and selects the top nprobe.
 // ---------------------------------------------------------------------
-constexpr int kPtTok = 128;     // tokens per CTA (M) = threads per CTA
+constexpr int kPtTok = 128;     // tokens per CTA (M) = epilogue threads
 constexpr int kPtCen = 64;      // centroids per tile (N)
 constexpr int kCand = 16;       // candidates kept per token per split
 constexpr int kStage = 36;      // staging row stride in floats (16 B aligned, conflict-free STS.128)
 constexpr uint32_t kPtTileBytes = kPtCen * 256;  // one swizzled BF16 centroid tile
-constexpr size_t kPtSmem = 1024 + 32768 /*A*/ + 2 * kPtTileBytes /*B*/ + kPtTok * kStage * 4 /*stage*/;
+constexpr int kPtStages = 3;    // centroid-tile ring stages
+constexpr int kPtThreads = 160;  // 4 epilogue warps (one thread per token row) + copy / MMA warp
+constexpr size_t kPtSmem = 1024 + 32768 /*A*/ + kPtStages * kPtTileBytes /*B ring*/ +
+                           kPtTok * kStage * 4 /*stage*/;
 
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
   asm volatile(
@@ -944,25 +958,25 @@ __device__ __forceinline__ void topk_insert(float (&s)[kCand], uint32_t (&d)[kCa
   d[0] = (bm & 1u) ? c : d[0];
 }
 
-__global__ void __launch_bounds__(kPtTok, 2)
+__global__ void __launch_bounds__(kPtThreads, 2)
 probe_tc_kernel(const float *__restrict__ q, uint32_t n_tok, const uint8_t *__restrict__ cen_sw,
                 uint32_t n_cent, uint32_t tiles_per_split, uint32_t n_tiles,
                 uint32_t *__restrict__ cand, unsigned *__restrict__ err) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint8_t *Aq = smem;                  // [2 K-blocks][128 rows][128 B]
-  uint8_t *Bc = smem + 32768;          // [2 bufs][2 K-blocks][64 rows][128 B]
-  float *stage = reinterpret_cast<float *>(Bc + 2 * kPtTileBytes) + threadIdx.x * kStage;
-  __shared__ uint64_t done[2];
+  uint8_t *Bc = smem + 32768;          // [kPtStages][2 K-blocks][64 rows][128 B]
+  float *stage_base = reinterpret_cast<float *>(Bc + kPtStages * kPtTileBytes);
+  __shared__ uint64_t bfull[kPtStages], bfree[kPtStages], dfull[2], dfree[2], mdone;
   __shared__ uint32_t tmem_base_s;
-  __shared__ int s_abort;
+  __shared__ volatile int s_abort;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint32_t t0 = blockIdx.y * kPtTok;
   const uint32_t tile_begin = blockIdx.x * tiles_per_split;
   const uint32_t tile_end = min(n_tiles, tile_begin + tiles_per_split);
   if (tile_begin >= tile_end) return;
-  const uint32_t idesc = idesc_bf16(kPtTok, kPtCen);
+  const uint32_t n_local = tile_end - tile_begin;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
@@ -971,25 +985,20 @@ probe_tc_kernel(const float *__restrict__ q, uint32_t n_tok, const uint8_t *__re
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
   }
   if (tid == 0) {
-    mbar_init(&done[0], 1);
-    mbar_init(&done[1], 1);
+    for (int s = 0; s < kPtStages; s++) {
+      mbar_init(&bfull[s], 1);
+      mbar_init(&bfree[s], 1);
+    }
+    for (int d = 0; d < 2; d++) {
+      mbar_init(&dfull[d], 1);
+      mbar_init(&dfree[d], 4);
+    }
+    mbar_init(&mdone, 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     s_abort = 0;
   }
-  // pre-swizzled centroid tile -> B[buf]: 16 KB = 8 x 16 B per thread
-  auto load_tile = [&](uint32_t tile, int buf) {
-    const uint8_t *src = cen_sw + (size_t)tile * kPtTileBytes;
-    uint8_t *dst = Bc + buf * kPtTileBytes;
-#pragma unroll
-    for (int u = 0; u < (int)(kPtTileBytes / 16 / kPtTok); u++) {
-      const int o = (tid + u * kPtTok) * 16;
-      cp_async16(dst + o, src + o);
-    }
-    cp_async_commit();
-  };
-  load_tile(tile_begin, 0);
   // query tokens -> A (BF16, swizzled; rows >= n_tok zero)
-  for (int i = tid; i < kPtTok * 16; i += kPtTok) {
+  for (int i = tid; i < kPtTok * 16; i += kPtThreads) {
     const int row = i >> 4, ch = i & 15;
     uint4 v = make_uint4(0, 0, 0, 0);
     if (t0 + row < n_tok) {
@@ -1004,92 +1013,125 @@ probe_tc_kernel(const float *__restrict__ q, uint32_t n_tok, const uint8_t *__re
     }
     *reinterpret_cast<uint4 *>(Aq + (ch >> 3) * 16384 + sw128_off(row, ch & 7)) = v;
   }
+  fence_async_smem();  // A (generic stores) before the MMAs read it
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = tmem_base_s;
-  const uint32_t a_base = smem_u32(Aq), b_base = smem_u32(Bc);
-  float ts[kCand];     // this thread's token: best kCand scores of the split so far
-  uint32_t td[kCand];  // and their centroid ids
-#pragma unroll
-  for (int k = 0; k < kCand; k++) { ts[k] = -INFINITY; td[k] = 0xffffffffu; }
 
-  auto wait_mma = [&](uint32_t j) -> bool {  // MMA of local tile j complete
-    const bool ok = __all_sync(kFull, mbar_wait(&done[j & 1], (j >> 1) & 1));
-    if (!ok && lane == 0) { atomicOr(err, 2u); s_abort = 1; }
-    return ok;
-  };
-  auto epilogue = [&](uint32_t j) {  // MMA j known complete
-    tc_fence_after();
+  if (warp == 4) {
+    // ---------------- copies and MMA issue (one thread) ----------------
+    if (lane == 0) {
+      const uint32_t idesc = idesc_bf16(kPtTok, kPtCen);
+      const uint32_t a_base = smem_u32(Aq), b_base = smem_u32(Bc);
+      uint32_t issued = 0;  // tiles whose copy was issued
+      bool ok = true;
+      // tile j -> ring stage j % kPtStages, once the MMA that read the
+      // stage's previous tile has completed
+      auto copy = [&](uint32_t j) -> bool {
+        const uint32_t s = j % kPtStages;
+        if (j >= (uint32_t)kPtStages &&
+            !mbar_wait(&bfree[s], ((j / kPtStages) + 1) & 1, kWaitNs))
+          return false;
+        mbar_expect_tx(&bfull[s], kPtTileBytes);
+        bulk_g2s(b_base + s * kPtTileBytes, cen_sw + (size_t)(tile_begin + j) * kPtTileBytes,
+                 kPtTileBytes, &bfull[s]);
+        issued = j + 1;
+        return true;
+      };
+      for (uint32_t j = 0; j < n_local && j + 1 < (uint32_t)kPtStages && ok; j++) ok = copy(j);
+      uint32_t j = 0;
+      for (; ok && j < n_local; j++) {
+        if (j + kPtStages - 1 < n_local && !copy(j + kPtStages - 1)) { ok = false; break; }
+        const uint32_t s = j % kPtStages, d = j & 1;
+        if (!mbar_wait(&bfull[s], (j / kPtStages) & 1, kWaitNs)) { ok = false; break; }
+        if (j >= 2 && !mbar_wait(&dfree[d], ((j >> 1) + 1) & 1, kWaitNs)) { ok = false; break; }
+        if (s_abort) { ok = false; break; }
+        tc_fence_after();
+        const uint32_t bt = b_base + s * kPtTileBytes;
 #pragma unroll
-    for (int part = 0; part < 2; part++) {
-      uint32_t r[32];
-      tmem_ld32(tmem + ((32u * warp) << 16) + (j & 1) * kPtCen + part * 32, r);
-      float mx = __uint_as_float(r[0]);
-#pragma unroll
-      for (int i = 1; i < 32; i++) mx = fmaxf(mx, __uint_as_float(r[i]));
-      const float thr = ts[kCand - 1];
-      if (__any_sync(kFull, mx > thr)) {
-        const uint32_t cbase = (tile_begin + j) * kPtCen + part * 32;
-        const uint32_t valid = cbase >= n_cent        ? 0u
-                               : n_cent - cbase >= 32 ? 0xffffffffu
-                                                      : (1u << (n_cent - cbase)) - 1u;
-        uint32_t m4[4] = {0, 0, 0, 0};
-#pragma unroll
-        for (int i = 0; i < 32; i++) m4[i >> 3] |= (__uint_as_float(r[i]) > thr ? 1u : 0u) << i;
-        uint32_t m = ((m4[0] | m4[1]) | (m4[2] | m4[3])) & valid;
-        if (m) {
-#pragma unroll
-          for (int i = 0; i < 8; i++)
-            reinterpret_cast<uint4 *>(stage)[i] =
-                make_uint4(r[4 * i], r[4 * i + 1], r[4 * i + 2], r[4 * i + 3]);
-          while (m) {
-            const int i = __ffs(m) - 1;
-            m &= m - 1;
-            const float v = stage[i];
-            if (v > ts[kCand - 1]) topk_insert(ts, td, v, cbase + i);
-          }
+        for (int kk = 0; kk < 8; kk++) {
+          const uint64_t ad = sw128_desc(a_base + (kk >> 2) * 16384 + (kk & 3) * 32);
+          const uint64_t bd = sw128_desc(bt + (kk >> 2) * (kPtTileBytes / 2) + (kk & 3) * 32);
+          mma_bf16(tmem + d * kPtCen, ad, bd, idesc, kk > 0 ? 1u : 0u);
         }
-        __syncwarp();
+        mma_commit(&dfull[d]);
+        mma_commit(&bfree[s]);
       }
+      if (!ok) {
+        atomicOr(err, 2u);
+        s_abort = 1;
+      }
+      mma_commit(&mdone);  // every MMA of this CTA has completed once this phase does
+      mbar_wait(&mdone, 0);
+      // the copies still in flight land before the CTA may exit
+      for (uint32_t i = issued > (uint32_t)kPtStages ? issued - kPtStages : 0; i < issued; i++)
+        mbar_wait(&bfull[i % kPtStages], (i / kPtStages) & 1);
     }
-    tc_fence_before();
-  };
-
-  const uint32_t n_local = tile_end - tile_begin;
-  for (uint32_t j = 0; j < n_local; j++) {
-    const int buf = j & 1;
-    // MMA j-1 read B[buf^1]: once it completed, stream tile j+1 into it
-    bool ok = true;
-    if (j >= 1) ok = wait_mma(j - 1);
-    if (j + 1 < n_local) load_tile(tile_begin + j + 1, buf ^ 1);
-    else cp_async_commit();
-    cp_async_wait<1>();  // this thread's part of tile j landed
-    fence_async_smem();
-    __syncthreads();     // all of tile j in smem; epilogue(j-2) done with D[buf]
-    if (s_abort) break;
-    if (tid == 0) {
+    __syncwarp();
+  } else {
+    // ---------------- epilogue: thread = token row ----------------
+    float *stage = stage_base + tid * kStage;
+    float ts[kCand];     // this thread's token: best kCand scores of the split so far
+    uint32_t td[kCand];  // and their centroid ids
+#pragma unroll
+    for (int k = 0; k < kCand; k++) { ts[k] = -INFINITY; td[k] = 0xffffffffu; }
+    for (uint32_t j = 0; j < n_local; j++) {
+      const uint32_t d = j & 1;
+      if (!__all_sync(kFull, mbar_wait(&dfull[d], (j >> 1) & 1, kWaitNs))) {
+        if (lane == 0) {
+          atomicOr(err, 2u);
+          s_abort = 1;
+        }
+        break;
+      }
       tc_fence_after();
-      const uint32_t bt = b_base + buf * kPtTileBytes;
+      uint32_t r0[32], r1[32];
+      tmem_ld32(tmem + ((32u * warp) << 16) + d * kPtCen, r0);
+      tmem_ld32(tmem + ((32u * warp) << 16) + d * kPtCen + 32, r1);
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&dfree[d]);
 #pragma unroll
-      for (int kk = 0; kk < 8; kk++) {
-        const uint64_t ad = sw128_desc(a_base + (kk >> 2) * 16384 + (kk & 3) * 32);
-        const uint64_t bd = sw128_desc(bt + (kk >> 2) * (kPtTileBytes / 2) + (kk & 3) * 32);
-        mma_bf16(tmem + buf * kPtCen, ad, bd, idesc, kk > 0 ? 1u : 0u);
+      for (int part = 0; part < 2; part++) {
+        const uint32_t(&r)[32] = part ? r1 : r0;
+        float mx = __uint_as_float(r[0]);
+#pragma unroll
+        for (int i = 1; i < 32; i++) mx = fmaxf(mx, __uint_as_float(r[i]));
+        const float thr = ts[kCand - 1];
+        if (__any_sync(kFull, mx > thr)) {
+          const uint32_t cbase = (tile_begin + j) * kPtCen + part * 32;
+          const uint32_t valid = cbase >= n_cent        ? 0u
+                                 : n_cent - cbase >= 32 ? 0xffffffffu
+                                                        : (1u << (n_cent - cbase)) - 1u;
+          uint32_t m4[4] = {0, 0, 0, 0};
+#pragma unroll
+          for (int i = 0; i < 32; i++) m4[i >> 3] |= (__uint_as_float(r[i]) > thr ? 1u : 0u) << i;
+          uint32_t m = ((m4[0] | m4[1]) | (m4[2] | m4[3])) & valid;
+          if (m) {
+#pragma unroll
+            for (int i = 0; i < 8; i++)
+              reinterpret_cast<uint4 *>(stage)[i] =
+                  make_uint4(r[4 * i], r[4 * i + 1], r[4 * i + 2], r[4 * i + 3]);
+            while (m) {
+              const int i = __ffs(m) - 1;
+              m &= m - 1;
+              const float v = stage[i];
+              if (v > ts[kCand - 1]) topk_insert(ts, td, v, cbase + i);
+            }
+          }
+          __syncwarp();
+        }
       }
-      mma_commit(&done[buf]);
+      if (__any_sync(kFull, s_abort != 0)) break;
     }
-    if (j >= 1 && ok) epilogue(j - 1);  // overlaps MMA j
-  }
-  cp_async_wait<0>();
-  if (!s_abort && wait_mma(n_local - 1)) epilogue(n_local - 1);
-  __syncthreads();
-  // this split's candidates of this token: [token][split][kCand], best first
-  if (t0 + tid < n_tok && !s_abort) {
-    uint4 *dst = reinterpret_cast<uint4 *>(cand + ((size_t)(t0 + tid) * gridDim.x + blockIdx.x) * kCand);
+    // this split's candidates of this token: [token][split][kCand], best first
+    if (t0 + tid < n_tok && !s_abort) {
+      uint4 *dst = reinterpret_cast<uint4 *>(cand + ((size_t)(t0 + tid) * gridDim.x + blockIdx.x) * kCand);
 #pragma unroll
-    for (int i = 0; i < kCand / 4; i++)
-      dst[i] = make_uint4(td[4 * i], td[4 * i + 1], td[4 * i + 2], td[4 * i + 3]);
+      for (int i = 0; i < kCand / 4; i++)
+        dst[i] = make_uint4(td[4 * i], td[4 * i + 1], td[4 * i + 2], td[4 * i + 3]);
+    }
   }
   tc_fence_before();
   __syncthreads();
@@ -1206,7 +1248,7 @@ cudaError_t launch_probe_tc(const float *q, uint32_t n_tok, const void *cen_sw, 
   const uint32_t n_tiles = (n_cent + kPtCen - 1) / kPtCen;
   const uint32_t per = (n_tiles + splits - 1) / splits;
   dim3 grid(splits, (n_tok + kPtTok - 1) / kPtTok);
-  probe_tc_kernel<<<grid, kPtTok, kPtSmem, st>>>(q, n_tok, reinterpret_cast<const uint8_t *>(cen_sw),
+  probe_tc_kernel<<<grid, kPtThreads, kPtSmem, st>>>(q, n_tok, reinterpret_cast<const uint8_t *>(cen_sw),
                                                  n_cent, per, n_tiles, cand, err);
   probe_rescore_kernel<<<(n_tok + 7) / 8, 256, 0, st>>>(q, n_tok, cen, n_cent, cand,
                                                        splits * kCand, nprobe, out_id, out_s);
@@ -1255,7 +1297,7 @@ cudaError_t launch_probe_tc(const float *q, uint32_t n_tok, const void *cen_sw, 
 // bulk copies still in flight and the MMA thread for its MMAs before TMEM
 // is freed.
 // ---------------------------------------------------------------------
-constexpr int kWsDocs = 64;          // shortlisted docs per CTA (default; 32, 64 or 128)
+constexpr int kWsDocs = 128;         // shortlisted docs per CTA (default; 32, 64 or 128)
 constexpr int kWsStages = 4;         // shared-memory ring stages (residual bytes of one tile)
 constexpr int kWsDStages = 3;        // D stages in TMEM
 constexpr int kWsThreads = 320;
@@ -1271,21 +1313,6 @@ __host__ __device__ constexpr size_t ws_smem_bytes(int nbit, int nmax) {
                     : 120 * 1024;
 }
 
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)),
-               "r"(bytes)
-               : "memory");
-}
-// 1-D bulk copy global -> shared (16-byte aligned addresses, size a multiple
-// of 16), completing on the mbarrier's transaction count
-__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes,
-                                         uint64_t *bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
-          dst),
-      "l"(src), "r"(bytes), "r"(smem_u32(bar))
-      : "memory");
-}
 __device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&r)[32]) {
   asm volatile(
       "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
@@ -2026,7 +2053,8 @@ cudaError_t configure_tc_kernels() {
   MVR_WS_ATTR(2, 64, false, 32) MVR_WS_ATTR(2, 64, false, 64) MVR_WS_ATTR(2, 64, false, 128)
   MVR_WS_ATTR(4, 32, false, 32) MVR_WS_ATTR(4, 32, false, 64) MVR_WS_ATTR(4, 32, false, 128)
   MVR_WS_ATTR(4, 64, false, 32) MVR_WS_ATTR(4, 64, false, 64) MVR_WS_ATTR(4, 64, false, 128)
-  MVR_WS_ATTR(2, 32, true, 64) MVR_WS_ATTR(4, 32, true, 64)
+  // the pruner's feature launch: the default docs per CTA
+  MVR_WS_ATTR(2, 32, true, kWsDocs) MVR_WS_ATTR(4, 32, true, kWsDocs)
 #undef MVR_WS_ATTR
   e = cudaFuncSetAttribute(prune_mlp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMlpSmem);
   if (e != cudaSuccess) return e;

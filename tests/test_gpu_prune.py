@@ -208,3 +208,39 @@ def test_prune_search_keep_and_fallback():
             if d != 0xFFFFFFFF:
                 assert sc == o.maxsim_item(q[off[k]:off[k + 1]], int(d))
     g.close()
+
+
+def test_prune_plain_path_keep_and_fallback():
+    """MVR_PRUNE without a precision flag (the pruned docs go straight to the
+    exact FP32 MaxSim): keep >= shortlist gives the plain path's results bit
+    for bit; a margin no gap reaches falls back on every query, same results;
+    margin -inf scores only the kept docs, and every returned score is the
+    exact FP32 MaxSim of its doc (the oracle's canonical arithmetic)."""
+    from helpers import make_queries, oracle_of
+    from mvr import PRUNE, prune
+    ix, g = _index(4, seed=85)
+    o = oracle_of(ix)
+    q, off = make_queries(ix, 12, 32, seed=86)
+    X, y, _ = prune.traces(g, q, off, 5, 150, per_query=40, seed=2)
+    params, _ = prune.train(X, y, epochs=20, batch=256, lr=2e-3)
+    s0, i0 = g.search(q.reshape(12, 32, 128), 10, 5, 150, semantics=0)
+    g.set_pruner(params, 150, 0.0)
+    s, i = g.search(q.reshape(12, 32, 128), 10, 5, 150, semantics=PRUNE)
+    np.testing.assert_array_equal(i, i0)
+    np.testing.assert_array_equal(s, s0)
+    g.set_pruner(params, 60, 1e9)
+    s, i, st = g.search(q.reshape(12, 32, 128), 10, 5, 150, semantics=PRUNE, with_stats=True)
+    np.testing.assert_array_equal(i, i0)
+    np.testing.assert_array_equal(s, s0)
+    assert st["n_prune_fallback"] == 12
+    g.set_pruner(params, 60, -1e9)
+    s, i, st = g.search(q.reshape(12, 32, 128), 10, 5, 150, semantics=PRUNE, with_stats=True)
+    assert st["n_prune_fallback"] == 0
+    assert st["n_rerank_tok"] < sum(
+        int(ix["item_n_vec"][int(d)]) for k in range(12) for d in
+        g.trace(q[off[k]:off[k + 1]], 10, 5, 150)["short_id"])
+    for k in range(12):
+        for d, sc in zip(i[k], s[k]):
+            if d != 0xFFFFFFFF:
+                assert sc == o.maxsim_item(q[off[k]:off[k + 1]], int(d))
+    g.close()
