@@ -361,6 +361,20 @@ int mvr_pack_residual_device(const float *d_vec, uint64_t n_vec,
                              uint32_t n_bit, uint8_t *d_out,
                              void *cuda_stream);
 
+/* Bucket cutoffs and weights of the residual quantizer (GPU counterpart of
+ * ComputeQuantizedScalarPack, ResidualScalarQuantizationPack.hpp:17-100):
+ * over all n_vec * 128 residual errors e = vec - centroid[code] (one rounded
+ * FP32 subtraction), cutoff_out[c] (host, 2^n_bit - 1 values) = the
+ * floor((c + 1) / 2^n_bit * N)-th smallest, weight_out[w] (host, 2^n_bit
+ * values) = the floor((w + 0.5) / 2^n_bit * N)-th smallest (0-based ranks,
+ * the reference's nth_element positions), selected exactly by two
+ * histogram passes over order keys. */
+int mvr_residual_quantiles_device(const float *d_vec, uint64_t n_vec,
+                                  const float *d_centroid, uint32_t dim,
+                                  const uint32_t *d_code, uint32_t n_bit,
+                                  float *cutoff_out, float *weight_out,
+                                  void *cuda_stream);
+
 /* FP64 k-means update: sum[c][d] += vec[i][d] and count[c] += 1 over
  * code[i] == c (double accumulation; caller zeroes sum/count). */
 int mvr_kmeans_accumulate_device(const float *d_vec, uint64_t n_vec,

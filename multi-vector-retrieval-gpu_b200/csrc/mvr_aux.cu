@@ -4,6 +4,9 @@
 // FP64 k-means accumulation).
 #include "mvr_aux.cuh"
 
+#include <cstring>
+#include <vector>
+
 namespace mvr {
 
 // ct[k][c] = centroid[c][k] for c < C, 0 for C <= c < C_pad.
@@ -136,6 +139,119 @@ cudaError_t launch_kmeans_accumulate(const float *vec, uint64_t n_vec, const uin
   kmeans_accumulate_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(
       vec, n_vec, code, sum, reinterpret_cast<unsigned long long *>(count));
   return cudaGetLastError();
+}
+
+// Order statistics of the residual errors e = vec[i][d] - centroid[code[i]][d]
+// (one rounded FP32 subtraction, as the codec computes them), without
+// materialising them: e is mapped to a 32-bit key whose unsigned order is
+// the float order; pass 1 counts the keys' high 16 bits, pass 2 the low 16
+// bits of the keys inside the high-half bins that hold a wanted rank.
+__device__ __forceinline__ uint32_t order_key(float f) {
+  const uint32_t u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+__global__ void residual_hist_hi_kernel(const float *__restrict__ vec, uint64_t n_vec,
+                                        const float *__restrict__ cen,
+                                        const uint32_t *__restrict__ code,
+                                        unsigned long long *__restrict__ hist) {
+  const uint64_t n = n_vec * kDim;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t v = i / kDim;
+    const uint32_t d = (uint32_t)(i % kDim);
+    const float e = __fsub_rn(vec[i], cen[(size_t)code[v] * kDim + d]);
+    atomicAdd(hist + (order_key(e) >> 16), 1ull);
+  }
+}
+
+// slot_of[hi] = index of the wanted high half hi among the pass-2 histograms
+// (-1: none); hist2[slot][lo]
+__global__ void residual_hist_lo_kernel(const float *__restrict__ vec, uint64_t n_vec,
+                                        const float *__restrict__ cen,
+                                        const uint32_t *__restrict__ code,
+                                        const int *__restrict__ slot_of,
+                                        unsigned long long *__restrict__ hist2) {
+  const uint64_t n = n_vec * kDim;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t v = i / kDim;
+    const uint32_t d = (uint32_t)(i % kDim);
+    const uint32_t k = order_key(__fsub_rn(vec[i], cen[(size_t)code[v] * kDim + d]));
+    const int sl = slot_of[k >> 16];
+    if (sl >= 0) atomicAdd(hist2 + (size_t)sl * 65536u + (k & 0xffffu), 1ull);
+  }
+}
+
+cudaError_t residual_select(const float *vec, uint64_t n_vec, const float *cen,
+                            const uint32_t *code, const uint64_t *rank, uint32_t n_rank,
+                            float *out, cudaStream_t st) {
+  if (n_rank == 0) return cudaSuccess;
+  const uint64_t n = n_vec * kDim;
+  for (uint32_t r = 0; r < n_rank; r++)
+    if (rank[r] >= n) return cudaErrorInvalidValue;
+  unsigned long long *hist = nullptr, *hist2 = nullptr;
+  int *slot_of = nullptr;
+  cudaError_t e = cudaMalloc(&hist, 65536 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMalloc(&slot_of, 65536 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&hist2, (size_t)n_rank * 65536 * sizeof(unsigned long long));
+  std::vector<unsigned long long> h(65536), h2;
+  std::vector<uint32_t> hi_of(n_rank);
+  std::vector<uint64_t> below(n_rank);  // keys in lower high-half bins
+  std::vector<int> slot(65536, -1);
+  std::vector<uint32_t> wanted;  // distinct high halves, in slot order
+  const unsigned grid = 148u * 8u;
+  if (e == cudaSuccess) e = cudaMemsetAsync(hist, 0, 65536 * sizeof(unsigned long long), st);
+  if (e == cudaSuccess) {
+    residual_hist_hi_kernel<<<grid, 256, 0, st>>>(vec, n_vec, cen, code, hist);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(h.data(), hist, 65536 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) {
+    for (uint32_t r = 0; r < n_rank; r++) {
+      uint64_t acc = 0;
+      uint32_t b = 0;
+      while (acc + h[b] <= rank[r]) acc += h[b++];
+      hi_of[r] = b;
+      below[r] = acc;
+      if (slot[b] < 0) {
+        slot[b] = (int)wanted.size();
+        wanted.push_back(b);
+      }
+    }
+    e = cudaMemcpyAsync(slot_of, slot.data(), 65536 * sizeof(int), cudaMemcpyHostToDevice, st);
+  }
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(hist2, 0, wanted.size() * 65536 * sizeof(unsigned long long), st);
+  if (e == cudaSuccess) {
+    residual_hist_lo_kernel<<<grid, 256, 0, st>>>(vec, n_vec, cen, code, slot_of, hist2);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) {
+    h2.resize(wanted.size() * 65536);
+    e = cudaMemcpyAsync(h2.data(), hist2, h2.size() * sizeof(unsigned long long),
+                        cudaMemcpyDeviceToHost, st);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) {
+    for (uint32_t r = 0; r < n_rank; r++) {
+      const unsigned long long *g = h2.data() + (size_t)slot[hi_of[r]] * 65536;
+      uint64_t acc = below[r];
+      uint32_t lo = 0;
+      while (acc + g[lo] <= rank[r]) acc += g[lo++];
+      const uint32_t k = (hi_of[r] << 16) | lo;
+      const uint32_t u = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
+      float f;
+      std::memcpy(&f, &u, 4);
+      out[r] = f;
+    }
+  }
+  cudaFree(hist);
+  cudaFree(slot_of);
+  cudaFree(hist2);
+  return e;
 }
 
 }  // namespace mvr

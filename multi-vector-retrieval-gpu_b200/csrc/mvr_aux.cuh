@@ -18,5 +18,10 @@ cudaError_t launch_pack_residual(const float *vec, uint64_t n_vec, const float *
                                  uint8_t *out, cudaStream_t st);
 cudaError_t launch_kmeans_accumulate(const float *vec, uint64_t n_vec, const uint32_t *code,
                                      double *sum, uint64_t *count, cudaStream_t st);
+// out[r] = the rank[r]-th smallest (0-based) residual error vec - centroid[code]
+// over all n_vec * 128 values (synchronises st)
+cudaError_t residual_select(const float *vec, uint64_t n_vec, const float *cen,
+                            const uint32_t *code, const uint64_t *rank, uint32_t n_rank,
+                            float *out, cudaStream_t st);
 
 }  // namespace mvr

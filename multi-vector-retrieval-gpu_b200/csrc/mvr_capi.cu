@@ -1472,6 +1472,28 @@ int mvr_pack_residual_device(const float *d_vec, uint64_t n_vec, const float *d_
   return MVR_OK;
 }
 
+int mvr_residual_quantiles_device(const float *d_vec, uint64_t n_vec, const float *d_centroid,
+                                  uint32_t dim, const uint32_t *d_code, uint32_t n_bit,
+                                  float *cutoff_out, float *weight_out, void *cuda_stream) {
+  if (dim != (uint32_t)kDim) return set_err(MVR_ERR_UNSUPPORTED, "dim %u not supported", dim);
+  if (n_bit != 1 && n_bit != 2 && n_bit != 4 && n_bit != 8)
+    return set_err(MVR_ERR_INVALID_ARG, "n_bit must be 1, 2, 4 or 8");
+  if (!d_vec || !d_centroid || !d_code || !cutoff_out || !weight_out)
+    return set_err(MVR_ERR_INVALID_ARG, "null argument");
+  if (n_vec == 0) return set_err(MVR_ERR_INVALID_ARG, "no vectors");
+  const uint32_t nq = 1u << n_bit;
+  const double n = (double)(n_vec * (uint64_t)kDim);
+  std::vector<uint64_t> rank;
+  for (uint32_t c = 0; c + 1 < nq; c++) rank.push_back((uint64_t)std::floor((1.0 * (c + 1) / nq) * n));
+  for (uint32_t w = 0; w < nq; w++) rank.push_back((uint64_t)std::floor((1.0 * w / nq + 0.5 / nq) * n));
+  std::vector<float> v(rank.size());
+  CUDA_TRY(residual_select(d_vec, n_vec, d_centroid, d_code, rank.data(), (uint32_t)rank.size(),
+                           v.data(), (cudaStream_t)cuda_stream));
+  for (uint32_t c = 0; c + 1 < nq; c++) cutoff_out[c] = v[c];
+  for (uint32_t w = 0; w < nq; w++) weight_out[w] = v[nq - 1 + w];
+  return MVR_OK;
+}
+
 int mvr_kmeans_accumulate_device(const float *d_vec, uint64_t n_vec, uint32_t dim,
                                  const uint32_t *d_code, double *d_sum, uint64_t *d_count,
                                  void *cuda_stream) {

@@ -653,6 +653,9 @@ filter_hash_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
       // 4 entries per lane in flight (the loads are independent; the
       // entries of one probe carry the same score, so their order is free)
       for (uint32_t p0 = 0; p0 < sz; p0 += 128) {
+        // a CTA past its fill limit stops: its query is redone by the
+        // rank-table filter
+        if (__any_sync(kFull, *reinterpret_cast<volatile uint32_t *>(&s_ovf) != 0u)) break;
         uint32_t its[4];
 #pragma unroll
         for (int u = 0; u < 4; u++) {
@@ -662,22 +665,31 @@ filter_hash_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
 #pragma unroll
         for (int u = 0; u < 4; u++) {
           const uint32_t it = its[u];
-          if (it == kEmpty) continue;
-          // find or insert `it` (linear probing; the fill limit keeps >= 1024
-          // slots empty, so the walk ends)
-          uint32_t h = (it * 2654435769u) >> (32 - kHashLog);
+          // find or insert `it` (linear probing; the walk is bounded by the
+          // table size, and a CTA stops inserting once its fill count passes
+          // the limit)
           uint32_t slot = kEmpty;
-          for (uint32_t step = 0; step < kHashCap; step++) {
-            const uint32_t k = *reinterpret_cast<volatile uint32_t *>(&tkey[h]);
-            if (k == it) { slot = h; break; }
-            if (k == kEmpty) {
-              if (atomicAdd(&s_fill, 1u) >= kHashFill) { s_ovf = 1; break; }
-              const uint32_t old = atomicCAS(&tkey[h], kEmpty, it);
-              if (old == kEmpty) { slot = h; break; }
-              atomicSub(&s_fill, 1u);  // lost the slot to another insert
-              if (old == it) { slot = h; break; }
+          bool inserted = false;
+          if (it != kEmpty) {
+            uint32_t h = (it * 2654435769u) >> (32 - kHashLog);
+            for (uint32_t step = 0; step < kHashCap; step++) {
+              const uint32_t k = *reinterpret_cast<volatile uint32_t *>(&tkey[h]);
+              if (k == it) { slot = h; break; }
+              if (k == kEmpty) {
+                const uint32_t old = atomicCAS(&tkey[h], kEmpty, it);
+                if (old == kEmpty) { slot = h; inserted = true; break; }
+                if (old == it) { slot = h; break; }
+              }
+              h = (h + 1) & (kHashCap - 1);
             }
-            h = (h + 1) & (kHashCap - 1);
+            if (slot == kEmpty) s_ovf = 1;  // the table is full
+          }
+          // the fill count (distinct docs inserted): one shared atomic per
+          // warp and round instead of one per insert on a single address
+          const unsigned ins = __ballot_sync(kFull, inserted);
+          if (lane == 0 && ins) {
+            const uint32_t n = (uint32_t)__popc(ins);
+            if (atomicAdd(&s_fill, n) + n > kHashFill) s_ovf = 1;
           }
           if (slot == kEmpty) continue;
           const uint32_t old = atomicOr(&tmask[slot * MW + word], bit);
@@ -689,9 +701,10 @@ filter_hash_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
   }
   __syncthreads();
 
-  // emit this CTA's candidates as (score, id) keys (at most kHashFill per CTA)
+  // emit this CTA's candidates as (score, id) keys (at most kHashFill per CTA:
+  // an overflowed CTA emits none, its query is redone by the rank-table filter)
   uint64_t *key = scr.hkey + (size_t)b * scr.key_stride;
-  for (uint32_t s0 = 0; s0 < kHashCap; s0 += blockDim.x) {
+  for (uint32_t s0 = 0; s0 < kHashCap && !s_ovf; s0 += blockDim.x) {
     const uint32_t sl = s0 + tid;
     const uint32_t k = sl < kHashCap ? tkey[sl] : kEmpty;
     const bool has = k != kEmpty;
