@@ -31,7 +31,7 @@ EXPORTS = (
     "mvr_search", "mvr_search_staged",
     "mvr_search_device", "mvr_search_trace", "mvr_decompress", "mvr_unpack_buckets",
     "mvr_assign_device", "mvr_assign_tc_device", "mvr_pack_residual_device",
-    "mvr_kmeans_accumulate_device",
+    "mvr_kmeans_accumulate_device", "mvr_residual_quantiles_device",
     "mvr_filter_noalloc", "mvr_index_set_wait_limit",
     "mvr_mlp_work_floats", "mvr_mlp_train_step", "mvr_mlp_forward", "mvr_index_set_pruner",
     "mvr_index_set_rerank_tile",
@@ -113,6 +113,7 @@ def lib():
         "mvr_assign_tc_device": [vp, u64, vp, u32, u32, vp, vp, vp],
         "mvr_pack_residual_device": [vp, u64, vp, u32, vp, vp, u32, vp, vp],
         "mvr_kmeans_accumulate_device": [vp, u64, u32, vp, vp, vp, vp],
+        "mvr_residual_quantiles_device": [vp, u64, vp, u32, vp, u32, vp, vp, vp],
         "mvr_filter_noalloc": [vp, vp, vp, u32, u32, u32, vp, vp, vp, vp],
         "mvr_index_set_wait_limit": [vp, u64],
         "mvr_mlp_train_step": [vp, vp, u32, vp, vp, vp, vp, C.c_float, u32, vp, vp],
