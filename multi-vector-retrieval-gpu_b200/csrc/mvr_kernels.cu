@@ -591,7 +591,8 @@ filter_hash_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
   __shared__ uint64_t lof[kMaxQueryTok * kMaxProbe];   // and offsets in ivf_ids
   __shared__ long long impf[kMaxQueryTok];  // imputed score of an unmatched token (0: off)
   __shared__ long long s_imp;               // sum of impf over the query's tokens
-  __shared__ uint32_t s_fill, s_ovf, s_entries, s_b;
+  __shared__ uint32_t s_fill, s_ovf, s_entries, s_b, s_kbase;
+  __shared__ uint32_t s_wsum[32];
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int n_warp = blockDim.x >> 5;
@@ -604,7 +605,6 @@ filter_hash_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
   const uint32_t pstep = (uint32_t)kHashParts / (uint32_t)(cta_off[b + 1] - cta_off[b]);
   const uint64_t tok0 = q_off[b];
   const uint32_t nq = (uint32_t)(q_off[b + 1] - tok0);
-  const unsigned lt_mask = (1u << lane) - 1u;
 
   for (uint32_t i = tid; i < kHashCap; i += blockDim.x) {
     tkey[i] = kEmpty;
@@ -702,19 +702,37 @@ filter_hash_kernel(DevIndex ix, const uint32_t *__restrict__ probe_id,
   __syncthreads();
 
   // emit this CTA's candidates as (score, id) keys (at most kHashFill per CTA:
-  // an overflowed CTA emits none, its query is redone by the rank-table filter)
+  // an overflowed CTA emits none, its query is redone by the rank-table
+  // filter).  One global atomic per CTA reserves the CTA's key range: each
+  // thread counts its slots (tid, tid + blockDim, ...), a block scan gives
+  // its offset, and it writes its keys there.
   uint64_t *key = scr.hkey + (size_t)b * scr.key_stride;
-  for (uint32_t s0 = 0; s0 < kHashCap && !s_ovf; s0 += blockDim.x) {
-    const uint32_t sl = s0 + tid;
-    const uint32_t k = sl < kHashCap ? tkey[sl] : kEmpty;
-    const bool has = k != kEmpty;
-    const unsigned m = __ballot_sync(kFull, has);
-    if (m) {
-      uint32_t base = 0;
-      if (lane == __ffs(m) - 1) base = atomicAdd(scr.qcnt + b, (uint32_t)__popc(m));
-      base = __shfl_sync(kFull, base, __ffs(m) - 1);
-      if (has)
-        key[base + __popc(m & lt_mask)] = make_key(from_fixed((long long)tacc[sl] + s_imp), k);
+  if (!s_ovf) {
+    uint32_t mine = 0;
+    for (uint32_t sl = tid; sl < kHashCap; sl += blockDim.x) mine += tkey[sl] != kEmpty ? 1u : 0u;
+    uint32_t inc = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t v = __shfl_up_sync(kFull, inc, o);
+      if (lane >= o) inc += v;
+    }
+    if (lane == 31) s_wsum[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+      uint32_t w = lane < n_warp ? s_wsum[lane] : 0u, wi = w;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(kFull, wi, o);
+        if (lane >= o) wi += v;
+      }
+      if (lane < n_warp) s_wsum[lane] = wi - w;  // exclusive warp offsets
+      if (lane == 31) s_kbase = wi ? atomicAdd(scr.qcnt + b, wi) : 0u;
+    }
+    __syncthreads();
+    uint32_t pos = s_kbase + s_wsum[warp] + inc - mine;
+    for (uint32_t sl = tid; sl < kHashCap; sl += blockDim.x) {
+      const uint32_t k = tkey[sl];
+      if (k != kEmpty) key[pos++] = make_key(from_fixed((long long)tacc[sl] + s_imp), k);
     }
   }
   if (tid == 0) {
