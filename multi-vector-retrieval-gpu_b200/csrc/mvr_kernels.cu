@@ -280,6 +280,8 @@ __device__ __forceinline__ uint32_t *cl_ptr(uint32_t *p, uint32_t rank) {
   }
 }
 
+constexpr int kSelU = 8;  // candidate keys per thread in flight in the select passes
+
 // Shared-memory state of select_emit.
 struct SelectSmem {
   uint32_t (*hist)[256];  // [2][256]
@@ -309,15 +311,22 @@ __device__ void select_emit(const DevIndex &ix, const uint64_t *__restrict__ key
       uint32_t *h = sm.hist[pass & 1];
       for (int i = tid; i < 256; i += blockDim.x) h[i] = 0;
       __syncthreads();
-      for (uint32_t i0 = cr * blockDim.x; i0 < n_cand; i0 += cstride) {
-        const uint32_t i = i0 + tid;
-        uint32_t dig = 256;
-        if (i < n_cand) {
-          const uint64_t k = key[i];
-          if ((k & mask) == prefix) dig = (uint32_t)(k >> shift) & 0xffu;
+      // kSelU keys per thread in flight
+      for (uint32_t i0 = cr * blockDim.x; i0 < n_cand; i0 += kSelU * cstride) {
+        uint64_t kv[kSelU];
+#pragma unroll
+        for (int u = 0; u < kSelU; u++) {
+          const uint32_t i = i0 + u * cstride + tid;
+          kv[u] = i < n_cand ? key[i] : ~0ull;
         }
-        const unsigned grp = __match_any_sync(kFull, dig);
-        if (dig < 256 && lane == __ffs(grp) - 1) atomicAdd(&h[dig], (uint32_t)__popc(grp));
+#pragma unroll
+        for (int u = 0; u < kSelU; u++) {
+          const uint32_t i = i0 + u * cstride + tid;
+          uint32_t dig = 256;
+          if (i < n_cand && (kv[u] & mask) == prefix) dig = (uint32_t)(kv[u] >> shift) & 0xffu;
+          const unsigned grp = __match_any_sync(kFull, dig);
+          if (dig < 256 && lane == __ffs(grp) - 1) atomicAdd(&h[dig], (uint32_t)__popc(grp));
+        }
       }
       filter_sync<CL>();  // every CTA's histogram of this pass complete
       if (warp == 0) {
@@ -361,28 +370,33 @@ __device__ void select_emit(const DevIndex &ix, const uint64_t *__restrict__ key
   }
 
   // ---- phase D: emit the shortlist (unordered) ----
-  for (uint32_t i0 = cr * blockDim.x; i0 < n_cand; i0 += cstride) {
-    const uint32_t i = i0 + tid;
-    uint64_t k = 0;
-    bool sel = false;
-    if (i < n_cand) {
-      k = key[i];
-      sel = (k & mask) >= prefix;
+  for (uint32_t j0 = cr * blockDim.x; j0 < n_cand; j0 += kSelU * cstride) {
+    uint64_t kv[kSelU];
+#pragma unroll
+    for (int u = 0; u < kSelU; u++) {
+      const uint32_t i = j0 + u * cstride + tid;
+      kv[u] = i < n_cand ? key[i] : 0ull;
     }
-    const unsigned m = __ballot_sync(kFull, sel);
-    if (m) {
-      uint32_t base = 0;
-      if (lane == __ffs(m) - 1) base = atomicAdd(g_sel, (uint32_t)__popc(m));
-      base = __shfl_sync(kFull, base, __ffs(m) - 1);
-      const uint32_t pos = base + __popc(m & lt_mask);
-      uint32_t len = 0;
-      if (sel && pos < probe_topk) {
-        short_id[(size_t)b * probe_topk + pos] = key_id(k);
-        short_approx[(size_t)b * probe_topk + pos] = key_score(k);
-        len = ix.item_n_vec[key_id(k)];
+#pragma unroll
+    for (int u = 0; u < kSelU; u++) {
+      const uint32_t i = j0 + u * cstride + tid;
+      const uint64_t k = kv[u];
+      const bool sel = i < n_cand && (k & mask) >= prefix;
+      const unsigned m = __ballot_sync(kFull, sel);
+      if (m) {
+        uint32_t base = 0;
+        if (lane == __ffs(m) - 1) base = atomicAdd(g_sel, (uint32_t)__popc(m));
+        base = __shfl_sync(kFull, base, __ffs(m) - 1);
+        const uint32_t pos = base + __popc(m & lt_mask);
+        uint32_t len = 0;
+        if (sel && pos < probe_topk) {
+          short_id[(size_t)b * probe_topk + pos] = key_id(k);
+          short_approx[(size_t)b * probe_topk + pos] = key_score(k);
+          len = ix.item_n_vec[key_id(k)];
+        }
+        const uint32_t tot = __reduce_add_sync(kFull, len);
+        if (lane == 0 && tot) atomicAdd(g_stok, tot);
       }
-      const uint32_t tot = __reduce_add_sync(kFull, len);
-      if (lane == 0 && tot) atomicAdd(g_stok, tot);
     }
   }
 }
