@@ -283,7 +283,8 @@ int mvr_index_set_pruner(mvr_index *h, const float *params, uint32_t keep,
                          float margin);
 
 /* Tile shape of the FP8 MaxSim kernel (MVR_PREC_FP8): shortlisted docs per
- * CTA, 32, 64 or 128 (0: the default, 128); chosen by the library's tuner
+ * CTA, 32, 64, 128 or 256 (0: the default, 256; queries of more than 32
+ * tokens use at most 128); chosen by the library's tuner
  * (mvr.tune.tune_tile).  No counterpart in the reference. */
 int mvr_index_set_rerank_tile(mvr_index *h, uint32_t docs_per_cta);
 

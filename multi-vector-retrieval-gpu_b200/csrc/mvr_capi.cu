@@ -170,7 +170,7 @@ struct mvr_index {
   // queries of the previous search call (0: none yet)
   double cand_per_probe = 0.0;
   uint64_t wait_ns = 1000000000ull;  // bound of the FP8 rerank's pipeline waits
-  uint32_t ws_docs = 128;            // shortlisted docs per CTA of the FP8 rerank
+  uint32_t ws_docs = 256;            // shortlisted docs per CTA of the FP8 rerank
   // learned pruner (mvr_index_set_pruner): BF16 weight tiles, b1/b2/w3/b3
   uint8_t *prune_wts = nullptr;
   float *prune_vecs = nullptr;
@@ -1184,9 +1184,9 @@ int mvr_index_set_pruner(mvr_index *h, const float *params, uint32_t keep, float
 
 int mvr_index_set_rerank_tile(mvr_index *h, uint32_t docs_per_cta) {
   if (!h) return set_err(MVR_ERR_INVALID_ARG, "null index handle");
-  if (docs_per_cta == 0) docs_per_cta = 128;
+  if (docs_per_cta == 0) docs_per_cta = 256;
   if (!ws_docs_supported(docs_per_cta))
-    return set_err(MVR_ERR_INVALID_ARG, "docs per CTA %u: 32, 64 or 128", docs_per_cta);
+    return set_err(MVR_ERR_INVALID_ARG, "docs per CTA %u: 32, 64, 128 or 256", docs_per_cta);
   DeviceGuard g(h->device);
   h->ws_docs = docs_per_cta;
   h->drop_graph();

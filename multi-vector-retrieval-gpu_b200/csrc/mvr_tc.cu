@@ -1297,7 +1297,7 @@ cudaError_t launch_probe_tc(const float *q, uint32_t n_tok, const void *cen_sw, 
 // bulk copies still in flight and the MMA thread for its MMAs before TMEM
 // is freed.
 // ---------------------------------------------------------------------
-constexpr int kWsDocs = 128;         // shortlisted docs per CTA (default; 32, 64 or 128)
+constexpr int kWsDocs = 256;         // shortlisted docs per CTA (default; 32, 64, 128 or 256)
 constexpr int kWsStages = 4;         // shared-memory ring stages (residual bytes of one tile)
 constexpr int kWsDStages = 3;        // D stages in TMEM
 constexpr int kWsThreads = 320;
@@ -1353,7 +1353,8 @@ rerank_ws_kernel(DevIndex ix, const uint8_t *__restrict__ cen8, TmWeights tw,
   static_assert(NBIT == 2 || NBIT == 4, "FP8 decode of 2- and 4-bit codes");
   static_assert(NMAX == 32 || NMAX == 64, "query tiles of 32 or 64 rows");
   static_assert(!FEAT || NMAX == 32, "pruner features: queries of up to 32 tokens");
-  static_assert(DOCS == 32 || DOCS == 64 || DOCS == 128, "docs per CTA");
+  static_assert(DOCS == 32 || DOCS == 64 || DOCS == 128 || (DOCS == 256 && NMAX == 32),
+                "docs per CTA (256: the 32-column variant only, whose maxima fit static smem)");
   constexpr int S = kWsStages, SA = ws_astages(NMAX), SD = kWsDStages;
   constexpr uint32_t BPV = 128u * NBIT / 8u;       // residual bytes per token
   constexpr uint32_t STAGE = ws_stage_bytes(NBIT);
@@ -2050,6 +2051,7 @@ cudaError_t configure_tc_kernels() {
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ws_smem_bytes(NB, NM)); \
   if (e != cudaSuccess) return e;
   MVR_WS_ATTR(2, 32, false, 32) MVR_WS_ATTR(2, 32, false, 64) MVR_WS_ATTR(2, 32, false, 128)
+  MVR_WS_ATTR(2, 32, false, 256) MVR_WS_ATTR(4, 32, false, 256)
   MVR_WS_ATTR(2, 64, false, 32) MVR_WS_ATTR(2, 64, false, 64) MVR_WS_ATTR(2, 64, false, 128)
   MVR_WS_ATTR(4, 32, false, 32) MVR_WS_ATTR(4, 32, false, 64) MVR_WS_ATTR(4, 32, false, 128)
   MVR_WS_ATTR(4, 64, false, 32) MVR_WS_ATTR(4, 64, false, 64) MVR_WS_ATTR(4, 64, false, 128)
@@ -2192,7 +2194,9 @@ cudaError_t launch_rerank_tmem(const DevIndex &ix, const void *cen_perm, const T
   return cudaGetLastError();
 }
 
-bool ws_docs_supported(uint32_t docs) { return docs == 32 || docs == 64 || docs == 128; }
+bool ws_docs_supported(uint32_t docs) {
+  return docs == 32 || docs == 64 || docs == 128 || docs == 256;
+}
 
 template <int NB, int NM, int DOCS>
 static void ws_launch(const DevIndex &ix, const uint8_t *c, const TmWeights &tw, const float *q,
@@ -2214,7 +2218,11 @@ static void ws_launch_docs(uint32_t docs, const DevIndex &ix, const uint8_t *c,
   if (docs == 32)
     ws_launch<NB, NM, 32>(ix, c, tw, q, q_off, n_query, short_id, n_short, probe_topk, semantics,
                           x_bound, approx, err, st, wait_ns);
-  else if (docs == 128)
+  else if (docs == 256 && NM == 32)  // the 64-column variant's maxima would not fit: 128 there
+    ws_launch<NB, NM, NM == 32 ? 256 : 128>(ix, c, tw, q, q_off, n_query, short_id, n_short,
+                                            probe_topk, semantics, x_bound, approx, err, st,
+                                            wait_ns);
+  else if (docs >= 128)
     ws_launch<NB, NM, 128>(ix, c, tw, q, q_off, n_query, short_id, n_short, probe_topk, semantics,
                            x_bound, approx, err, st, wait_ns);
   else

@@ -57,7 +57,7 @@ cudaError_t launch_rerank_ws(const DevIndex &ix, const void *cen8, const TmWeigh
                              uint32_t probe_topk, int semantics, uint32_t nq_max, float x_bound,
                              float *approx, unsigned *err, cudaStream_t st, int *n_launch,
                              uint64_t wait_ns, uint32_t docs);
-// shortlisted docs per CTA the FP8 kernel is built for (32, 64, 128)
+// shortlisted docs per CTA the FP8 kernel is built for (32, 64, 128, 256)
 bool ws_docs_supported(uint32_t docs);
 
 // Learned-pruner features of every shortlisted doc with the FP8 kernel's

@@ -140,8 +140,9 @@ class Index:
         check(lib().mvr_index_set_pruner(self._h, _ptr(p), int(keep), float(margin)))
 
     def set_rerank_tile(self, docs_per_cta=0):
-        """Shortlisted docs per CTA of the FP8 MaxSim kernel: 32, 64 or 128
-        (0: the default)."""
+        """Shortlisted docs per CTA of the FP8 MaxSim kernel: 32, 64, 128 or
+        256 (0: the default, 256; queries of more than 32 tokens use at most
+        128)."""
         check(lib().mvr_index_set_rerank_tile(self._h, int(docs_per_cta)))
 
     def set_wait_limit(self, wait_ns=0):

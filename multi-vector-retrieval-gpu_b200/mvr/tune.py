@@ -83,7 +83,7 @@ def tune_batch(index, queries, k, nprobe, probe_topk, semantics,
     return dict(pick, table=table)
 
 
-def tune_tile(index, queries, k, nprobe, probe_topk, semantics, tiles=(32, 64, 128), repeats=3,
+def tune_tile(index, queries, k, nprobe, probe_topk, semantics, tiles=(32, 64, 128, 256), repeats=3,
               tok_off=None, stage=3):
     """Tile shape of the FP8 MaxSim kernel (shortlisted docs per CTA): every
     candidate is set on the index (set_rerank_tile) and the same search timed
