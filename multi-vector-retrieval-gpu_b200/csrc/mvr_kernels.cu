@@ -1192,6 +1192,108 @@ topk_kernel(const uint32_t *__restrict__ short_id, const float *__restrict__ exa
 }
 
 // ---------------------------------------------------------------------
+// K4 for k well below the list length: the same sorted top-k by a radix
+// select of the k-th largest key in shared memory (8-bit digits, high to
+// low, stopping once the boundary digit is unique), a compaction of the k
+// keys at or above it (the keys are unique: exactly k), and a bitonic sort
+// of those k only.  Same output as topk_kernel.
+// ---------------------------------------------------------------------
+__global__ void __launch_bounds__(512)
+topk_select_kernel(const uint32_t *__restrict__ short_id, const float *__restrict__ exact,
+                   const uint32_t *__restrict__ n_short, uint32_t probe_topk, uint32_t k_pad,
+                   uint32_t topk, float *__restrict__ out_s, uint32_t *__restrict__ out_id,
+                   uint32_t *__restrict__ n_out) {
+  extern __shared__ uint64_t keys[];  // [probe_topk] keys, then [k_pad] selected
+  uint64_t *sel = keys + probe_topk;
+  __shared__ uint32_t hist[256];
+  __shared__ uint32_t s_digit, s_need, s_done, s_cnt;
+  const uint32_t b = blockIdx.x;
+  const uint32_t n = min(n_short[b], probe_topk);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (n_out && tid == 0) n_out[b] = min(n, topk);
+  for (uint32_t i = tid; i < n; i += blockDim.x)
+    keys[i] = make_key(exact[(size_t)b * probe_topk + i], short_id[(size_t)b * probe_topk + i]);
+  for (uint32_t i = tid; i < k_pad; i += blockDim.x) sel[i] = 0ull;
+  if (tid == 0) s_cnt = 0;
+  uint64_t prefix = 0, mask = 0;
+  if (n > topk) {
+    uint32_t need = topk;
+    for (int pass = 0; pass < 8; pass++) {
+      const int shift = 56 - 8 * pass;
+      for (int i = tid; i < 256; i += blockDim.x) hist[i] = 0;
+      __syncthreads();
+      for (uint32_t i0 = 0; i0 < n; i0 += blockDim.x) {
+        const uint32_t i = i0 + tid;
+        uint32_t dig = 256;
+        if (i < n && (keys[i] & mask) == prefix) dig = (uint32_t)(keys[i] >> shift) & 0xffu;
+        const unsigned grp = __match_any_sync(kFull, dig);
+        if (dig < 256 && lane == __ffs(grp) - 1) atomicAdd(&hist[dig], (uint32_t)__popc(grp));
+      }
+      __syncthreads();
+      if (warp == 0) {  // lane l owns bins 255-8l .. 248-8l (high to low)
+        uint32_t cnt[8], sum = 0;
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          cnt[u] = hist[255 - 8 * lane - u];
+          sum += cnt[u];
+        }
+        uint32_t incl = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t v = __shfl_up_sync(kFull, incl, o);
+          if (lane >= o) incl += v;
+        }
+        const uint32_t excl = incl - sum;
+        if (excl < need && need <= incl) {
+          uint32_t above = excl;
+#pragma unroll
+          for (int u = 0; u < 8; u++) {
+            if (above < need && need <= above + cnt[u]) {
+              s_digit = 255 - 8 * lane - u;
+              s_need = need - above;
+              s_done = (need - above == cnt[u]) ? 1u : 0u;
+            }
+            above += cnt[u];
+          }
+        }
+      }
+      __syncthreads();
+      prefix |= (uint64_t)s_digit << shift;
+      mask |= (uint64_t)0xff << shift;
+      need = s_need;
+      if (s_done) break;
+    }
+  }
+  __syncthreads();
+  // the top keys (all n when n <= topk), unordered, then sorted descending
+  for (uint32_t i = tid; i < n; i += blockDim.x)
+    if ((keys[i] & mask) >= prefix) sel[atomicAdd(&s_cnt, 1u)] = keys[i];
+  __syncthreads();
+  for (uint32_t kk = 2; kk <= k_pad; kk <<= 1) {
+    for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
+      for (uint32_t i = tid; i < k_pad; i += blockDim.x) {
+        const uint32_t l = i ^ j;
+        if (l > i) {
+          const uint64_t a = sel[i], c = sel[l];
+          const bool desc = (i & kk) == 0;
+          if (desc ? (a < c) : (a > c)) { sel[i] = c; sel[l] = a; }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (uint32_t i = tid; i < topk; i += blockDim.x) {
+    if (i < n) {
+      out_s[(size_t)b * topk + i] = key_score(sel[i]);
+      out_id[(size_t)b * topk + i] = key_id(sel[i]);
+    } else {
+      out_s[(size_t)b * topk + i] = -INFINITY;
+      out_id[(size_t)b * topk + i] = 0xffffffffu;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------
 // host-side launchers
 // ---------------------------------------------------------------------
 // The register split of rerank_kernel (setmaxnreg) hands the FMA warps' and
@@ -1232,6 +1334,9 @@ cudaError_t configure_kernels() {
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(filter_hash_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)hash_smem_bytes(2));
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(topk_select_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)((kMaxShort + kMaxShort / 4) * sizeof(uint64_t)));
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)(kMaxShort * sizeof(uint64_t)));
@@ -1376,8 +1481,17 @@ cudaError_t launch_topk(const uint32_t *short_id, const float *exact,
                         uint32_t *out_id, uint32_t *n_out, cudaStream_t st, int *n_launch) {
   uint32_t n_pad = 1;
   while (n_pad < probe_topk) n_pad <<= 1;
-  topk_kernel<<<n_query, 512, n_pad * sizeof(uint64_t), st>>>(short_id, exact, n_short, probe_topk,
-                                                            n_pad, topk, out_s, out_id, n_out);
+  uint32_t k_pad = 1;
+  while (k_pad < topk) k_pad <<= 1;
+  if (probe_topk >= 512 && 4 * topk <= probe_topk) {
+    // select, then sort only the k best
+    topk_select_kernel<<<n_query, 512, (probe_topk + k_pad) * sizeof(uint64_t), st>>>(
+        short_id, exact, n_short, probe_topk, k_pad, topk, out_s, out_id, n_out);
+  } else {
+    topk_kernel<<<n_query, 512, n_pad * sizeof(uint64_t), st>>>(short_id, exact, n_short,
+                                                              probe_topk, n_pad, topk, out_s,
+                                                              out_id, n_out);
+  }
   *n_launch += 1;
   return cudaGetLastError();
 }
