@@ -114,7 +114,7 @@ struct Workspace {
   // per batch
   uint32_t batch_slots = 0, tok_cap = 0, np_cap = 0, short_cap = 0, topk_cap = 0;
   size_t part_cap = 0;
-  float *q = nullptr;
+  float *q = nullptr, *q2 = nullptr;  // query tokens (host-buffer calls: two, alternating)
   uint32_t *probe_id = nullptr, *part_id = nullptr;
   float *probe_s = nullptr, *part_s = nullptr;
   uint32_t *short_id = nullptr, *n_short = nullptr;
@@ -152,6 +152,9 @@ struct mvr_index {
   uint64_t device_bytes = 0;
   cudaStream_t stream = nullptr;
   std::vector<cudaEvent_t> events;
+  // host-buffer calls: query copies on their own stream, one event per batch
+  cudaStream_t copy_stream = nullptr;
+  std::vector<cudaEvent_t> copy_events;
   uint32_t batch_cap = 0;
   uint32_t rescore = 0;          // FP32 re-score count of the BF16 path (0: 4 * topk)
   void *cen_bf16 = nullptr;      // [C][128] BF16 centroid rows
@@ -219,6 +222,9 @@ struct mvr_index {
     if (ws.h_off) cudaFreeHost(ws.h_off);
     if (ws.h_qstat) cudaFreeHost(ws.h_qstat);
     for (auto e : events) cudaEventDestroy(e);
+    for (auto e : copy_events) cudaEventDestroy(e);
+    if (copy_stream) cudaStreamSynchronize(copy_stream);
+    if (copy_stream) cudaStreamDestroy(copy_stream);
     if (stream) cudaStreamDestroy(stream);
   }
   void free_scratch() {
@@ -236,7 +242,7 @@ struct mvr_index {
     ws.pr_slots = ws.pr_short = ws.pr_keep = 0;
   }
   void free_batch() {
-    for (void *p : {(void *)ws.q, (void *)ws.probe_id, (void *)ws.part_id, (void *)ws.probe_s,
+    for (void *p : {(void *)ws.q, (void *)ws.q2, (void *)ws.probe_id, (void *)ws.part_id, (void *)ws.probe_s,
                     (void *)ws.part_s, (void *)ws.short_id, (void *)ws.n_short,
                     (void *)ws.short_approx, (void *)ws.exact, (void *)ws.out_s, (void *)ws.out_id,
                     (void *)ws.r_id, (void *)ws.n_r, (void *)ws.r_score, (void *)ws.r_exact,
@@ -247,7 +253,7 @@ struct mvr_index {
     ws.r_id = ws.n_r = nullptr;
     ws.r_score = ws.r_exact = nullptr;
     ws.r_cap = 0;
-    ws.q = nullptr; ws.probe_id = ws.part_id = nullptr; ws.probe_s = ws.part_s = nullptr;
+    ws.q = ws.q2 = nullptr; ws.probe_id = ws.part_id = nullptr; ws.probe_s = ws.part_s = nullptr;
     ws.short_id = ws.n_short = nullptr; ws.short_approx = ws.exact = nullptr;
     ws.out_s = nullptr; ws.out_id = nullptr;
     ws.batch_slots = ws.tok_cap = ws.np_cap = ws.short_cap = ws.topk_cap = 0;
@@ -341,6 +347,7 @@ int ensure_batch(mvr_index *h, uint32_t slots, uint32_t tok_cap, uint32_t nprobe
   h->free_batch();
   h->ws_gen++;
   MVR_TRY(dalloc(&w.q, (size_t)tok_cap * kDim));
+  MVR_TRY(dalloc(&w.q2, (size_t)tok_cap * kDim));
   MVR_TRY(dalloc(&w.probe_id, (size_t)tok_cap * nprobe));
   MVR_TRY(dalloc(&w.probe_s, (size_t)tok_cap * nprobe));
   MVR_TRY(dalloc(&w.part_id, part_need));
@@ -367,6 +374,8 @@ int ensure_batch(mvr_index *h, uint32_t slots, uint32_t tok_cap, uint32_t nprobe
   return MVR_OK;
 }
 
+constexpr int kStages = 6;
+
 int ensure_call(mvr_index *h, size_t n_off, size_t n_stat, size_t n_events) {
   Workspace &w = h->ws;
   if (w.off_cap < n_off || w.stat_cap < n_stat || h->events.size() < n_events) h->ws_gen++;
@@ -392,6 +401,11 @@ int ensure_call(mvr_index *h, size_t n_off, size_t n_stat, size_t n_events) {
     cudaEvent_t e;
     CUDA_TRY(cudaEventCreate(&e));
     h->events.push_back(e);
+  }
+  while (h->copy_events.size() * kStages + 1 < n_events) {
+    cudaEvent_t e;
+    CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    h->copy_events.push_back(e);
   }
   return MVR_OK;
 }
@@ -445,12 +459,12 @@ int build_offsets(const uint64_t *tok_off, uint32_t n_query, uint32_t query_n_ve
 }
 
 // The shared batched pipeline.  host_io: queries/results are host buffers
-// (copied per batch inside the call); otherwise device buffers.
+// (copied per batch inside the call: each batch's queries on the handle's
+// copy stream while the previous batch computes); otherwise device buffers.
 // Events: kStages+0 per batch at the stage boundaries plus one closing event;
 // stage k of a batch = events[bt*kStages+k] .. events[bt*kStages+k+1]:
 //   0 query copy, 1 centroid scoring + probe, 2 candidate filter + shortlist,
 //   3 rerank (FP32, or BF16 tensor-core), 4 FP32 re-score + top-k, 5 result copy.
-constexpr int kStages = 6;
 
 int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, uint32_t n_query,
                 uint32_t query_n_vec, uint32_t topk, uint32_t nprobe, uint32_t probe_topk,
@@ -565,6 +579,25 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
     };
     CUDA_TRY(cudaMemcpyAsync(w.q_off, w.h_off, 2 * n_off * sizeof(uint64_t),
                              cudaMemcpyHostToDevice, rs));
+    // host buffers: batch bt's query tokens go to device buffer bt % 2 on
+    // the copy stream, one batch ahead of the kernels, once batch bt - 2
+    // (the buffer's previous user) has finished
+    auto qbuf = [&](uint32_t bt) { return (bt & 1) ? w.q2 : w.q; };
+    auto copy_in = [&](uint32_t bt) -> int {
+      const uint32_t s = bt * B, e = std::min(n_query, s + B);
+      const uint32_t T = (uint32_t)(off[e] - off[s]);
+      if (bt >= 2) CUDA_TRY(cudaStreamWaitEvent(h->copy_stream, ev(bt - 2, 5), 0));
+      CUDA_TRY(cudaMemcpyAsync(qbuf(bt), query + off[s] * kDim, (size_t)T * kDim * sizeof(float),
+                               cudaMemcpyHostToDevice, h->copy_stream));
+      CUDA_TRY(cudaEventRecord(h->copy_events[bt], h->copy_stream));
+      h2d += (size_t)T * kDim * sizeof(float);
+      return MVR_OK;
+    };
+    if (host_io) {
+      CUDA_TRY(cudaEventRecord(h->ev_in, rs));  // the copies after the caller's prior work
+      CUDA_TRY(cudaStreamWaitEvent(h->copy_stream, h->ev_in, 0));
+      MVR_TRY(copy_in(0));
+    }
     for (uint32_t bt = 0; bt < n_batch; bt++) {
       const uint32_t s = bt * B, e = std::min(n_query, s + B), nb = e - s;
       CUDA_TRY(rec(ev(bt, 0)));
@@ -572,10 +605,9 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
       const uint64_t *qo = w.q_off + (size_t)s + bt;
       const float *qp;
       if (host_io) {
-        CUDA_TRY(cudaMemcpyAsync(w.q, query + off[s] * kDim, (size_t)T * kDim * sizeof(float),
-                                 cudaMemcpyHostToDevice, rs));
-        h2d += (size_t)T * kDim * sizeof(float);
-        qp = w.q;
+        if (bt + 1 < n_batch) MVR_TRY(copy_in(bt + 1));
+        CUDA_TRY(cudaStreamWaitEvent(rs, h->copy_events[bt], 0));
+        qp = qbuf(bt);
       } else {
         qp = query + off[s] * kDim;
       }
@@ -904,6 +936,7 @@ int new_handle(int device, std::unique_ptr<mvr_index> &h) {
   CUDA_TRY(configure_kernels());
   CUDA_TRY(configure_tc_kernels());
   CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  CUDA_TRY(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
   MVR_TRY(dalloc(&h->d_err, 1));
   CUDA_TRY(cudaMemset(h->d_err, 0, sizeof(unsigned)));
   MVR_TRY(dalloc(&h->d_epoch, 1));
