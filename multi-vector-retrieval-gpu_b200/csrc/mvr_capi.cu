@@ -582,6 +582,8 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
     // host buffers: batch bt's query tokens go to device buffer bt % 2 on
     // the copy stream, one batch ahead of the kernels, once batch bt - 2
     // (the buffer's previous user) has finished
+    // (a single batch has nothing to overlap: its copy stays on rs)
+    const bool pipelined = host_io && n_batch > 1;
     auto qbuf = [&](uint32_t bt) { return (bt & 1) ? w.q2 : w.q; };
     auto copy_in = [&](uint32_t bt) -> int {
       const uint32_t s = bt * B, e = std::min(n_query, s + B);
@@ -593,7 +595,7 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
       h2d += (size_t)T * kDim * sizeof(float);
       return MVR_OK;
     };
-    if (host_io) {
+    if (pipelined) {
       CUDA_TRY(cudaEventRecord(h->ev_in, rs));  // the copies after the caller's prior work
       CUDA_TRY(cudaStreamWaitEvent(h->copy_stream, h->ev_in, 0));
       MVR_TRY(copy_in(0));
@@ -604,10 +606,15 @@ int search_impl(mvr_index *h, const float *query, const uint64_t *tok_off_in, ui
       const uint32_t T = (uint32_t)(off[e] - off[s]);
       const uint64_t *qo = w.q_off + (size_t)s + bt;
       const float *qp;
-      if (host_io) {
+      if (pipelined) {
         if (bt + 1 < n_batch) MVR_TRY(copy_in(bt + 1));
         CUDA_TRY(cudaStreamWaitEvent(rs, h->copy_events[bt], 0));
         qp = qbuf(bt);
+      } else if (host_io) {
+        CUDA_TRY(cudaMemcpyAsync(w.q, query + off[s] * kDim, (size_t)T * kDim * sizeof(float),
+                                 cudaMemcpyHostToDevice, rs));
+        h2d += (size_t)T * kDim * sizeof(float);
+        qp = w.q;
       } else {
         qp = query + off[s] * kDim;
       }
