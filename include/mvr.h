@@ -290,10 +290,11 @@ int mvr_index_set_rerank_tile(mvr_index *h, uint32_t docs_per_cta);
 
 /* Failure detection (test hook; no counterpart in the reference, whose
  * kernels have no bounded waits): the time bound of every pipeline wait of
- * the FP8 MaxSim kernel, in ns (0 restores the default, 1 s).  A wait that
- * runs out stops the kernel, which still lets its own copies and MMAs finish
- * and frees its tensor memory; the search then fails with MVR_ERR_CUDA and
- * the handle stays usable.  Tests set a tiny bound to make a wait run out. */
+ * the FP8 MaxSim kernel and of the exact FP32 MaxSim kernel, in ns (0
+ * restores the default, 1 s).  A wait that runs out stops the kernel, which
+ * still lets its own copies and MMAs finish and frees its tensor memory; the
+ * search then fails with MVR_ERR_CUDA and the handle stays usable.  Tests set
+ * a tiny bound to make a wait run out. */
 int mvr_index_set_wait_limit(mvr_index *h, uint64_t wait_ns);
 
 /* Candidate filter for ONE query with no device allocation in the call: the

@@ -146,8 +146,9 @@ class Index:
         check(lib().mvr_index_set_rerank_tile(self._h, int(docs_per_cta)))
 
     def set_wait_limit(self, wait_ns=0):
-        """Time bound (ns) of the FP8 MaxSim kernel's pipeline waits; 0 restores
-        the default (1 s).  A failure-detection test hook."""
+        """Time bound (ns) of the pipeline waits of the FP8 and the exact FP32
+        MaxSim kernels; 0 restores the default (1 s).  A failure-detection
+        test hook."""
         check(lib().mvr_index_set_wait_limit(self._h, int(wait_ns)))
 
     def set_graphs(self, enable=True):

@@ -198,13 +198,16 @@ def test_fp8_rescore_all_equals_plain_and_other_widths_run(pair2):
 
 @pytest.mark.parametrize("n_bit", [2, 4])
 def test_fp8_doc_group_boundaries(n_bit):
-    """The FP8 kernel lays each doc out in groups of 32 rows: docs of 1, 31,
-    32, 33, 63, 64, 65, 96 and 97 tokens (and random lengths up to 200) fill
-    groups exactly, leave one padding row, or spill one token into a new
-    group; shortlists of 64+ docs span several CTAs and end in partial tiles.
-    Approximate scores stay within FP8 rounding of the exact MaxSim and the
-    returned scores are exact, for 20..32-token and 33..64-token queries in
-    one batch, at every tile shape (32, 64, 128 docs per CTA)."""
+    """The FP8 kernel packs the tokens of a CTA's docs densely into 128-row
+    MMA tiles, and each epilogue warp takes 32 of those rows: docs of 1, 31,
+    32, 33, 63, 64, 65, 96 and 97 tokens (and random lengths up to 200) start
+    and end at every offset of a 32-row group, fill one exactly or cross into
+    the next, and cross tile boundaries; shortlists of 333 docs span several
+    CTAs and end in partial tiles.  Approximate scores stay within FP8
+    rounding of the exact MaxSim and the returned scores are exact, for
+    20..32-token and 33..64-token queries in one batch, at every tile shape
+    (256 -- the default; 128 for queries of more than 32 tokens --, 64, 32
+    and 128 docs per CTA)."""
     rng = np.random.default_rng(91 + n_bit)
     edge = [1, 31, 32, 33, 63, 64, 65, 96, 97]
     lens = np.concatenate([np.tile(edge, 12), rng.integers(1, 201, 300)]).astype(np.uint32)
@@ -212,7 +215,7 @@ def test_fp8_doc_group_boundaries(n_bit):
     ix = tiny_index(n_doc=len(lens), n_centroid=64, n_bit=n_bit, seed=92 + n_bit, lengths=lens)
     g, o = gpu_index(ix), oracle_of(ix)
     q, off = make_queries(ix, 6, (20, 64), seed=93)
-    for docs in (64, 32, 128):
+    for docs in (256, 64, 32, 128):
         g.set_rerank_tile(docs)
         rel = []
         for i in range(6):
